@@ -1,0 +1,806 @@
+// dd2d.cu -- distance-driven fan-beam (equiangular) and parallel-beam
+// projector pair for sm_100a.
+//
+// Operator (reference: distanceDriven2DBoxInt.cu:21-235, the box-integral
+// DDFPTracing with the 0.12 blend band; distanceDriven2DUtils.cu for the
+// back-projection pre-weights and detector mappings):
+//
+//   prj[ray] = wx * Ly * sum_rows  int_{x1(row)}^{x2(row)} img_row / |x2-x1|
+//            + (1-wx) * Lx * sum_cols int_{y1(col)}^{y2(col)} img_col / |y2-y1|
+//
+// with the two detector-cell edge rays intersected with every row (column)
+// centre and z linearly interpolated between two slices.
+//
+// Design:
+//  * dd_table_kernel evaluates, once per call and in FP64, the footprint edges
+//    of every detector-cell edge ray of every view as lines x(row) = A + B*t in
+//    image coordinates (t = row - anchor), the footprint width per cell as
+//    WA + WB*t, and the ray-length factor L per cell.  The forward projector
+//    and its exact transpose read the same FP32 table entries, so both see
+//    bit-identical footprints.
+//  * Forward projection: one thread per ray, rows read with coalesced loads
+//    (adjacent threads = adjacent cells).  Views traced along x read a
+//    transposed copy of the image so that those walks are row reads too.
+//  * Back projection is a gather (no atomics): a CTA owns a 16x16 pixel tile,
+//    streams chunks of views and stages, per view, only the window of
+//    detector cells that the tile projects onto in shared memory.  Two modes:
+//      - reference parity: the normalised detector-space box integral of
+//        DDBPFanKernel / DDBPParallelKernel (distanceDriven2DBoxInt.cu:319,409),
+//      - exact adjoint: the transpose of the forward projector, with the
+//        image-space overlaps taken from the same edge table.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "ctp_common.cuh"
+
+namespace ctp {
+
+namespace {
+
+constexpr int kTile = 16;       // back-projection pixel tile edge
+constexpr int kBPViews = 32;    // views per staged chunk (parity)
+constexpr int kAdjViews = 8;    // views per staged chunk (adjoint)
+constexpr int kMaxWin = 192;    // largest staged detector window (cells)
+constexpr int kFPThreads = 128;
+
+struct DDTab {
+    const float* eA[2];  // [nview][nu+1] edge position at the anchor row/col
+    const float* eB[2];  // [nview][nu+1] edge slope per row/col
+    const float* cWA[2]; // [nview][nu] footprint width at the anchor
+    const float* cWB[2]; // [nview][nu] width slope
+    const float* cL[2];  // [nview][nu] ray length factor dy/|cos| or dx/|sin|
+    const float* wx;     // [nview] blend weight of the row (y main axis) sweep
+    int ym, xm;          // anchor row / column
+};
+
+struct DDTabW {
+    float* eA[2];
+    float* eB[2];
+    float* cWA[2];
+    float* cWB[2];
+    float* cL[2];
+    float* wx;
+};
+
+size_t table_floats(size_t nview, size_t nu) { return 2 * (2 * nview * (nu + 1) + 3 * nview * nu) + nview; }
+
+// Table carve-out in a float buffer; the same layout for readers and writers.
+void carve_table(float* base, size_t nview, size_t nu, DDTabW& w) {
+    size_t ne = nview * (nu + 1), nc = nview * nu;
+    float* p = base;
+    for (int o = 0; o < 2; ++o) {
+        w.eA[o] = p; p += ne;
+        w.eB[o] = p; p += ne;
+        w.cWA[o] = p; p += nc;
+        w.cWB[o] = p; p += nc;
+        w.cL[o] = p; p += nc;
+    }
+    w.wx = p;
+}
+
+DDTab as_read(const DDTabW& w, int ym, int xm) {
+    DDTab t;
+    for (int o = 0; o < 2; ++o) {
+        t.eA[o] = w.eA[o]; t.eB[o] = w.eB[o];
+        t.cWA[o] = w.cWA[o]; t.cWB[o] = w.cWB[o]; t.cL[o] = w.cL[o];
+    }
+    t.wx = w.wx;
+    t.ym = ym;
+    t.xm = xm;
+    return t;
+}
+
+// Two points of the edge ray of detector edge j in image coordinates.
+// Fan: source (dso sin, -dso cos) and the arc point at angle e_j
+// (distanceDriven2DBoxInt.cu:213-226).  Parallel: the two virtual points at
+// +-(nx dx + ny dy) along the rotated axis (:143-163).  Edge j sits at
+// e_j = (-(j - nu/2) - off_u) du, so cell k spans edges k and k+1.
+__device__ void edge_ray(int geom, double th, int j, const Grid& g, const Det& d, double dsd, double dso,
+                         double& sx, double& sy, double& ex, double& ey) {
+    double s, c;
+    sincos(th, &s, &c);
+    double e = (-((double)j - 0.5 * d.nu) - (double)d.off_u) * (double)d.du;
+    if (geom == 0) {
+        sx = dso * s;
+        sy = -dso * c;
+        double lx = dsd * sin(e), ly = -dso + dsd * cos(e);
+        ex = lx * c - ly * s;
+        ey = lx * s + ly * c;
+    } else {
+        double r = (double)g.nx * g.dx + (double)g.ny * g.dy;
+        sx = e * c + r * s;
+        sy = e * s - r * c;
+        ex = e * c - r * s;
+        ey = e * s + r * c;
+    }
+    sx = (sx - g.cx) / g.dx + 0.5 * g.nx;
+    sy = (sy - g.cy) / g.dy + 0.5 * g.ny;
+    ex = (ex - g.cx) / g.dx + 0.5 * g.nx;
+    ey = (ey - g.cy) / g.dy + 0.5 * g.ny;
+}
+
+__global__ void dd_table_kernel(DDTabW t, const float* __restrict__ deg, int nview, Grid g, Det d, double dsd,
+                                double dso, int geom, int ym, int xm) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    int view = blockIdx.y;
+    if (j > d.nu || view >= nview) return;
+    double th = (double)deg[view];
+    double sx, sy, ex, ey;
+    edge_ray(geom, th, j, g, d, dsd, dso, sx, sy, ex, ey);
+    double by = (ex - sx) / (ey - sy), ay = sx + by * (ym + 0.5 - sy);
+    double bx = (ey - sy) / (ex - sx), ax = sy + bx * (xm + 0.5 - sx);
+    size_t ie = (size_t)view * (d.nu + 1) + j;
+    t.eA[0][ie] = (float)ay;
+    t.eB[0][ie] = (float)by;
+    t.eA[1][ie] = (float)ax;
+    t.eB[1][ie] = (float)bx;
+    if (j < d.nu) {
+        double sx2, sy2, ex2, ey2;
+        edge_ray(geom, th, j + 1, g, d, dsd, dso, sx2, sy2, ex2, ey2);
+        double by2 = (ex2 - sx2) / (ey2 - sy2), ay2 = sx2 + by2 * (ym + 0.5 - sy2);
+        double bx2 = (ey2 - sy2) / (ex2 - sx2), ax2 = sy2 + bx2 * (xm + 0.5 - sx2);
+        size_t ic = (size_t)view * d.nu + j;
+        t.cWA[0][ic] = (float)(ay2 - ay);
+        t.cWB[0][ic] = (float)(by2 - by);
+        t.cWA[1][ic] = (float)(ax2 - ax);
+        t.cWB[1][ic] = (float)(bx2 - bx);
+        double a = geom == 0 ? (-((double)j - 0.5 * (d.nu - 1)) - (double)d.off_u) * (double)d.du : 0.0;
+        t.cL[0][ic] = (float)((double)g.dy / fabs(cos(th - a)));
+        t.cL[1][ic] = (float)((double)g.dx / fabs(sin(th - a)));
+    }
+    if (j == 0) {
+        double s, c;
+        sincos(th, &s, &c);
+        double r = (fabs(c) - fabs(s) + kDDMarginD) / (2 * kDDMarginD);
+        t.wx[view] = (float)(r < 0 ? 0.0 : (r > 1 ? 1.0 : r));
+    }
+}
+
+// [nslice][ny][nx] -> [nslice][nx][ny]
+template <typename T>
+__global__ void transpose_kernel(T* __restrict__ out, const T* __restrict__ in, int nx, int ny) {
+    __shared__ T tile[32][33];
+    size_t slice = blockIdx.z;
+    const T* src = in + slice * (size_t)nx * ny;
+    T* dst = out + slice * (size_t)nx * ny;
+    int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        int x = x0 + threadIdx.x, y = y0 + k;
+        if (x < nx && y < ny) tile[k][threadIdx.x] = src[(size_t)y * nx + x];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        int y = y0 + threadIdx.x, x = x0 + k;
+        if (x < nx && y < ny) dst[(size_t)x * ny + y] = tile[threadIdx.x][k];
+    }
+}
+
+// z interpolation of one detector row, in the reference's float arithmetic
+// (distanceDriven2DBoxInt.cu:35-42, :214, :227).
+__device__ __forceinline__ void row_z(int iv, const Grid& g, const Det& d, int& iz, int& iz1, float& wz) {
+    float z = ((float)iv - (d.nv - 1) / 2.0f + d.off_v) * d.dv;
+    z = (z - g.cz) / g.dz + g.nz / 2.f - 0.5f;
+    z = clampf(z, 0.f, (float)g.nz);
+    int a = (int)z;
+    int b = a + 1;
+    a = min(max(a, 0), g.nz - 1);
+    b = min(max(b, 0), g.nz - 1);
+    iz = a;
+    iz1 = b;
+    wz = z - (float)a;
+}
+
+// One sweep of one ray over the lines of a slice pair.  Lines are rows of the
+// image (n = nx cells per line, nl = ny lines) or rows of the transposed image.
+template <typename Tin, bool COUNT>
+__device__ __forceinline__ float sweep(const Tin* __restrict__ s0, const Tin* __restrict__ s1, float wz, int n,
+                                       int nl, int anchor, float Aa, float Ba, float Ab, float Bb, float WA,
+                                       float WB, unsigned long long& cnt) {
+    float sum = 0.f;
+    for (int l = 0; l < nl; ++l) {
+        float t = (float)(l - anchor);
+        float xa = fmaf(Ba, t, Aa);
+        float xb = fmaf(Bb, t, Ab);
+        float lo = fminf(xa, xb), hi = fmaxf(xa, xb);
+        if (COUNT) {
+            float c1 = clampf(lo, 0.f, (float)n), c2 = clampf(hi, 0.f, (float)n);
+            if (c2 > c1) cnt += (unsigned long long)(min((int)c2, n - 1) - min((int)c1, n - 1) + 1) * (wz != 0.f ? 2 : 1);
+            continue;
+        }
+        float v = box_line(s0 + (size_t)l * n, 1, lo, hi, n);
+        if (wz != 0.f) v = v * (1.f - wz) + box_line(s1 + (size_t)l * n, 1, lo, hi, n) * wz;
+        sum += __fdividef(v, fabsf(fmaf(WB, t, WA)));
+    }
+    return sum;
+}
+
+template <typename Tin, typename Tout, bool COUNT>
+__global__ void __launch_bounds__(kFPThreads) dd2d_fp_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
+                                                             const Tin* __restrict__ imgT, DDTab tab, Grid g,
+                                                             Det d, int nview, const float* __restrict__ deg,
+                                                             int unweight_par, int accumulate,
+                                                             unsigned long long* __restrict__ count) {
+    int iu = blockIdx.x * blockDim.x + threadIdx.x;
+    int view = blockIdx.y;
+    int bz = blockIdx.z;
+    unsigned long long cnt = 0;
+    if (iu < d.nu) {
+        int iv = bz % d.nv, b = bz / d.nv;
+        int iz, iz1;
+        float wz;
+        row_z(iv, g, d, iz, iz1, wz);
+        float wx = tab.wx[view];
+        float acc = 0.f;
+        size_t ie = (size_t)view * (d.nu + 1) + iu;
+        size_t ic = (size_t)view * d.nu + iu;
+        size_t plane = (size_t)g.nx * g.ny;
+        if (wx > 0.f) {
+            const Tin* s0 = img + ((size_t)b * g.nz + iz) * plane;
+            const Tin* s1 = img + ((size_t)b * g.nz + iz1) * plane;
+            float sum = sweep<Tin, COUNT>(s0, s1, wz, g.nx, g.ny, tab.ym, tab.eA[0][ie], tab.eB[0][ie],
+                                          tab.eA[0][ie + 1], tab.eB[0][ie + 1], tab.cWA[0][ic], tab.cWB[0][ic],
+                                          cnt);
+            acc += sum * tab.cL[0][ic] * wx;
+        }
+        if (wx < 1.f) {
+            const Tin* s0 = imgT + ((size_t)b * g.nz + iz) * plane;
+            const Tin* s1 = imgT + ((size_t)b * g.nz + iz1) * plane;
+            float sum = sweep<Tin, COUNT>(s0, s1, wz, g.ny, g.nx, tab.xm, tab.eA[1][ie], tab.eB[1][ie],
+                                          tab.eA[1][ie + 1], tab.eB[1][ie + 1], tab.cWA[1][ic], tab.cWB[1][ic],
+                                          cnt);
+            acc += sum * tab.cL[1][ic] * (1.f - wx);
+        }
+        if (!COUNT) {
+            if (unweight_par) {
+                // FORCE_FBP on parallel FP: cancel the ray-length weight
+                // (ReverseWeightBPParallelKernel, distanceDriven2DUtils.cu:68).
+                float s, c;
+                sincosf(deg[view], &s, &c);
+                acc /= (fabsf(c) > fabsf(s)) ? g.dy / fabsf(c) : g.dx / fabsf(s);
+            }
+            Tout* o = prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu;
+            if (accumulate) acc += rdf(o);
+            stf(o, acc);
+        }
+    }
+    if (COUNT) {
+        __shared__ unsigned long long blk;
+        if (threadIdx.x == 0) blk = 0;
+        __syncthreads();
+        if (cnt) atomicAdd(&blk, cnt);
+        __syncthreads();
+        if (threadIdx.x == 0 && blk) atomicAdd(count, blk);
+    }
+}
+
+// Fan pre-weight of the copied sinogram for the normalised back projection
+// (PreweightBPKernel, distanceDriven2DUtils.cu:8-33): hard switch on the view
+// angle, weight from the ray angle.
+template <typename Tin>
+__global__ void fan_preweight_kernel(float* __restrict__ out, const Tin* __restrict__ prj,
+                                     const float* __restrict__ deg, int nview, Det d, Grid g, size_t total) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    int iu = (int)(i % d.nu);
+    int view = (int)((i / ((size_t)d.nu * d.nv)) % nview);
+    float th = deg[view];
+    float a = (-((float)iu - (d.nu - 1) / 2.0f) - d.off_u) * d.du;
+    float s, c, sa, ca;
+    sincosf(th, &s, &c);
+    sincosf(th - a, &sa, &ca);
+    float w = (fabsf(c) > fabsf(s)) ? g.dy / fabsf(ca) : g.dx / fabsf(sa);
+    out[i] = ldf(prj + i) * w;
+}
+
+// Detector edge coordinate (cell k spans [k, k+1]) of a physical point for
+// one view: fan atan(rx/(ry+dso)) (distanceDriven2DUtils.cu:96-101),
+// parallel x cos + y sin (:104-107), then -(a/du + off_u) + nu/2.
+__device__ __forceinline__ float det_coord(bool fan, float x, float y, float c, float s, float dso, const Det& d) {
+    float a;
+    if (fan) {
+        float rx = x * c + y * s;
+        float ry = -x * s + y * c;
+        a = atanf(rx / (ry + dso));
+    } else {
+        a = x * c + y * s;
+    }
+    return -(a / d.du + d.off_u) + d.nu / 2.0f;
+}
+
+__device__ __forceinline__ double det_coord_d(bool fan, double x, double y, double c, double s, double dso,
+                                              const Det& d) {
+    double a;
+    if (fan) {
+        double rx = x * c + y * s;
+        double ry = -x * s + y * c;
+        a = atan(rx / (ry + dso));
+    } else {
+        a = x * c + y * s;
+    }
+    return -(a / d.du + (double)d.off_u) + 0.5 * d.nu;
+}
+
+// Window of detector cells covering a pixel tile for one view: the tile
+// corners' detector coordinates (extreme over a convex tile) with a margin.
+__device__ void tile_window(bool fan, int tx0, int ty0, const Grid& g, const Det& d, double c, double s,
+                            double dso, int win, int& w0, int& ok) {
+    int tx1 = min(tx0 + kTile, g.nx), ty1 = min(ty0 + kTile, g.ny);
+    double xs[2] = {(tx0 - 0.5 * g.nx) * g.dx + g.cx, (tx1 - 0.5 * g.nx) * g.dx + g.cx};
+    double ys[2] = {(ty0 - 0.5 * g.ny) * g.dy + g.cy, (ty1 - 0.5 * g.ny) * g.dy + g.cy};
+    double jmin = 1e300, jmax = -1e300;
+    bool good = true;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            if (fan && (-xs[a] * s + ys[b] * c) + dso <= 0) good = false;
+            double j = det_coord_d(fan, xs[a], ys[b], c, s, dso, d);
+            jmin = fmin(jmin, j);
+            jmax = fmax(jmax, j);
+        }
+    if (!(jmin > -1e9 && jmax < 1e9)) good = false;
+    if (good) {
+        w0 = (int)floor(jmin) - 2;
+        good = ((int)ceil(jmax) + 2 - w0) <= win;
+    } else {
+        w0 = 0;
+    }
+    ok = good ? 1 : 0;
+}
+
+// Reference-parity normalised back projection (and FBP mode).
+//   fan:      DDBPFanKernel distanceDriven2DBoxInt.cu:319-396
+//   parallel: DDBPParallelKernel :409-497
+// src is the (pre-weighted, for fan non-FBP) sinogram of this batch item.
+template <bool FAN, typename Tp, typename Tout>
+__global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
+    Tout* __restrict__ img, const Tp* __restrict__ src, const float* __restrict__ deg, int nview, Grid g, Det d,
+    float dso, int fbp, int accumulate, int win) {
+    extern __shared__ float smem[];
+    float* s_win = smem;                               // [kBPViews][win]
+    float* s_cos = s_win + kBPViews * win;             // [kBPViews]
+    float* s_sin = s_cos + kBPViews;
+    int* s_w0 = (int*)(s_sin + kBPViews);
+    int* s_ok = s_w0 + kBPViews;
+
+    int tiles_x = (g.nx + kTile - 1) / kTile;
+    int tx0 = (blockIdx.x % tiles_x) * kTile, ty0 = (blockIdx.x / tiles_x) * kTile;
+    int bz = blockIdx.y;
+    int iz = bz % g.nz, b = bz / g.nz;
+    int tid = threadIdx.x;
+    int ix = tx0 + (tid % kTile), iy = ty0 + (tid / kTile);
+
+    // pixel geometry (ImgToPhysics + half pixel, :340-350)
+    float xc = ((float)ix - g.nx / 2.f) * g.dx + g.cx + g.dx / 2;
+    float yc = ((float)iy - g.ny / 2.f) * g.dy + g.cy + g.dy / 2;
+    float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
+    float x1 = xc - g.dx / 2.0f, x2 = xc + g.dx / 2.0f;
+    float y1 = yc - g.dy / 2.0f, y2 = yc + g.dy / 2.0f;
+    float ivf = zc / d.dv + d.off_v + d.nv / 2.f - 0.5f;
+    int iv = (int)ivf;  // float passed to an int parameter: truncation (:383)
+    bool row_ok = iv >= 0 && iv < d.nv;
+    const Tp* rows = src + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
+    size_t view_stride = (size_t)d.nv * d.nu;
+
+    float acc = 0.f;
+    for (int v0 = 0; v0 < nview && row_ok; v0 += kBPViews) {
+        int nvc = min(kBPViews, nview - v0);
+        if (tid < nvc) {
+            double s, c;
+            sincos((double)deg[v0 + tid], &s, &c);
+            s_cos[tid] = (float)c;
+            s_sin[tid] = (float)s;
+            int w0, ok;
+            tile_window(FAN, tx0, ty0, g, d, c, s, dso, win, w0, ok);
+            s_w0[tid] = w0;
+            s_ok[tid] = ok;
+        }
+        __syncthreads();
+        for (int i = tid; i < nvc * win; i += blockDim.x) {
+            int vi = i / win, k = i - vi * win;
+            int cell = s_w0[vi] + k;
+            float val = 0.f;
+            if (s_ok[vi] && cell >= 0 && cell < d.nu) val = ldf(rows + (size_t)(v0 + vi) * view_stride + cell);
+            s_win[i] = val;
+        }
+        __syncthreads();
+        if (ix < g.nx && iy < g.ny) {
+            for (int vi = 0; vi < nvc; ++vi) {
+                float c = s_cos[vi], s = s_sin[vi];
+                const float* w = s_win + vi * win;
+                float off = (float)s_w0[vi];
+                bool ok = s_ok[vi] != 0;
+                const Tp* grow = rows + (size_t)(v0 + vi) * view_stride;
+                if (FAN) {
+                    float a1, a2;
+                    if (fabsf(c) > fabsf(s)) {
+                        a1 = det_coord(true, x1, yc, c, s, dso, d);
+                        a2 = det_coord(true, x2, yc, c, s, dso, d);
+                    } else {
+                        a1 = det_coord(true, xc, y1, c, s, dso, d);
+                        a2 = det_coord(true, xc, y2, c, s, dso, d);
+                    }
+                    float lo = fminf(a1, a2), hi = fmaxf(a1, a2);
+                    float val = ok ? box_line_smem(w, lo - off, hi - off, win) : box_line(grow, 1, lo, hi, d.nu);
+                    val = val / (hi - lo);
+                    if (fbp) {
+                        float rx = xc * c + yc * s, ry = -xc * s + yc * c;
+                        val *= dso * dso / (rx * rx + (dso + ry) * (dso + ry));
+                    }
+                    acc += val;
+                } else {
+                    float valx = 0.f, valy = 0.f;
+                    if (fabsf(c) > fabsf(s) - kDDMargin) {
+                        float u1 = det_coord(false, x1, yc, c, s, dso, d);
+                        float u2 = det_coord(false, x2, yc, c, s, dso, d);
+                        float lo = fminf(u1, u2), hi = fmaxf(u1, u2);
+                        valx = (ok ? box_line_smem(w, lo - off, hi - off, win) : box_line(grow, 1, lo, hi, d.nu)) /
+                               (hi - lo);
+                    }
+                    if (fabsf(c) < fabsf(s) + kDDMargin) {
+                        float u1 = det_coord(false, xc, y1, c, s, dso, d);
+                        float u2 = det_coord(false, xc, y2, c, s, dso, d);
+                        float lo = fminf(u1, u2), hi = fmaxf(u1, u2);
+                        valy = (ok ? box_line_smem(w, lo - off, hi - off, win) : box_line(grow, 1, lo, hi, d.nu)) /
+                               (hi - lo);
+                    }
+                    float wx = clampf((fabsf(c) - fabsf(s) + kDDMargin) / (2 * kDDMargin), 0.f, 1.f);
+                    float val = valx * wx + valy * (1 - wx);
+                    if (!fbp) val *= (fabsf(c) > fabsf(s)) ? g.dy / fabsf(c) : g.dx / fabsf(s);  // :39-65
+                    acc += val;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (ix < g.nx && iy < g.ny) {
+        Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+        if (accumulate) acc += rdf(o);
+        stf(o, acc);
+    }
+}
+
+// Exact transpose of dd2d_fp_kernel, as a gather over a pixel tile.
+// For each pixel and view, the candidate cells come from the pixel's detector
+// coordinates (+-1 cell); the weight of cell k is the image-space overlap of
+// the pixel with the cell's footprint on the pixel's row (column) divided by
+// the footprint width, times L and the blend weight -- the forward
+// projector's coefficient, from the same table entries.
+template <bool FAN, typename Tp, typename Tout>
+__global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
+    Tout* __restrict__ img, const Tp* __restrict__ prj, const float* __restrict__ deg, DDTab tab, int nview, Grid g,
+    Det d, float dso, int accumulate, int win) {
+    extern __shared__ float smem[];
+    // per view: p[win], then per orientation: A[win+1], B[win+1], WA[win], WB[win], L[win]
+    const int per_o = 2 * (win + 1) + 3 * win;
+    const int per_v = win + 2 * per_o;
+    float* s_view = smem;                           // [kAdjViews][per_v]
+    float* s_cos = s_view + kAdjViews * per_v;      // [kAdjViews]
+    float* s_sin = s_cos + kAdjViews;
+    float* s_wx = s_sin + kAdjViews;
+    int* s_w0 = (int*)(s_wx + kAdjViews);
+    int* s_ok = s_w0 + kAdjViews;
+
+    int tiles_x = (g.nx + kTile - 1) / kTile;
+    int tx0 = (blockIdx.x % tiles_x) * kTile, ty0 = (blockIdx.x / tiles_x) * kTile;
+    int bz = blockIdx.y;
+    int iz = bz % g.nz, b = bz / g.nz;
+    int tid = threadIdx.x;
+    int ix = tx0 + (tid % kTile), iy = ty0 + (tid / kTile);
+    float xc = ((float)ix - g.nx / 2.f) * g.dx + g.cx + g.dx / 2;
+    float yc = ((float)iy - g.ny / 2.f) * g.dy + g.cy + g.dy / 2;
+    float x1 = xc - g.dx / 2.0f, x2 = xc + g.dx / 2.0f;
+    float y1 = yc - g.dy / 2.0f, y2 = yc + g.dy / 2.0f;
+    float ty = (float)(iy - tab.ym), tx = (float)(ix - tab.xm);
+    float fx = (float)ix, fy = (float)iy;
+
+    float acc = 0.f;
+    for (int iv = 0; iv < d.nv; ++iv) {
+        // weight of slice iz in the z interpolation of detector row iv
+        int za, zb;
+        float wz;
+        row_z(iv, g, d, za, zb, wz);
+        float om = (za == iz ? 1.f - wz : 0.f) + ((zb == iz && wz != 0.f) ? wz : 0.f);
+        if (om == 0.f) continue;
+        const Tp* rows = prj + ((size_t)b * nview * d.nv + iv) * d.nu;
+        for (int v0 = 0; v0 < nview; v0 += kAdjViews) {
+            int nvc = min(kAdjViews, nview - v0);
+            if (tid < nvc) {
+                double s, c;
+                sincos((double)deg[v0 + tid], &s, &c);
+                s_cos[tid] = (float)c;
+                s_sin[tid] = (float)s;
+                s_wx[tid] = tab.wx[v0 + tid];
+                int w0, ok;
+                tile_window(FAN, tx0, ty0, g, d, c, s, dso, win, w0, ok);
+                s_w0[tid] = w0;
+                s_ok[tid] = ok;
+            }
+            __syncthreads();
+            for (int i = tid; i < nvc * per_v; i += blockDim.x) {
+                int vi = i / per_v, r = i - vi * per_v;
+                int view = v0 + vi;
+                int w0 = s_w0[vi];
+                float val = 0.f;
+                if (s_ok[vi]) {
+                    if (r < win) {
+                        int cell = w0 + r;
+                        if (cell >= 0 && cell < d.nu) val = ldf(rows + (size_t)view * d.nv * d.nu + cell) * om;
+                    } else {
+                        int q = r - win;
+                        int o = q / per_o;
+                        q -= o * per_o;
+                        if (q < 2 * (win + 1)) {
+                            int e = w0 + (q % (win + 1));
+                            if (e >= 0 && e <= d.nu) {
+                                size_t ie = (size_t)view * (d.nu + 1) + e;
+                                val = (q < win + 1) ? tab.eA[o][ie] : tab.eB[o][ie];
+                            }
+                        } else {
+                            q -= 2 * (win + 1);
+                            int which = q / win;
+                            int cell = w0 + (q - which * win);
+                            if (cell >= 0 && cell < d.nu) {
+                                size_t ic = (size_t)view * d.nu + cell;
+                                val = which == 0 ? tab.cWA[o][ic] : (which == 1 ? tab.cWB[o][ic] : tab.cL[o][ic]);
+                            }
+                        }
+                    }
+                }
+                s_view[i] = val;
+            }
+            __syncthreads();
+            if (ix < g.nx && iy < g.ny) {
+                for (int vi = 0; vi < nvc; ++vi) {
+                    int view = v0 + vi;
+                    float c = s_cos[vi], s = s_sin[vi], wx = s_wx[vi];
+                    int w0 = s_w0[vi];
+                    bool ok = s_ok[vi] != 0;
+                    const float* sv = s_view + vi * per_v;
+                    for (int o = 0; o < 2; ++o) {
+                        float wo = o == 0 ? wx : 1.f - wx;
+                        if (!(wo > 0.f)) continue;
+                        float j1, j2, t, pmin;
+                        if (o == 0) {
+                            j1 = det_coord(FAN, x1, yc, c, s, dso, d);
+                            j2 = det_coord(FAN, x2, yc, c, s, dso, d);
+                            t = ty;
+                            pmin = fx;
+                        } else {
+                            j1 = det_coord(FAN, xc, y1, c, s, dso, d);
+                            j2 = det_coord(FAN, xc, y2, c, s, dso, d);
+                            t = tx;
+                            pmin = fy;
+                        }
+                        int kmin = max((int)floorf(fminf(j1, j2)) - 1, 0);
+                        int kmax = min((int)floorf(fmaxf(j1, j2)) + 1, d.nu - 1);
+                        float sum = 0.f;
+                        const float* sp = sv;
+                        const float* sA = sv + win + o * per_o;
+                        const float* sB = sA + (win + 1);
+                        const float* sWA = sB + (win + 1);
+                        const float* sWB = sWA + win;
+                        const float* sL = sWB + win;
+                        for (int k = kmin; k <= kmax; ++k) {
+                            float Aa, Ba, Ab, Bb, WA, WB, L, p;
+                            int kk = k - w0;
+                            if (ok && kk >= 0 && kk < win) {
+                                Aa = sA[kk]; Ba = sB[kk]; Ab = sA[kk + 1]; Bb = sB[kk + 1];
+                                WA = sWA[kk]; WB = sWB[kk]; L = sL[kk]; p = sp[kk];
+                            } else {
+                                size_t ie = (size_t)view * (d.nu + 1) + k, ic = (size_t)view * d.nu + k;
+                                Aa = tab.eA[o][ie]; Ba = tab.eB[o][ie]; Ab = tab.eA[o][ie + 1]; Bb = tab.eB[o][ie + 1];
+                                WA = tab.cWA[o][ic]; WB = tab.cWB[o][ic]; L = tab.cL[o][ic];
+                                p = ldf(rows + (size_t)view * d.nv * d.nu + k) * om;
+                            }
+                            float xa = fmaf(Ba, t, Aa), xb = fmaf(Bb, t, Ab);
+                            float ov = fminf(fmaxf(xa, xb), pmin + 1.f) - fmaxf(fminf(xa, xb), pmin);
+                            if (ov > 0.f) sum += p * L * __fdividef(ov, fabsf(fmaf(WB, t, WA)));
+                        }
+                        acc += sum * wo;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (ix < g.nx && iy < g.ny) {
+        Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+        if (accumulate) acc += rdf(o);
+        stf(o, acc);
+    }
+}
+
+// Staged window (cells) needed by a 16x16 tile, from a conservative bound on
+// the tile's projected size.  0 means "read the sinogram from global memory".
+int window_cells(const ctp_geometry& g, int geom) {
+    double diag = kTile * sqrt((double)g.dx * g.dx + (double)g.dy * g.dy);
+    double cells;
+    if (geom == 0) {
+        double hx = 0.5 * g.nx * g.dx, hy = 0.5 * g.ny * g.dy;
+        double rmax = sqrt((fabs(g.cx) + hx) * (fabs(g.cx) + hx) + (fabs(g.cy) + hy) * (fabs(g.cy) + hy));
+        double near = (double)g.dso - rmax;
+        if (near <= diag) return 0;
+        cells = 2 * atan(0.5 * diag / near) / fabs((double)g.du);
+    } else {
+        cells = diag / fabs((double)g.du);
+    }
+    int w = (int)ceil(cells) + 8;
+    return w <= kMaxWin ? w : 0;
+}
+
+template <typename T>
+const T* cptr(const void* p) { return static_cast<const T*>(p); }
+template <typename T>
+T* mptr(void* p) { return static_cast<T*>(p); }
+
+size_t fp_workspace(const ctp_geometry& g) {
+    return align_up(table_floats(g.nview, g.nu) * sizeof(float)) + align_up(g.nbatch * g.nz * g.ny * g.nx * 4);
+}
+
+int build_table(float* base, const float* deg, const ctp_geometry& g, int geom, cudaStream_t s, DDTab& tab) {
+    DDTabW w;
+    carve_table(base, g.nview, g.nu, w);
+    int ym = (int)(g.ny / 2), xm = (int)(g.nx / 2);
+    double dsd = geom == 0 ? g.dsd : 1000.0, dso = geom == 0 ? g.dso : 500.0;
+    dim3 grid((unsigned)((g.nu + 1 + 127) / 128), (unsigned)g.nview);
+    dd_table_kernel<<<grid, 128, 0, s>>>(w, deg, (int)g.nview, make_grid(g), make_det(g), dsd, dso, geom, ym, xm);
+    tab = as_read(w, ym, xm);
+    return check_launch("dd_table_kernel");
+}
+
+template <typename Tin, typename Tout>
+int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
+              unsigned flags, char* ws, cudaStream_t s) {
+    DDTab tab;
+    int rc = build_table(reinterpret_cast<float*>(ws), deg, g, geom, s, tab);
+    if (rc) return rc;
+    Tin* imgT = reinterpret_cast<Tin*>(ws + align_up(table_floats(g.nview, g.nu) * sizeof(float)));
+    dim3 tg((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 31) / 32), (unsigned)(g.nbatch * g.nz));
+    transpose_kernel<Tin><<<tg, dim3(32, 8), 0, s>>>(imgT, cptr<Tin>(img), (int)g.nx, (int)g.ny);
+    if ((rc = check_launch("transpose_kernel"))) return rc;
+    dim3 grid((unsigned)((g.nu + kFPThreads - 1) / kFPThreads), (unsigned)g.nview, (unsigned)(g.nbatch * g.nv));
+    int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
+    dd2d_fp_kernel<Tin, Tout, false><<<grid, kFPThreads, 0, s>>>(
+        mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g), (int)g.nview, deg, unweight,
+        (flags & CTP_FLAG_ZERO_OUT) ? 0 : 0, nullptr);
+    return check_launch("dd2d_fp_kernel");
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+size_t dd2d_fp_workspace(const ctp_geometry& g, int, int, unsigned) { return fp_workspace(g); }
+
+int dd2d_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
+            unsigned flags, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
+    Scratch scr;
+    int rc = scr.acquire(workspace, workspace_bytes, fp_workspace(g), s);
+    if (rc) return rc;
+    bool in16 = flags & (CTP_FLAG_IN_BF16 | CTP_FLAG_IN_FP16);
+    bool out16 = flags & (CTP_FLAG_OUT_BF16 | CTP_FLAG_OUT_FP16);
+    if (!in16 && !out16) return launch_fp<float, float>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_BF16) && (flags & CTP_FLAG_OUT_BF16))
+        return launch_fp<__nv_bfloat16, __nv_bfloat16>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_FP16) && (flags & CTP_FLAG_OUT_FP16))
+        return launch_fp<__half, __half>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_BF16) && !out16)
+        return launch_fp<__nv_bfloat16, float>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_FP16) && !out16)
+        return launch_fp<__half, float>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+    return set_error(CTP_ERR_UNSUPPORTED, "dd2d_fp: unsupported storage type combination (flags 0x%x)", flags);
+}
+
+int dd2d_nnz(unsigned long long* nnz_host, const float* deg, const ctp_geometry& g, int geom, cudaStream_t s) {
+    if (!nnz_host) return set_error(CTP_ERR_INVALID_ARGUMENT, "nnz output pointer is null");
+    Scratch scr;
+    size_t need = align_up(table_floats(g.nview, g.nu) * sizeof(float)) + 256;
+    int rc = scr.acquire(nullptr, 0, need, s);
+    if (rc) return rc;
+    DDTab tab;
+    if ((rc = build_table(reinterpret_cast<float*>(scr.base()), deg, g, geom, s, tab))) return rc;
+    unsigned long long* cnt =
+        reinterpret_cast<unsigned long long*>(scr.base() + align_up(table_floats(g.nview, g.nu) * sizeof(float)));
+    cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
+    dim3 grid((unsigned)((g.nu + kFPThreads - 1) / kFPThreads), (unsigned)g.nview, (unsigned)g.nv);
+    dd2d_fp_kernel<float, float, true><<<grid, kFPThreads, 0, s>>>(nullptr, nullptr, nullptr, tab, make_grid(g),
+                                                                    make_det(g), (int)g.nview, deg, 0, 0, cnt);
+    if ((rc = check_launch("dd2d_fp_kernel<count>"))) return rc;
+    cudaError_t e = cudaMemcpyAsync(nnz_host, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_error((int)e, "dd2d_nnz: %s", cudaGetErrorString(e));
+    return CTP_OK;
+}
+
+namespace {
+
+size_t bp_workspace(const ctp_geometry& g, int geom, int type, unsigned flags) {
+    if (flags & CTP_FLAG_ADJOINT) return align_up(table_floats(g.nview, g.nu) * sizeof(float));
+    bool fbp = type & (CTP_TYPE_FBP | CTP_TYPE_FORCE_FBP);
+    if (geom == 0 && !fbp) return align_up(g.nbatch * g.nview * g.nv * g.nu * sizeof(float));
+    return 0;
+}
+
+template <typename Tin, typename Tout>
+int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& g, int geom, int type,
+              unsigned flags, char* ws, cudaStream_t s) {
+    Grid gr = make_grid(g);
+    Det dt = make_det(g);
+    int nview = (int)g.nview;
+    float dso = geom == 0 ? g.dso : 500.0f;
+    int accumulate = (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1;
+    int tiles = (int)(((g.nx + kTile - 1) / kTile) * ((g.ny + kTile - 1) / kTile));
+    dim3 grid((unsigned)tiles, (unsigned)(g.nbatch * g.nz));
+    int win = window_cells(g, geom);
+    int wl = win > 0 ? win : 1;
+    int rc;
+    if (flags & CTP_FLAG_ADJOINT) {
+        DDTab tab;
+        if ((rc = build_table(reinterpret_cast<float*>(ws), deg, g, geom, s, tab))) return rc;
+        int per_v = wl + 2 * (2 * (wl + 1) + 3 * wl);
+        size_t shm = (size_t)kAdjViews * per_v * 4 + kAdjViews * 5 * 4;
+        if (geom == 0) {
+            auto k = dd2d_bp_adjoint_kernel<true, Tin, Tout>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, tab, nview, gr, dt, dso,
+                                               accumulate, win > 0 ? win : 0);
+        } else {
+            auto k = dd2d_bp_adjoint_kernel<false, Tin, Tout>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, tab, nview, gr, dt, dso,
+                                               accumulate, win > 0 ? win : 0);
+        }
+        return check_launch("dd2d_bp_adjoint_kernel");
+    }
+    int fbp = (type & (CTP_TYPE_FBP | CTP_TYPE_FORCE_FBP)) ? 1 : 0;
+    size_t shm = (size_t)kBPViews * wl * 4 + kBPViews * 4 * 4;
+    if (geom == 0) {
+        if (!fbp) {
+            float* wprj = reinterpret_cast<float*>(ws);
+            size_t total = g.nbatch * g.nview * g.nv * g.nu;
+            fan_preweight_kernel<Tin><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(wprj, cptr<Tin>(prj), deg,
+                                                                                    nview, dt, gr, total);
+            if ((rc = check_launch("fan_preweight_kernel"))) return rc;
+            auto k = dd2d_bp_parity_kernel<true, float, Tout>;
+            k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), wprj, deg, nview, gr, dt, dso, 0, accumulate,
+                                               win > 0 ? win : 0);
+        } else {
+            auto k = dd2d_bp_parity_kernel<true, Tin, Tout>;
+            k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, 1,
+                                               accumulate, win > 0 ? win : 0);
+        }
+    } else {
+        auto k = dd2d_bp_parity_kernel<false, Tin, Tout>;
+        k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, fbp,
+                                           accumulate, win > 0 ? win : 0);
+    }
+    return check_launch("dd2d_bp_parity_kernel");
+}
+
+}  // namespace
+
+size_t dd2d_bp_workspace(const ctp_geometry& g, int geom, int type, unsigned flags) {
+    return bp_workspace(g, geom, type, flags);
+}
+
+int dd2d_bp(void* img, const void* prj, const float* deg, const ctp_geometry& g, int geom, int type,
+            unsigned flags, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
+    Scratch scr;
+    size_t need = bp_workspace(g, geom, type, flags);
+    int rc = scr.acquire(workspace, workspace_bytes, need, s);
+    if (rc) return rc;
+    bool in16 = flags & (CTP_FLAG_IN_BF16 | CTP_FLAG_IN_FP16);
+    bool out16 = flags & (CTP_FLAG_OUT_BF16 | CTP_FLAG_OUT_FP16);
+    if (!in16 && !out16) return launch_bp<float, float>(img, prj, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_BF16) && (flags & CTP_FLAG_OUT_BF16))
+        return launch_bp<__nv_bfloat16, __nv_bfloat16>(img, prj, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_FP16) && (flags & CTP_FLAG_OUT_FP16))
+        return launch_bp<__half, __half>(img, prj, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_BF16) && !out16)
+        return launch_bp<__nv_bfloat16, float>(img, prj, deg, g, geom, type, flags, scr.base(), s);
+    if ((flags & CTP_FLAG_IN_FP16) && !out16)
+        return launch_bp<__half, float>(img, prj, deg, g, geom, type, flags, scr.base(), s);
+    return set_error(CTP_ERR_UNSUPPORTED, "dd2d_bp: unsupported storage type combination (flags 0x%x)", flags);
+}
+
+}  // namespace ctp

@@ -1,0 +1,371 @@
+// fbp.cu -- ramp filtering (parallel / equiangular fan) and the pixel-driven
+// fan FBP back projector for sm_100a.
+//
+// Ramp filter (reference: GetRamp fbpMath.cu:90-267, fbpParallel::Filter
+// fbpParallel.cu:14-109, fbpFan::Filter fbp.cu:15-162).  The reference builds a
+// spatial ramp h of length L = 2nu-1 (offset k = i-(nu-1)), applies the window
+// in the L-point frequency domain, and convolves every zero-padded detector
+// row with the result, keeping outputs nu-1 .. 2nu-2.  That is the linear
+// convolution
+//      out[i] = scale * sum_j p[j] g[i-j],   g = real(IDFT_L(DFT_L(h) W)),
+// which this file evaluates as a circular convolution of size N >= 2nu-1
+// (N = 2^a 3^b), exact because g has support [-(nu-1), nu-1]:
+//   * g is computed once per (nu, da, window, geometry) on the host in FP64
+//     and its N-point spectrum (real: g is even) cached on the device;
+//   * one pad/weight kernel writes all rows of the batch into an in-place
+//     R2C layout, cuFFT runs batched R2C and C2R over every row at once, a
+//     multiply kernel scales the spectrum, and a crop kernel writes the first
+//     nu samples of each row.
+#include <cufft.h>
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "ctp_common.cuh"
+
+namespace ctp {
+
+namespace {
+
+int fft_size(int nu) {
+    int need = 2 * nu - 1, best = 1 << 30;
+    for (long p2 = 1; p2 < (1L << 30); p2 *= 2)
+        for (long p3 = p2; p3 < (1L << 30); p3 *= 3) {
+            if (p3 >= need && p3 < best) best = (int)p3;
+            if (p3 >= need) break;
+        }
+    return best;
+}
+
+// Windowed ramp g[k], k = 0..nu-1 (g is even), FP64, following GetRamp.
+std::vector<double> ramp_kernel(int nu, double da, int filter, bool equiangular) {
+    const int L = 2 * nu - 1;
+    std::vector<double> h(L), w(L), cosL(L), sinL(L);
+    for (int i = 0; i < L; ++i) {
+        long k = (long)i - (nu - 1);
+        if (k == 0)
+            h[i] = 1.0 / (4 * da * da);
+        else if (k % 2 != 0)
+            h[i] = equiangular ? -1.0 / (M_PI * M_PI * sin(k * da) * sin(k * da))
+                               : -1.0 / (M_PI * M_PI * (double)k * (double)k * da * da);
+        else
+            h[i] = 0;
+        double t = 2 * M_PI * i / L;
+        switch (filter) {  // fbpMath.cu:178-208
+            case 1: w[i] = 0.54 + 0.46 * cos(t); break;
+            case 2: w[i] = 0.5 + 0.5 * cos(t); break;
+            case 3: w[i] = fabs(cos(M_PI * i / L)); break;
+            default: w[i] = 1.0;
+        }
+        cosL[i] = cos(t);
+        sinL[i] = sin(t);
+    }
+    // H = DFT_L(h);  g = real(IDFT_L(H .* w)) / L
+    std::vector<double> Hr(L), Hi(L);
+    for (int m = 0; m < L; ++m) {
+        double re = 0, im = 0;
+        long idx = 0;
+        for (int n = 0; n < L; ++n) {
+            re += h[n] * cosL[idx];
+            im -= h[n] * sinL[idx];
+            idx += m;
+            if (idx >= L) idx -= L;
+        }
+        Hr[m] = re * w[m];
+        Hi[m] = im * w[m];
+    }
+    std::vector<double> g(nu);
+    for (int k = 0; k < nu; ++k) {
+        // average of offsets +k and -k (exactly equal in exact arithmetic)
+        double acc = 0;
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            long n = (long)(nu - 1) + sgn * k;
+            double re = 0;
+            long idx = 0;
+            for (int m = 0; m < L; ++m) {
+                re += Hr[m] * cosL[idx] - Hi[m] * sinL[idx];
+                idx += n;
+                idx %= L;
+            }
+            acc += re / L;
+            if (k == 0) { acc *= 2; break; }
+        }
+        g[k] = acc / 2;
+    }
+    return g;
+}
+
+struct Spectrum {
+    float* dev = nullptr;  // N/2+1 real coefficients
+    int n = 0;
+};
+
+std::mutex g_spec_mu;
+std::map<std::tuple<int, int, long long, int, int, int>, Spectrum> g_spec;
+
+// Device spectrum of g for this (device, nu, da, filter, kind, N); built once.
+int get_spectrum(int nu, double da, int filter, bool equiangular, int N, const float** out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    long long dkey;
+    memcpy(&dkey, &da, sizeof(dkey));
+    auto key = std::make_tuple(dev, nu, dkey, filter, (int)equiangular, N);
+    std::lock_guard<std::mutex> lk(g_spec_mu);
+    auto it = g_spec.find(key);
+    if (it != g_spec.end()) {
+        *out = it->second.dev;
+        return CTP_OK;
+    }
+    std::vector<double> g = ramp_kernel(nu, da, filter, equiangular);
+    int M = N / 2 + 1;
+    std::vector<float> G(M);
+    std::vector<double> cosN(N);
+    for (int i = 0; i < N; ++i) cosN[i] = cos(2 * M_PI * i / N);
+    for (int m = 0; m < M; ++m) {
+        double acc = g[0];
+        long long idx = 0;
+        for (int k = 1; k < nu; ++k) {
+            idx += m;
+            if (idx >= N) idx -= N;
+            acc += 2 * g[k] * cosN[idx];
+        }
+        G[m] = (float)acc;
+    }
+    Spectrum sp;
+    sp.n = M;
+    cudaError_t e = cudaMalloc(&sp.dev, sizeof(float) * M);  // one-time table, kept for the process
+    if (e == cudaSuccess) e = cudaMemcpy(sp.dev, G.data(), sizeof(float) * M, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return set_error((int)e, "ramp spectrum upload: %s", cudaGetErrorString(e));
+    g_spec[key] = sp;
+    *out = sp.dev;
+    return CTP_OK;
+}
+
+struct Plan {
+    cufftHandle fwd = 0, inv = 0;
+    size_t work = 0;
+    std::mutex mu;
+};
+
+std::mutex g_plan_mu;
+std::map<std::tuple<int, int, int>, std::unique_ptr<Plan>> g_plans;
+
+int get_plan(int N, int batch, Plan** out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    auto key = std::make_tuple(dev, N, batch);
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plans.find(key);
+    if (it != g_plans.end()) {
+        *out = it->second.get();
+        return CTP_OK;
+    }
+    std::unique_ptr<Plan> p(new Plan());
+    int n[1] = {N};
+    int rembed[1] = {2 * (N / 2 + 1)}, cembed[1] = {N / 2 + 1};
+    size_t w1 = 0, w2 = 0;
+    if (cufftCreate(&p->fwd) != CUFFT_SUCCESS || cufftCreate(&p->inv) != CUFFT_SUCCESS)
+        return set_error(CTP_ERR_CUFFT, "cufftCreate failed");
+    cufftSetAutoAllocation(p->fwd, 0);
+    cufftSetAutoAllocation(p->inv, 0);
+    if (cufftMakePlanMany(p->fwd, 1, n, rembed, 1, rembed[0], cembed, 1, cembed[0], CUFFT_R2C, batch, &w1) !=
+            CUFFT_SUCCESS ||
+        cufftMakePlanMany(p->inv, 1, n, cembed, 1, cembed[0], rembed, 1, rembed[0], CUFFT_C2R, batch, &w2) !=
+            CUFFT_SUCCESS)
+        return set_error(CTP_ERR_CUFFT, "cufftMakePlanMany failed (N=%d, batch=%d)", N, batch);
+    p->work = w1 > w2 ? w1 : w2;
+    *out = p.get();
+    g_plans[key] = std::move(p);
+    return CTP_OK;
+}
+
+constexpr int kMaxRowsPerExec = 32768;
+
+// Zero-pad and pre-weight rows into the in-place R2C layout.
+__global__ void pad_kernel(float* __restrict__ buf, const float* __restrict__ prj, int nu, int N, int stride,
+                           size_t rows, int fan, float da, float off_u) {
+    size_t r = blockIdx.y + (size_t)blockIdx.z * gridDim.y;
+    if (r >= rows) return;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < stride; n += gridDim.x * blockDim.x) {
+        float v = 0.f;
+        if (n < nu) {
+            v = prj[r * nu + n];
+            if (fan) v *= cosf(((n - (nu - 1) / 2.f) - off_u) * da);  // fbp.cu:62-66
+        }
+        buf[r * stride + n] = v;
+    }
+}
+
+__global__ void spectrum_mul_kernel(float2* __restrict__ spec, const float* __restrict__ G, int M, size_t rows,
+                                    float scale) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= rows * M) return;
+    float g = G[i % M] * scale;
+    float2 v = spec[i];
+    spec[i] = make_float2(v.x * g, v.y * g);
+}
+
+__global__ void crop_kernel(float* __restrict__ out, const float* __restrict__ buf, int nu, int stride, size_t rows) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= rows * nu) return;
+    size_t r = i / nu;
+    int n = (int)(i - r * nu);
+    out[i] = buf[r * stride + n];
+}
+
+}  // namespace
+
+size_t ramp_filter_workspace(const ctp_geometry& g, int, int) {
+    size_t rows = g.nbatch * g.nview * g.nv;
+    int N = fft_size((int)g.nu);
+    size_t chunk = rows < (size_t)kMaxRowsPerExec ? rows : (size_t)kMaxRowsPerExec;
+    Plan* p = nullptr;
+    if (chunk == 0 || get_plan(N, (int)chunk, &p)) return 0;
+    return align_up(chunk * 2 * (N / 2 + 1) * sizeof(float)) + align_up(p->work);
+}
+
+int ramp_filter(float* fprj, const float* prj, const ctp_geometry& g, int geom, int filter, unsigned,
+                void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
+    int nu = (int)g.nu;
+    size_t rows = g.nbatch * g.nview * g.nv;
+    int N = fft_size(nu), M = N / 2 + 1, stride = 2 * M;
+    size_t chunk = rows < (size_t)kMaxRowsPerExec ? rows : (size_t)kMaxRowsPerExec;
+    Plan* plan = nullptr;
+    int rc = get_plan(N, (int)chunk, &plan);
+    if (rc) return rc;
+    const float* G = nullptr;
+    bool fan = geom == 0;
+    if ((rc = get_spectrum(nu, (double)g.du, filter, fan, N, &G))) return rc;
+    Scratch scr;
+    size_t buf_bytes = align_up(chunk * stride * sizeof(float));
+    if ((rc = scr.acquire(workspace, workspace_bytes, buf_bytes + align_up(plan->work), s))) return rc;
+    float* buf = reinterpret_cast<float*>(scr.base());
+    void* work = scr.base() + buf_bytes;
+    // fbpParallel.cu:59 / fbp.cu:103 scale, with the 1/N of the unnormalised C2R
+    double scale = M_PI / (double)g.nview * (double)g.du / (fan ? (double)g.dso : 1.0) / N;
+    for (size_t r0 = 0; r0 < rows; r0 += chunk) {
+        size_t nr = rows - r0 < chunk ? rows - r0 : chunk;
+        dim3 pg((unsigned)((stride + 255) / 256 > 8 ? 8 : (stride + 255) / 256), (unsigned)(nr < 65535 ? nr : 65535),
+                (unsigned)((nr + 65534) / 65535));
+        pad_kernel<<<pg, 256, 0, s>>>(buf, prj + r0 * nu, nu, N, stride, nr, fan ? 1 : 0, g.du, g.off_u);
+        if ((rc = check_launch("pad_kernel"))) return rc;
+        {
+            std::lock_guard<std::mutex> lk(plan->mu);
+            cufftSetStream(plan->fwd, s);
+            cufftSetStream(plan->inv, s);
+            cufftSetWorkArea(plan->fwd, work);
+            cufftSetWorkArea(plan->inv, work);
+            if (nr != chunk) {
+                // last partial chunk: zero the tail rows so the fixed-batch plan
+                // transforms defined data
+                cudaMemsetAsync(buf + nr * stride, 0, (chunk - nr) * stride * sizeof(float), s);
+            }
+            if (cufftExecR2C(plan->fwd, buf, reinterpret_cast<cufftComplex*>(buf)) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecR2C failed");
+            size_t ns = nr * (size_t)M;
+            spectrum_mul_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(reinterpret_cast<float2*>(buf), G, M,
+                                                                           nr, (float)scale);
+            if ((rc = check_launch("spectrum_mul_kernel"))) return rc;
+            if (cufftExecC2R(plan->inv, reinterpret_cast<cufftComplex*>(buf), buf) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecC2R failed");
+        }
+        size_t no = nr * (size_t)nu;
+        crop_kernel<<<(unsigned)((no + 255) / 256), 256, 0, s>>>(fprj + r0 * nu, buf, nu, stride, nr);
+        if ((rc = check_launch("crop_kernel"))) return rc;
+    }
+    return CTP_OK;
+}
+
+// ------------------------------------------------------------------ fbp_bp
+namespace {
+
+constexpr int kFbpViews = 64;
+constexpr int kFbpZ = 4;
+
+// Pixel-driven fan back projection with the FBP distance weight,
+// bpFanKernel3D fbp.cu:265-337; bilinear InterpolateXY(truncate = true),
+// cudaMath.cu:227-260.  One thread per pixel and kFbpZ slices.
+__global__ void fbp_fan_bp_kernel(float* __restrict__ img, const float* __restrict__ prj,
+                                  const float* __restrict__ deg, int nview, Grid g, Det d, float dso,
+                                  int accumulate) {
+    __shared__ float s_c[kFbpViews], s_s[kFbpViews];
+    int ix = blockIdx.x * 32 + (threadIdx.x & 31);
+    int iy = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int zb = blockIdx.z % ((g.nz + kFbpZ - 1) / kFbpZ);
+    int b = blockIdx.z / ((g.nz + kFbpZ - 1) / kFbpZ);
+    int iz0 = zb * kFbpZ;
+    float x = ((float)ix + 0.5f - g.nx / 2.f) * g.dx + g.cx;
+    float y = ((float)iy + 0.5f - g.ny / 2.f) * g.dy + g.cy;
+    float z0 = ((float)iz0 + 0.5f - g.nz / 2.f) * g.dz + g.cz;
+    float acc[kFbpZ];
+#pragma unroll
+    for (int q = 0; q < kFbpZ; ++q) acc[q] = 0.f;
+    const float* pb = prj + (size_t)b * nview * d.nv * d.nu;
+    for (int v0 = 0; v0 < nview; v0 += kFbpViews) {
+        int nvc = min(kFbpViews, nview - v0);
+        if (threadIdx.x < nvc) {
+            double s, c;
+            sincos((double)deg[v0 + threadIdx.x], &s, &c);
+            s_c[threadIdx.x] = (float)c;
+            s_s[threadIdx.x] = (float)s;
+        }
+        __syncthreads();
+        if (ix < g.nx && iy < g.ny) {
+            for (int vi = 0; vi < nvc; ++vi) {
+                float c = s_c[vi], s = s_s[vi];
+                float rx = x * c + y * s, ry = -x * s + y * c;
+                float a = atanf(rx / (ry + dso));
+                float dist = dso * dso / (rx * rx + (dso + ry) * (dso + ry));
+                float pu = -(a / d.du + d.off_u) + (d.nu - 1.0f) / 2.0f;
+                if (pu < 0 || pu >= d.nu) continue;
+                int i0 = (int)pu;
+                int i1 = min(i0 + 1, d.nu - 1);
+                float wu = pu - (float)i0;
+                const float* pv_base = pb + (size_t)(v0 + vi) * d.nv * d.nu;
+#pragma unroll
+                for (int q = 0; q < kFbpZ; ++q) {
+                    float pv = (z0 + q * g.dz) / d.dv + d.off_v + (d.nv - 1.0f) / 2.f;
+                    if (pv < 0 || pv >= d.nv) continue;
+                    int j0 = (int)pv;
+                    int j1 = min(j0 + 1, d.nv - 1);
+                    float wv = pv - (float)j0;
+                    const float* r0 = pv_base + (size_t)j0 * d.nu;
+                    const float* r1 = pv_base + (size_t)j1 * d.nu;
+                    float v = __ldg(r0 + i0) * (1 - wu) * (1 - wv) + __ldg(r0 + i1) * wu * (1 - wv) +
+                              __ldg(r1 + i0) * (1 - wu) * wv + __ldg(r1 + i1) * wu * wv;
+                    acc[q] += v * dist;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (ix < g.nx && iy < g.ny) {
+#pragma unroll
+        for (int q = 0; q < kFbpZ; ++q) {
+            int iz = iz0 + q;
+            if (iz >= g.nz) break;
+            float* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+            *o = (accumulate ? *o : 0.f) + acc[q];
+        }
+    }
+}
+
+}  // namespace
+
+int fbp_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry& g, unsigned flags,
+               cudaStream_t s) {
+    int zb = (int)((g.nz + kFbpZ - 1) / kFbpZ);
+    dim3 grid((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 7) / 8), (unsigned)(g.nbatch * zb));
+    fbp_fan_bp_kernel<<<grid, 256, 0, s>>>(img, prj, deg, (int)g.nview, make_grid(g), make_det(g), g.dso,
+                                           (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1);
+    return check_launch("fbp_fan_bp_kernel");
+}
+
+}  // namespace ctp

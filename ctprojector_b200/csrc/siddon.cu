@@ -1,0 +1,268 @@
+// siddon.cu -- Siddon cone-beam projector pair for arbitrary trajectories,
+// sm_100a.
+//
+// Reference: siddon.cu (InboundAlpha :37, InboundFirstVoxel :59,
+// OutboundFirstVoxel :78, GetAlpha :95, InitializeSiddon :104, SiddonRayTracing
+// :175, SiddonRayTracingTransposeAtomicAdd :259, MoveSourceDstNearGrid :342)
+// and siddonCone.cu:12-74 (one ray per detector cell; u,v measured from the
+// detector centre along det_u / det_v).
+//
+// The ray set-up (near-grid move, entry/exit parameters, first voxel) and the
+// alpha recurrences run in FP64, so segment lengths do not drift along the
+// walk; the line integral accumulates in FP32.  Forward and back projection
+// share the same walk function, so the back projector is the exact transpose
+// of the forward projector up to FP32 rounding of the accumulation.
+// One thread per ray; a 32x8 block covers a detector tile so that a warp's
+// rays traverse neighbouring voxels.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "ctp_common.cuh"
+
+namespace ctp {
+
+namespace {
+
+constexpr double kEps = 1e-6;  // siddon.cu:35
+
+struct Ray {
+    double alpha[3], dalpha[3];
+    int ng[3];
+    int step[3];  // voxel index step along x, y, z (+-1, or 0)
+    double aprev;
+    bool hit;
+};
+
+// Ray end points for cell (iu, iv) of a view, moved near the grid.
+__device__ void ray_ends(double src[3], double dst[3], int view, int iu, int iv, const float* __restrict__ dc,
+                         const float* __restrict__ du_, const float* __restrict__ dv_,
+                         const float* __restrict__ sr, const Grid& g, const Det& d) {
+    double u = ((double)iu - d.off_u - (d.nu - 1) / 2.0) * d.du;
+    double v = ((double)iv - d.off_v - (d.nv - 1) / 2.0) * d.dv;
+    for (int k = 0; k < 3; ++k) {
+        src[k] = (double)sr[view * 3 + k];
+        dst[k] = (double)dc[view * 3 + k] + (double)du_[view * 3 + k] * u + (double)dv_[view * 3 + k] * v;
+    }
+    // MoveSourceDstNearGrid, siddon.cu:342-362
+    double ex = (double)g.nx * g.dx, ey = (double)g.ny * g.dy, ez = (double)g.nz * g.dz;
+    double r = sqrt(ex * ex + ey * ey + ez * ez);
+    double dd[3] = {dst[0] - src[0], dst[1] - src[1], dst[2] - src[2]};
+    double len = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+    if (len >= 1e-6)
+        for (int k = 0; k < 3; ++k) dd[k] /= len;
+    double t0 = (g.cx - src[0]) * dd[0] + (g.cy - src[1]) * dd[1] + (g.cz - src[2]) * dd[2];
+    double t1 = (dst[0] - g.cx) * dd[0] + (dst[1] - g.cy) * dd[1] + (dst[2] - g.cz) * dd[2];
+    if (t0 > r)
+        for (int k = 0; k < 3; ++k) src[k] += (t0 - r) * dd[k];
+    if (t1 > r)
+        for (int k = 0; k < 3; ++k) dst[k] -= (t1 - r) * dd[k];
+}
+
+// InitializeSiddon, siddon.cu:104-173 (alphas scaled by the ray length).
+__device__ Ray init_ray(const double src[3], const double dst[3], const Grid& g) {
+    Ray R;
+    R.hit = false;
+    double dist = sqrt((src[0] - dst[0]) * (src[0] - dst[0]) + (src[1] - dst[1]) * (src[1] - dst[1]) +
+                       (src[2] - dst[2]) * (src[2] - dst[2]));
+    double cen[3] = {(double)g.cx, (double)g.cy, (double)g.cz};
+    double sp[3] = {(double)g.dx, (double)g.dy, (double)g.dz};
+    int n[3] = {g.nx, g.ny, g.nz};
+    double s[3], dd[3], a0[3] = {1, 1, 1}, a1[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) {
+        s[k] = (src[k] - cen[k]) / sp[k] + 0.5 * n[k];
+        double e = (dst[k] - cen[k]) / sp[k] + 0.5 * n[k];
+        dd[k] = e - s[k];
+        if (fabs(dd[k]) > kEps) {
+            a0[k] = (0 - s[k]) / dd[k];
+            a1[k] = (n[k] - s[k]) / dd[k];
+        } else if (s[k] < 0 || s[k] > n[k]) {
+            return R;
+        }
+    }
+    double amin = 0, amax = 1;
+    for (int k = 0; k < 3; ++k) {
+        amin = fmax(amin, fmin(a0[k], a1[k]));
+        amax = fmin(amax, fmax(a0[k], a1[k]));
+    }
+    if (amax <= amin) return R;
+    for (int k = 0; k < 3; ++k) {
+        double p0 = s[k] + amin * dd[k];
+        int v = (int)p0;
+        if (fabs(dd[k]) > kEps) v = v < 0 ? 0 : (v >= n[k] ? n[k] - 1 : v);
+        if (v < 0 || v >= n[k]) return R;
+        R.ng[k] = v;
+        double p1 = dd[k] > kEps ? (double)(v + 1) : (double)v;
+        if (fabs(dd[k]) > kEps) {
+            R.alpha[k] = (p1 - s[k]) / dd[k] * dist;
+            R.dalpha[k] = dist / fabs(dd[k]);
+        } else {
+            R.alpha[k] = 2.0 * dist;
+            R.dalpha[k] = 0;
+        }
+        R.step[k] = dd[k] > 0 ? 1 : -1;
+    }
+    R.aprev = amin * dist;
+    R.hit = true;
+    return R;
+}
+
+// The walk of SiddonRayTracing (siddon.cu:187-252): pick the nearest
+// crossing (ties go to the later axis), emit the segment in the current voxel,
+// step, stop when the index leaves the grid.
+template <typename F>
+__device__ __forceinline__ void walk(Ray& R, const Grid& g, F&& emit) {
+    int n[3] = {g.nx, g.ny, g.nz};
+    long long nxy = (long long)g.nx * g.ny;
+    long long idx = R.ng[2] * nxy + (long long)R.ng[1] * g.nx + R.ng[0];
+    long long mv[3] = {R.step[0], (long long)R.step[1] * g.nx, R.step[2] * nxy};
+    while (true) {
+        int k = (R.alpha[0] < R.alpha[1] && R.alpha[0] < R.alpha[2]) ? 0 : (R.alpha[1] < R.alpha[2] ? 1 : 2);
+        double anow = R.alpha[k];
+        R.alpha[k] += R.dalpha[k];
+        R.ng[k] += R.step[k];
+        emit(idx, (float)(anow - R.aprev));
+        R.aprev = anow;
+        if (R.ng[k] < 0 || R.ng[k] >= n[k]) break;
+        idx += mv[k];
+    }
+}
+
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(256) siddon_fp_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
+                                                        const float* __restrict__ dc, const float* __restrict__ du_,
+                                                        const float* __restrict__ dv_, const float* __restrict__ sr,
+                                                        int nview, Grid g, Det d, int accumulate) {
+    int iu = blockIdx.x * 32 + (threadIdx.x & 31);
+    int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int view = blockIdx.z % nview, b = blockIdx.z / nview;
+    if (iu >= d.nu || iv >= d.nv) return;
+    double src[3], dst[3];
+    ray_ends(src, dst, view, iu, iv, dc, du_, dv_, sr, g, d);
+    Ray R = init_ray(src, dst, g);
+    float acc = 0.f;
+    if (R.hit) {
+        const Tin* vol = img + (size_t)b * g.nx * g.ny * g.nz;
+        walk(R, g, [&](long long idx, float len) { acc += ldf(vol + idx) * len; });
+    }
+    Tout* o = prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu;
+    stf(o, (accumulate ? rdf(o) : 0.f) + acc);
+}
+
+// Transpose: scatter prj * length into the volume (FP32 atomics, as the
+// reference's SiddonRayTracingTransposeAtomicAdd, siddon.cu:332).
+template <typename Tin>
+__global__ void __launch_bounds__(256) siddon_bp_kernel(float* __restrict__ img, const Tin* __restrict__ prj,
+                                                        const float* __restrict__ dc, const float* __restrict__ du_,
+                                                        const float* __restrict__ dv_, const float* __restrict__ sr,
+                                                        int nview, Grid g, Det d) {
+    int iu = blockIdx.x * 32 + (threadIdx.x & 31);
+    int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int view = blockIdx.z % nview, b = blockIdx.z / nview;
+    if (iu >= d.nu || iv >= d.nv) return;
+    float p = ldf(prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu);
+    if (p == 0.f) return;
+    double src[3], dst[3];
+    ray_ends(src, dst, view, iu, iv, dc, du_, dv_, sr, g, d);
+    Ray R = init_ray(src, dst, g);
+    if (!R.hit) return;
+    float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
+    walk(R, g, [&](long long idx, float len) { atomicAdd(vol + idx, p * len); });
+}
+
+__global__ void __launch_bounds__(256) siddon_count_kernel(unsigned long long* __restrict__ count,
+                                                           const float* __restrict__ dc, const float* __restrict__ du_,
+                                                           const float* __restrict__ dv_,
+                                                           const float* __restrict__ sr, int nview, Grid g, Det d) {
+    int iu = blockIdx.x * 32 + (threadIdx.x & 31);
+    int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int view = blockIdx.z;
+    unsigned long long c = 0;
+    if (iu < d.nu && iv < d.nv) {
+        double src[3], dst[3];
+        ray_ends(src, dst, view, iu, iv, dc, du_, dv_, sr, g, d);
+        Ray R = init_ray(src, dst, g);
+        if (R.hit) walk(R, g, [&](long long, float) { ++c; });
+    }
+    __shared__ unsigned long long blk;
+    if (threadIdx.x == 0) blk = 0;
+    __syncthreads();
+    if (c) atomicAdd(&blk, c);
+    __syncthreads();
+    if (threadIdx.x == 0 && blk) atomicAdd(count, blk);
+}
+
+dim3 ray_grid(const ctp_geometry& g, size_t nz_mult) {
+    return dim3((unsigned)((g.nu + 31) / 32), (unsigned)((g.nv + 7) / 8), (unsigned)(g.nview * nz_mult));
+}
+
+}  // namespace
+
+int siddon_fp(void* prj, const void* img, const float* dc, const float* du_, const float* dv_, const float* sr,
+              const ctp_geometry& g, unsigned flags, cudaStream_t s) {
+    int acc = (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1;
+    dim3 grid = ray_grid(g, g.nbatch);
+    Grid gr = make_grid(g);
+    Det dt = make_det(g);
+    int nv = (int)g.nview;
+    if (flags & CTP_FLAG_IN_BF16) {
+        if (flags & CTP_FLAG_OUT_BF16)
+            siddon_fp_kernel<__nv_bfloat16, __nv_bfloat16><<<grid, 256, 0, s>>>(
+                (__nv_bfloat16*)prj, (const __nv_bfloat16*)img, dc, du_, dv_, sr, nv, gr, dt, acc);
+        else
+            siddon_fp_kernel<__nv_bfloat16, float><<<grid, 256, 0, s>>>((float*)prj, (const __nv_bfloat16*)img, dc,
+                                                                       du_, dv_, sr, nv, gr, dt, acc);
+    } else if (flags & CTP_FLAG_IN_FP16) {
+        if (flags & CTP_FLAG_OUT_FP16)
+            siddon_fp_kernel<__half, __half><<<grid, 256, 0, s>>>((__half*)prj, (const __half*)img, dc, du_, dv_, sr,
+                                                                  nv, gr, dt, acc);
+        else
+            siddon_fp_kernel<__half, float><<<grid, 256, 0, s>>>((float*)prj, (const __half*)img, dc, du_, dv_, sr,
+                                                                 nv, gr, dt, acc);
+    } else {
+        if (flags & (CTP_FLAG_OUT_BF16 | CTP_FLAG_OUT_FP16))
+            return set_error(CTP_ERR_UNSUPPORTED, "siddon_fp: FP32 input with 16-bit output is not supported");
+        siddon_fp_kernel<float, float><<<grid, 256, 0, s>>>((float*)prj, (const float*)img, dc, du_, dv_, sr, nv, gr,
+                                                            dt, acc);
+    }
+    return check_launch("siddon_fp_kernel");
+}
+
+int siddon_bp(void* img, const void* prj, const float* dc, const float* du_, const float* dv_, const float* sr,
+              const ctp_geometry& g, unsigned flags, cudaStream_t s) {
+    if (flags & (CTP_FLAG_OUT_BF16 | CTP_FLAG_OUT_FP16))
+        return set_error(CTP_ERR_UNSUPPORTED, "siddon_bp accumulates in FP32: 16-bit output is not supported");
+    if (flags & CTP_FLAG_ZERO_OUT) {
+        cudaError_t e = cudaMemsetAsync(img, 0, g.nbatch * g.nz * g.ny * g.nx * sizeof(float), s);
+        if (e != cudaSuccess) return set_error((int)e, "siddon_bp memset: %s", cudaGetErrorString(e));
+    }
+    dim3 grid = ray_grid(g, g.nbatch);
+    if (flags & CTP_FLAG_IN_BF16)
+        siddon_bp_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>((float*)img, (const __nv_bfloat16*)prj, dc, du_, dv_,
+                                                             sr, (int)g.nview, make_grid(g), make_det(g));
+    else if (flags & CTP_FLAG_IN_FP16)
+        siddon_bp_kernel<__half><<<grid, 256, 0, s>>>((float*)img, (const __half*)prj, dc, du_, dv_, sr,
+                                                      (int)g.nview, make_grid(g), make_det(g));
+    else
+        siddon_bp_kernel<float><<<grid, 256, 0, s>>>((float*)img, (const float*)prj, dc, du_, dv_, sr,
+                                                     (int)g.nview, make_grid(g), make_det(g));
+    return check_launch("siddon_bp_kernel");
+}
+
+int siddon_nnz(unsigned long long* nnz_host, const float* dc, const float* du_, const float* dv_, const float* sr,
+               const ctp_geometry& g, cudaStream_t s) {
+    if (!nnz_host) return set_error(CTP_ERR_INVALID_ARGUMENT, "nnz output pointer is null");
+    Scratch scr;
+    int rc = scr.acquire(nullptr, 0, 256, s);
+    if (rc) return rc;
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(scr.base());
+    cudaMemsetAsync(cnt, 0, sizeof(*cnt), s);
+    siddon_count_kernel<<<ray_grid(g, 1), 256, 0, s>>>(cnt, dc, du_, dv_, sr, (int)g.nview, make_grid(g),
+                                                      make_det(g));
+    if ((rc = check_launch("siddon_count_kernel"))) return rc;
+    cudaError_t e = cudaMemcpyAsync(nnz_host, cnt, sizeof(*cnt), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_error((int)e, "siddon_nnz: %s", cudaGetErrorString(e));
+    return CTP_OK;
+}
+
+}  // namespace ctp

@@ -1,0 +1,28 @@
+"""Tomosynthesis geometry (detector u = (1,0,0), v = (0,1,0)), device arrays.
+
+Same calls as ct_projector/projector/cupy/tomo.py of the reference:
+distance_driven_fp (:15), distance_driven_bp (:85).  ``branchless`` selects
+the same operator (both are the exact box integral).
+"""
+from __future__ import annotations
+
+from ... import _lib
+from ...errors import CTProjectorError
+from .. import _device as D
+from .ct_projector import ct_projector
+
+
+def distance_driven_fp(projector: ct_projector, img, det_center, src, branchless: bool = False, *, out=None,
+                       stream=None):
+    return D.like_input(D.tomo_fp(projector, img, det_center, src, out=out, stream=stream), img)
+
+
+def distance_driven_bp(projector: ct_projector, prj, det_center, src, branchless: bool = False, *, out=None,
+                       stream=None):
+    return D.like_input(D.tomo_bp(projector, prj, det_center, src, out=out, stream=stream), prj)
+
+
+def filter_fbp(projector: ct_projector, prj, det_center, src, filter_type: str = "hann", cutoff_x: float = 1,
+               cutoff_y: float = 1):
+    """The tomosynthesis FBP filter (reference tomo.py:157) is not part of this build."""
+    raise CTProjectorError(_lib.CTP_ERR_UNSUPPORTED, "tomo.filter_fbp is not implemented in ctprojector_b200")

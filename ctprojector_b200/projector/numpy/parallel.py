@@ -1,0 +1,54 @@
+"""Parallel-beam geometry, host arrays.
+
+Same calls as ct_projector/projector/numpy/parallel.py of the reference:
+ramp_filter (:20), distance_driven_fp (:133), distance_driven_bp (:192).
+"""
+from __future__ import annotations
+
+from ctypes import c_size_t
+from typing import Union
+
+import numpy as np
+
+from .._device import filter_code
+from ._host import c_float, c_int, call, f32, geom_args, p
+from .ct_projector import ct_projector
+
+
+def ramp_filter(projector: ct_projector, prj: np.ndarray, filter_type: str = "hann") -> np.ndarray:
+    prj = f32(prj)
+    fprj = np.zeros(prj.shape, np.float32)
+    call("cfbpParallelFilter", p(fprj), p(prj), c_int(prj.shape[0]), c_size_t(prj.shape[3]), c_size_t(prj.shape[2]),
+         c_size_t(prj.shape[1]), c_float(projector.du), c_float(projector.dv), c_float(projector.off_u),
+         c_float(projector.off_v), c_int(filter_code(filter_type)))
+    return fprj
+
+
+def distance_driven_fp(projector: ct_projector, img: np.ndarray, angles: np.ndarray,
+                       branchless: Union[bool, int] = False) -> np.ndarray:
+    img = f32(img)
+    angles = f32(angles)
+    prj = np.zeros([img.shape[0], len(angles), projector.nv, projector.nu], np.float32)
+    call("cDistanceDrivenParallelProjection", p(prj), p(img), p(angles),
+         *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(projector.du),
+         c_float(projector.dv), c_float(projector.off_u), c_float(projector.off_v), c_int(2 if branchless else 0))
+    return prj
+
+
+def distance_driven_bp(projector: ct_projector, prj: np.ndarray, angles: np.ndarray,
+                       is_fbp: Union[bool, int] = False, branchless: Union[bool, int] = False) -> np.ndarray:
+    prj = f32(prj)
+    angles = f32(angles)
+    img = np.zeros([prj.shape[0], projector.nz, projector.ny, projector.nx], np.float32)
+    call("cDistanceDrivenParallelBackprojection", p(img), p(prj), p(angles),
+         *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(projector.du),
+         c_float(projector.dv), c_float(projector.off_u), c_float(projector.off_v),
+         c_int((1 if is_fbp else 0) + (2 if branchless else 0)))
+    return img
+
+
+def pixel_driven_bp(projector: ct_projector, prj, angles):
+    """The pixel-driven parallel back projector (reference :75) is not part of this build."""
+    from ...errors import CTProjectorError
+
+    raise CTProjectorError(1002, "parallel.pixel_driven_bp is not implemented in ctprojector_b200")

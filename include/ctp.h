@@ -1,0 +1,265 @@
+/*
+ * ctp.h -- C ABI of libctp.so, the sm_100a projector pair (ctprojector_b200).
+ *
+ * Two families of entry points:
+ *
+ *  1. Reference-compatible entries.  Same symbol names, argument order and
+ *     meaning as the reference libprojector.so (wudufan/CTProjector,
+ *     src/ct_projector/kernel/projector/cuda/), so a caller that binds the
+ *     reference library through ctypes can load this library instead.
+ *       c*    take HOST pointers: device buffers are taken from a
+ *             stream-ordered pool, data is copied in and out, and the call
+ *             returns when the result is on the host.
+ *       cupy* take DEVICE pointers and run asynchronously on the legacy
+ *             default stream, like the reference (which also synchronises).
+ *     Each returns 0 on success, a CUDA error code, or a CTP_ERR_* code.
+ *     Output semantics follow the reference: DD and tomo forward projection
+ *     and tomo back projection overwrite the output; DD back projection,
+ *     Siddon forward/back projection and fbp_bp accumulate into it; the
+ *     filters overwrite.
+ *
+ *  2. Extended entries (ctp_*): explicit cudaStream_t (as void*), caller
+ *     workspace, and flags.  They never synchronise the device.  A NULL
+ *     workspace makes the library take scratch from the stream-ordered pool
+ *     (cudaMallocAsync/cudaFreeAsync on the same stream).
+ *
+ * Array layouts (row-major, float32 unless a flag says otherwise):
+ *   image    [nbatch][nz][ny][nx]
+ *   sinogram [nbatch][nview][nv][nu]
+ *   angles   [nview] radians
+ *   cone/tomo geometry arrays [nview][3] as (x, y, z) in mm.
+ */
+#ifndef CTP_H
+#define CTP_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (CUDA runtime codes pass through unchanged) ---------- */
+#define CTP_OK 0
+#define CTP_ERR_INVALID_ARGUMENT 1001 /* null pointer, zero or inconsistent size */
+#define CTP_ERR_UNSUPPORTED 1002      /* flag or geometry this build does not handle */
+#define CTP_ERR_WORKSPACE 1003        /* caller workspace smaller than required */
+#define CTP_ERR_CUFFT 1004            /* cuFFT plan or execution failure */
+#define CTP_ERR_TOO_LARGE 1005        /* request exceeds a fixed-size internal buffer */
+
+/* ---- flags for the extended entries ------------------------------------ */
+#define CTP_FLAG_ZERO_OUT 0x1  /* treat the output as zero (write instead of accumulate) */
+#define CTP_FLAG_ADJOINT 0x2   /* DD back projection: exact transpose of the forward projector */
+#define CTP_FLAG_IN_BF16 0x10  /* the input array is bfloat16 (FP32 accumulation) */
+#define CTP_FLAG_IN_FP16 0x20  /* the input array is float16 */
+#define CTP_FLAG_OUT_BF16 0x40 /* the output array is bfloat16 */
+#define CTP_FLAG_OUT_FP16 0x80 /* the output array is float16 */
+
+/* typeProjector bits of the DD 2D entries, as in the reference
+ * (distanceDriven2D.cu:12-25): bit0 FBP weighting, bit1 branchless,
+ * bit2 force FBP weighting.  Branchless selects the same operator as the box
+ * integral here (both are the exact integral of the piecewise-constant image);
+ * this build evaluates it one way only. */
+#define CTP_TYPE_FBP 0x1
+#define CTP_TYPE_BRANCHLESS 0x2
+#define CTP_TYPE_FORCE_FBP 0x4
+
+/* Geometry of one call (mirrors the reference Grid/Detector structs,
+ * projector.h:7-28, plus batch, view count and source distances). */
+typedef struct ctp_geometry {
+    size_t nbatch;
+    size_t nx, ny, nz;
+    float dx, dy, dz;
+    float cx, cy, cz;
+    size_t nu, nv, nview;
+    float du, dv;
+    float off_u, off_v;
+    float dsd, dso;
+} ctp_geometry;
+
+/* Last error message of the calling thread ("" when none). */
+const char* ctpGetLastErrorString(void);
+/* Library version string. */
+const char* ctpVersion(void);
+
+/* ======================================================================== */
+/* 1. Reference-compatible entries                                          */
+/* ======================================================================== */
+
+/* projector.cu:12 */
+int SetDevice(int device);
+
+/* distanceDriven2D.cu:109 (cupy*) / :205 (c*): fan-beam equiangular DD
+ * forward projection; da is the angular cell size du/dsd. */
+int cupyDistanceDrivenFanProjection(float* prj, const float* img, const float* deg, size_t nBatches, size_t nx,
+                                    size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy,
+                                    float cz, size_t nu, size_t nv, size_t nview, float da, float dv, float off_a,
+                                    float off_v, float dsd, float dso, int typeProjector);
+int cDistanceDrivenFanProjection(float* prj, const float* img, const float* deg, size_t nBatches, size_t nx,
+                                 size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                                 size_t nu, size_t nv, size_t nview, float da, float dv, float off_a, float off_v,
+                                 float dsd, float dso, int typeProjector);
+
+/* distanceDriven2D.cu:158 (cupy*) / :285 (c*): parallel-beam DD forward
+ * projection (the reference injects dsd=1000, dso=500, :187). */
+int cupyDistanceDrivenParallelProjection(float* prj, const float* img, const float* deg, size_t nBatches,
+                                         size_t nx, size_t ny, size_t nz, float dx, float dy, float dz, float cx,
+                                         float cy, float cz, size_t nu, size_t nv, size_t nview, float du, float dv,
+                                         float off_u, float off_v, int typeProjector);
+int cDistanceDrivenParallelProjection(float* prj, const float* img, const float* deg, size_t nBatches, size_t nx,
+                                      size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy,
+                                      float cz, size_t nu, size_t nv, size_t nview, float du, float dv, float off_u,
+                                      float off_v, int typeProjector);
+
+/* distanceDriven2D.cu:384 (cupy*) / :482 (c*): fan DD back projection,
+ * accumulates into img. */
+int cupyDistanceDrivenFanBackprojection(float* img, const float* prj, const float* deg, size_t nBatches, size_t nx,
+                                        size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy,
+                                        float cz, size_t nu, size_t nv, size_t nview, float da, float dv,
+                                        float off_a, float off_v, float dsd, float dso, int typeProjector);
+int cDistanceDrivenFanBackprojection(float* img, const float* prj, const float* deg, size_t nBatches, size_t nx,
+                                     size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                                     size_t nu, size_t nv, size_t nview, float da, float dv, float off_a,
+                                     float off_v, float dsd, float dso, int typeProjector);
+
+/* distanceDriven2D.cu:434 (cupy*) / :560 (c*): parallel DD back projection,
+ * accumulates into img. */
+int cupyDistanceDrivenParallelBackprojection(float* img, const float* prj, const float* deg, size_t nBatches,
+                                             size_t nx, size_t ny, size_t nz, float dx, float dy, float dz,
+                                             float cx, float cy, float cz, size_t nu, size_t nv, size_t nview,
+                                             float du, float dv, float off_u, float off_v, int typeProjector);
+int cDistanceDrivenParallelBackprojection(float* img, const float* prj, const float* deg, size_t nBatches,
+                                          size_t nx, size_t ny, size_t nz, float dx, float dy, float dz, float cx,
+                                          float cy, float cz, size_t nu, size_t nv, size_t nview, float du, float dv,
+                                          float off_u, float off_v, int typeProjector);
+
+/* distanceDriven3D.cu:184 (c*) / :264 (cupy*): tomosynthesis DD forward
+ * projection (detector u=(1,0,0), v=(0,1,0)), overwrites prj.  detCenter and
+ * src are [nview][3].  typeProjector 1 (branchless) selects the same
+ * operator. */
+int cupyDistanceDrivenTomoProjection(float* prj, const float* img, const float* detCenter, const float* src,
+                                     size_t nBatches, size_t nx, size_t ny, size_t nz, float dx, float dy, float dz,
+                                     float cx, float cy, float cz, size_t nu, size_t nv, size_t nview, float du,
+                                     float dv, float off_u, float off_v, int typeProjector);
+int cDistanceDrivenTomoProjection(float* prj, const float* img, const float* detCenter, const float* src,
+                                  size_t nBatches, size_t nx, size_t ny, size_t nz, float dx, float dy, float dz,
+                                  float cx, float cy, float cz, size_t nu, size_t nv, size_t nview, float du,
+                                  float dv, float off_u, float off_v, int typeProjector);
+
+/* distanceDriven3D.cu:312 (c*) / :393 (cupy*): tomosynthesis DD back
+ * projection, overwrites img. */
+int cupyDistanceDrivenTomoBackprojection(float* img, const float* prj, const float* detCenter, const float* src,
+                                         size_t nBatches, size_t nx, size_t ny, size_t nz, float dx, float dy,
+                                         float dz, float cx, float cy, float cz, size_t nu, size_t nv, size_t nview,
+                                         float du, float dv, float off_u, float off_v, int typeProjector);
+int cDistanceDrivenTomoBackprojection(float* img, const float* prj, const float* detCenter, const float* src,
+                                      size_t nBatches, size_t nx, size_t ny, size_t nz, float dx, float dy, float dz,
+                                      float cx, float cy, float cz, size_t nu, size_t nv, size_t nview, float du,
+                                      float dv, float off_u, float off_v, int typeProjector);
+
+/* siddonCone.cu:137 (c*) / :233 (cupy*): Siddon cone-beam forward projection
+ * for arbitrary trajectories; accumulates into prj. */
+int cupySiddonConeProjectionArbitrary(float* prj, const float* img, const float* detCenter, const float* detU,
+                                      const float* detV, const float* src, size_t nBatches, size_t nx, size_t ny,
+                                      size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu,
+                                      size_t nv, size_t nview, float du, float dv, float off_u, float off_v);
+int cSiddonConeProjectionArbitrary(float* prj, const float* img, const float* detCenter, const float* detU,
+                                   const float* detV, const float* src, size_t nBatches, size_t nx, size_t ny,
+                                   size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu,
+                                   size_t nv, size_t nview, float du, float dv, float off_u, float off_v);
+
+/* siddonCone.cu:282 (c*) / :378 (cupy*): Siddon cone-beam back projection
+ * (transpose, same segment lengths); accumulates into img. */
+int cupySiddonConeBackprojectionArbitrary(float* img, const float* prj, const float* detCenter, const float* detU,
+                                          const float* detV, const float* src, size_t nBatches, size_t nx,
+                                          size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy,
+                                          float cz, size_t nu, size_t nv, size_t nview, float du, float dv,
+                                          float off_u, float off_v);
+int cSiddonConeBackprojectionArbitrary(float* img, const float* prj, const float* detCenter, const float* detU,
+                                       const float* detV, const float* src, size_t nBatches, size_t nx, size_t ny,
+                                       size_t nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                                       size_t nu, size_t nv, size_t nview, float du, float dv, float off_u,
+                                       float off_v);
+
+/* fbp.cu:165 (cupy*) / :204 (c*): equiangular fan ramp filter; typeFilter
+ * 1 hamming, 2 hann, 3 cosine, else Ram-Lak.  Overwrites pFPrj. */
+int cupyfbpFanFilter(float* pFPrj, const float* pPrj, int nBatches, size_t nu, size_t nv, size_t nview, float da,
+                     float dv, float off_a, float off_v, float dsd, float dso, int typeFilter);
+int cfbpFanFilter(float* pFPrj, const float* pPrj, int nBatches, size_t nu, size_t nv, size_t nview, float da,
+                  float dv, float off_a, float off_v, float dsd, float dso, int typeFilter);
+
+/* fbpParallel.cu:111 (cupy*) / :146 (c*): parallel-beam ramp filter. */
+int cupyfbpParallelFilter(float* pFPrj, const float* pPrj, int nBatches, size_t nu, size_t nv, size_t nview,
+                          float du, float dv, float off_u, float off_v, int typeFilter);
+int cfbpParallelFilter(float* pFPrj, const float* pPrj, int nBatches, size_t nu, size_t nv, size_t nview, float du,
+                       float dv, float off_u, float off_v, int typeFilter);
+
+/* fbp.cu:362 (cupy*) / :409 (c*): pixel-driven fan FBP back projection,
+ * accumulates into pImg. */
+int cupyfbpFanBackprojection(float* pImg, const float* pPrj, const float* pDeg, size_t nBatches, size_t nx,
+                             size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                             size_t nu, size_t nv, size_t nview, float da, float dv, float off_a, float off_v,
+                             float dsd, float dso);
+int cfbpFanBackprojection(float* pImg, const float* pPrj, const float* pDeg, size_t nBatches, size_t nx, size_t ny,
+                          size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu,
+                          size_t nv, size_t nview, float da, float dv, float off_a, float off_v, float dsd,
+                          float dso);
+
+/* ======================================================================== */
+/* 2. Extended entries: explicit stream, workspace and flags                */
+/* ======================================================================== */
+/* geom 0 = fan (g->du is the angular cell size), 1 = parallel.
+ * Replaces the cupyDistanceDriven{Fan,Parallel}Projection path
+ * (distanceDriven2D.cu:109-200).  Default: overwrite prj. */
+int ctp_dd2d_fp(void* prj, const void* img, const float* deg, const ctp_geometry* g, int geom, int typeProjector,
+                unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
+size_t ctp_dd2d_fp_workspace(const ctp_geometry* g, int geom, int typeProjector, unsigned flags);
+
+/* DD back projection (distanceDriven2D.cu:384-478).  Default: img += BP(prj)
+ * in the reference's normalised form; CTP_FLAG_ADJOINT gives the exact
+ * transpose of ctp_dd2d_fp. */
+int ctp_dd2d_bp(void* img, const void* prj, const float* deg, const ctp_geometry* g, int geom, int typeProjector,
+                unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
+size_t ctp_dd2d_bp_workspace(const ctp_geometry* g, int geom, int typeProjector, unsigned flags);
+
+/* Number of operator nonzeros of the DD forward projector for one batch
+ * item (the pixel count of every ray footprint on every main-axis line). */
+int ctp_dd2d_nnz(unsigned long long* nnz_host, const float* deg, const ctp_geometry* g, int geom, void* stream);
+
+/* Ramp filter (fbp.cu:15-162 fan, fbpParallel.cu:14-109 parallel); overwrites
+ * fprj.  geom 0 = fan (g->du angular), 1 = parallel. */
+int ctp_ramp_filter(float* fprj, const float* prj, const ctp_geometry* g, int geom, int typeFilter, unsigned flags,
+                    void* workspace, size_t workspace_bytes, void* stream);
+size_t ctp_ramp_filter_workspace(const ctp_geometry* g, int geom, int typeFilter);
+
+/* Pixel-driven fan FBP back projection (fbp.cu:265-359); img += BP. */
+int ctp_fbp_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,
+                   void* stream);
+
+/* Siddon cone-beam projector pair (siddonCone.cu:12-135). */
+int ctp_siddon_fp(void* prj, const void* img, const float* detCenter, const float* detU, const float* detV,
+                  const float* src, const ctp_geometry* g, unsigned flags, void* stream);
+int ctp_siddon_bp(void* img, const void* prj, const float* detCenter, const float* detU, const float* detV,
+                  const float* src, const ctp_geometry* g, unsigned flags, void* stream);
+int ctp_siddon_nnz(unsigned long long* nnz_host, const float* detCenter, const float* detU, const float* detV,
+                   const float* src, const ctp_geometry* g, void* stream);
+
+/* Tomosynthesis DD projector pair (distanceDriven3DBoxInt.cu:28-280). */
+int ctp_tomo_fp(float* prj, const float* img, const float* detCenter, const float* src, const ctp_geometry* g,
+                unsigned flags, void* stream);
+int ctp_tomo_bp(float* img, const float* prj, const float* detCenter, const float* src, const ctp_geometry* g,
+                unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
+size_t ctp_tomo_bp_workspace(const ctp_geometry* g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* CTP_H */

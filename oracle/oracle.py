@@ -1,0 +1,283 @@
+"""CPU FP64 oracle for the CTProjector projector pair.
+
+TEST INFRASTRUCTURE ONLY.  The parity tests, ``__graft_entry__.smoke()`` and
+the ``cpu_baseline`` leg of ``bench.py`` use this module as the checker; the
+``ctprojector_b200`` product never imports it.
+
+The distance-driven, Siddon, tomosynthesis and ``fbp_bp`` operators are the C
+restatement in ``ctp_oracle.c`` (FP64, OpenMP).  The ramp filter is restated
+here in numpy float64, following ``fbpMath.cu:90-267`` (``GetRamp``),
+``fbpParallel.cu:14-109`` and ``fbp.cu:15-162`` of the reference
+(src/ct_projector/kernel/projector/cuda/).
+
+Every function takes the same ``projector`` object the reference Python
+wrappers take (attributes nx, ny, nz, dx, ..., du, dv, off_u, off_v, dsd, dso)
+and follows the argument conventions of the reference wrapper it names.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, Structure, c_double, c_float, c_int, c_long, c_longlong
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_SRC_PATH = os.path.join(_HERE, "ctp_oracle.c")
+
+
+def build(force: bool = False) -> str:
+    """Compile ctp_oracle.c into liboracle.so next to it (gcc, OpenMP)."""
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(_SRC_PATH):
+        cmd = ["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-std=c11", _SRC_PATH, "-o", _LIB_PATH, "-lm"]
+        subprocess.run(cmd, check=True)
+    return _LIB_PATH
+
+
+class _Grid(Structure):
+    _fields_ = [("nx", c_long), ("ny", c_long), ("nz", c_long),
+                ("dx", c_double), ("dy", c_double), ("dz", c_double),
+                ("cx", c_double), ("cy", c_double), ("cz", c_double)]
+
+
+class _Det(Structure):
+    _fields_ = [("nu", c_long), ("nv", c_long),
+                ("du", c_double), ("dv", c_double), ("off_u", c_double), ("off_v", c_double)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        dp = POINTER(c_double)
+        fp = POINTER(c_float)
+        L.oracle_dd2d_fp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int]
+        L.oracle_dd2d_bp_adjoint.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int]
+        L.oracle_dd2d_nnz.argtypes = [dp, _Grid, _Det, c_long, c_double, c_double, c_int]
+        L.oracle_dd2d_nnz.restype = c_longlong
+        L.oracle_dd2d_bp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int, c_int]
+        L.oracle_fbp_fan_bp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double]
+        L.oracle_siddon_fp.argtypes = [dp, dp, fp, fp, fp, fp, c_long, _Grid, _Det, c_long]
+        L.oracle_siddon_bp.argtypes = [dp, dp, fp, fp, fp, fp, c_long, _Grid, _Det, c_long]
+        L.oracle_siddon_nnz.argtypes = [fp, fp, fp, fp, _Grid, _Det, c_long]
+        L.oracle_siddon_nnz.restype = c_longlong
+        L.oracle_tomo_fp.argtypes = [dp, dp, fp, fp, c_long, _Grid, _Det, c_long]
+        L.oracle_tomo_bp.argtypes = [dp, dp, fp, fp, c_long, _Grid, _Det, c_long]
+        L.oracle_num_threads.restype = c_int
+        _lib = L
+    return _lib
+
+
+def num_threads() -> int:
+    return int(lib().oracle_num_threads())
+
+
+def _grid(p, shape=None):
+    nz, ny, nx = (shape if shape is not None else (p.nz, p.ny, p.nx))
+    return _Grid(int(nx), int(ny), int(nz), float(np.float32(p.dx)), float(np.float32(p.dy)),
+                 float(np.float32(p.dz)), float(np.float32(p.cx)), float(np.float32(p.cy)),
+                 float(np.float32(p.cz)))
+
+
+def _det(p, nu, nv, du=None):
+    du = p.du if du is None else du
+    return _Det(int(nu), int(nv), float(np.float32(du)), float(np.float32(p.dv)),
+                float(np.float32(p.off_u)), float(np.float32(p.off_v)))
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f3(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr(a, t=c_double):
+    return a.ctypes.data_as(POINTER(t))
+
+
+def _fan_da(p):
+    # The reference wrappers pass the angular cell size du / dsd in float32.
+    return float(np.float32(np.float32(p.du) / np.float32(p.dsd)))
+
+
+# --------------------------------------------------------------------------- DD 2D
+def dd_fp(p, img, angles, geom: str):
+    """Fan (geom='fan') or parallel DD forward projection.  Mirrors
+    fan_equiangular.distance_driven_fp / parallel.distance_driven_fp."""
+    img = _d(img)
+    ang = _d(angles)
+    nb = img.shape[0]
+    prj = np.zeros([nb, len(ang), int(p.nv), int(p.nu)], np.float64)
+    g = _grid(p, img.shape[1:])
+    if geom == "fan":
+        d = _det(p, p.nu, p.nv, _fan_da(p))
+        lib().oracle_dd2d_fp(_ptr(prj), _ptr(img), _ptr(ang), nb, g, d, len(ang), float(np.float32(p.dsd)),
+                             float(np.float32(p.dso)), 0)
+    else:
+        d = _det(p, p.nu, p.nv)
+        lib().oracle_dd2d_fp(_ptr(prj), _ptr(img), _ptr(ang), nb, g, d, len(ang), 1000.0, 500.0, 1)
+    return prj
+
+
+def dd_bp(p, prj, angles, geom: str, is_fbp=False, adjoint=False):
+    """DD back projection: reference-parity normalised mode, FBP mode, or the
+    exact transpose of dd_fp (adjoint=True)."""
+    prj = _d(prj)
+    ang = _d(angles)
+    nb, nview, nv, nu = prj.shape
+    img = np.zeros([nb, int(p.nz), int(p.ny), int(p.nx)], np.float64)
+    g = _grid(p)
+    if geom == "fan":
+        d = _det(p, nu, nv, _fan_da(p))
+        dsd, dso, gi = float(np.float32(p.dsd)), float(np.float32(p.dso)), 0
+    else:
+        d = _det(p, nu, nv)
+        dsd, dso, gi = 1000.0, 500.0, 1
+    if adjoint:
+        lib().oracle_dd2d_bp_adjoint(_ptr(img), _ptr(prj), _ptr(ang), nb, g, d, nview, dsd, dso, gi)
+    else:
+        lib().oracle_dd2d_bp(_ptr(img), _ptr(prj), _ptr(ang), nb, g, d, nview, dsd, dso, gi, int(bool(is_fbp)))
+    return img
+
+
+def dd_nnz(p, angles, geom: str, shape=None) -> int:
+    ang = _d(angles)
+    g = _grid(p, shape)
+    if geom == "fan":
+        return int(lib().oracle_dd2d_nnz(_ptr(ang), g, _det(p, p.nu, p.nv, _fan_da(p)), len(ang),
+                                         float(np.float32(p.dsd)), float(np.float32(p.dso)), 0))
+    return int(lib().oracle_dd2d_nnz(_ptr(ang), g, _det(p, p.nu, p.nv), len(ang), 1000.0, 500.0, 1))
+
+
+def fbp_bp(p, prj, angles):
+    """Pixel-driven fan FBP back projection (fan_equiangular.fbp_bp)."""
+    prj = _d(prj)
+    ang = _d(angles)
+    nb, nview, nv, nu = prj.shape
+    img = np.zeros([nb, int(p.nz), int(p.ny), int(p.nx)], np.float64)
+    lib().oracle_fbp_fan_bp(_ptr(img), _ptr(prj), _ptr(ang), nb, _grid(p), _det(p, nu, nv, _fan_da(p)), nview,
+                            float(np.float32(p.dsd)), float(np.float32(p.dso)))
+    return img
+
+
+# --------------------------------------------------------------------------- Siddon cone
+def siddon_fp(p, img, det_center, det_u, det_v, src):
+    """cone.siddon_fp_arbitrary: geometry arrays [nview, 3] as (x, y, z)."""
+    img = _d(img)
+    dc, du_, dv_, sr = _f3(det_center), _f3(det_u), _f3(det_v), _f3(src)
+    nb = img.shape[0]
+    nview = dc.shape[0]
+    prj = np.zeros([nb, nview, int(p.nv), int(p.nu)], np.float64)
+    lib().oracle_siddon_fp(_ptr(prj), _ptr(img), _ptr(dc, c_float), _ptr(du_, c_float), _ptr(dv_, c_float),
+                           _ptr(sr, c_float), nb, _grid(p, img.shape[1:]), _det(p, p.nu, p.nv), nview)
+    return prj
+
+
+def siddon_bp(p, prj, det_center, det_u, det_v, src):
+    prj = _d(prj)
+    dc, du_, dv_, sr = _f3(det_center), _f3(det_u), _f3(det_v), _f3(src)
+    nb, nview, nv, nu = prj.shape
+    img = np.zeros([nb, int(p.nz), int(p.ny), int(p.nx)], np.float64)
+    lib().oracle_siddon_bp(_ptr(img), _ptr(prj), _ptr(dc, c_float), _ptr(du_, c_float), _ptr(dv_, c_float),
+                           _ptr(sr, c_float), nb, _grid(p), _det(p, nu, nv), nview)
+    return img
+
+
+def siddon_nnz(p, det_center, det_u, det_v, src, shape=None) -> int:
+    dc, du_, dv_, sr = _f3(det_center), _f3(det_u), _f3(det_v), _f3(src)
+    return int(lib().oracle_siddon_nnz(_ptr(dc, c_float), _ptr(du_, c_float), _ptr(dv_, c_float),
+                                       _ptr(sr, c_float), _grid(p, shape), _det(p, p.nu, p.nv), dc.shape[0]))
+
+
+# --------------------------------------------------------------------------- tomo
+def tomo_fp(p, img, det_center, src):
+    img = _d(img)
+    dc, sr = _f3(det_center), _f3(src)
+    nb = img.shape[0]
+    prj = np.zeros([nb, dc.shape[0], int(p.nv), int(p.nu)], np.float64)
+    lib().oracle_tomo_fp(_ptr(prj), _ptr(img), _ptr(dc, c_float), _ptr(sr, c_float), nb, _grid(p, img.shape[1:]),
+                         _det(p, p.nu, p.nv), dc.shape[0])
+    return prj
+
+
+def tomo_bp(p, prj, det_center, src):
+    prj = _d(prj)
+    dc, sr = _f3(det_center), _f3(src)
+    nb, nview, nv, nu = prj.shape
+    img = np.zeros([nb, int(p.nz), int(p.ny), int(p.nx)], np.float64)
+    lib().oracle_tomo_bp(_ptr(img), _ptr(prj), _ptr(dc, c_float), _ptr(sr, c_float), nb, _grid(p),
+                         _det(p, nu, nv), nview)
+    return img
+
+
+# --------------------------------------------------------------------------- ramp filter
+FILTERS = {"hamming": 1, "hann": 2, "cosine": 3}
+
+
+def filter_code(filter_type: str) -> int:
+    """fan_equiangular.ramp_filter / parallel.ramp_filter: unknown names are RL (0)."""
+    return FILTERS.get(filter_type.lower(), 0)
+
+
+def ramp_kernel(nu: int, da: float, ifilter: int, equiangular: bool) -> np.ndarray:
+    """Windowed spatial ramp of length 2nu-1, index i <-> offset i-(nu-1).
+
+    GetRamp, fbpMath.cu:90-241: spatial ramp, FFT, window, inverse FFT, real
+    part divided by the length."""
+    L = 2 * nu - 1
+    k = np.arange(L) - (nu - 1)
+    h = np.zeros(L)
+    h[k == 0] = 1.0 / (4 * da * da)
+    odd = (k % 2) != 0
+    if equiangular:
+        h[odd] = -1.0 / (np.pi ** 2 * np.sin(k[odd] * da) ** 2)
+    else:
+        h[odd] = -1.0 / (np.pi ** 2 * k[odd].astype(np.float64) ** 2 * da * da)
+    i = np.arange(L)
+    if ifilter == 1:
+        w = 0.54 + 0.46 * np.cos(2 * np.pi * i / L)
+    elif ifilter == 2:
+        w = 0.5 + 0.5 * np.cos(2 * np.pi * i / L)
+    elif ifilter == 3:
+        w = np.abs(np.cos(np.pi * i / L))
+    else:
+        w = np.ones(L)
+    return np.real(np.fft.ifft(np.fft.fft(h) * w))
+
+
+def ramp_filter(p, prj, filter_type: str = "hann", geom: str = "parallel"):
+    """parallel.ramp_filter / fan_equiangular.ramp_filter.
+
+    Each detector row is zero padded, convolved with the windowed ramp and
+    cropped: out[i] = scale * sum_j p[j] g[i - j + nu - 1]
+    (fbpParallel.cu:56-86, fbp.cu:50-134).  Fan rows are pre-weighted by
+    cos(((i - (nu-1)/2) - off_u) da) (fbp.cu:60-67)."""
+    prj = _d(prj)
+    nb, nview, nv, nu = prj.shape
+    ifilter = filter_code(filter_type)
+    if geom == "fan":
+        da = _fan_da(p)
+        g = ramp_kernel(nu, da, ifilter, equiangular=True)
+        wgt = np.cos(((np.arange(nu) - (nu - 1) / 2.0) - float(np.float32(p.off_u))) * da)
+        x = prj * wgt
+        scale = np.pi / nview * da / float(np.float32(p.dso))
+    else:
+        du = float(np.float32(p.du))
+        g = ramp_kernel(nu, du, ifilter, equiangular=False)
+        x = prj
+        scale = np.pi / nview * du
+    n = 1
+    while n < 3 * nu - 2:
+        n *= 2
+    X = np.fft.rfft(x, n=n, axis=-1)
+    G = np.fft.rfft(g, n=n)
+    full = np.fft.irfft(X * G, n=n, axis=-1)
+    return full[..., nu - 1: 2 * nu - 1] * scale

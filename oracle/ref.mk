@@ -1,0 +1,38 @@
+# Builds the reference projector library (wudufan/CTProjector, kernel/projector/cuda)
+# from its own sources, for sm_100a, into oracle/_ref/libprojector.so.
+#
+# This is test infrastructure: the library is the GPU oracle that produces the
+# golden fixtures under tests/golden/ and the timed reference arm of bench.py.
+# It is never linked into, or called by, the ctprojector_b200 product path.
+#
+#   make -f oracle/ref.mk REF=/root/reference        (run from the repo root)
+#
+# The sources are read where they lie; nothing is copied into this repository.
+
+REF     ?= /root/reference
+SRC_DIR := $(REF)/src/ct_projector/kernel/projector/cuda
+OUT     := oracle/_ref
+OBJ_DIR := $(OUT)/obj
+NVCC    ?= nvcc
+ARCH    := -gencode arch=compute_100a,code=sm_100a
+
+SOURCES := $(wildcard $(SRC_DIR)/*.cu)
+OBJECTS := $(patsubst $(SRC_DIR)/%.cu,$(OBJ_DIR)/%.o,$(SOURCES))
+
+.PHONY: all clean
+
+all: $(OUT)/libprojector.so
+
+$(OUT)/libprojector.so: $(OBJECTS)
+	$(NVCC) --shared $(ARCH) $(OBJECTS) -lcufft -o $@
+
+# The reference defines device helpers in one translation unit and calls them
+# from another, so it needs relocatable device code (-dc) and a device link.
+$(OBJ_DIR)/%.o: $(SRC_DIR)/%.cu | $(OBJ_DIR)
+	$(NVCC) -O3 $(ARCH) -I$(SRC_DIR)/.. -dc --compiler-options '-fPIC' -w $< -o $@
+
+$(OBJ_DIR):
+	mkdir -p $(OBJ_DIR)
+
+clean:
+	rm -rf $(OUT)

@@ -1,0 +1,177 @@
+"""Generate the golden fixtures tests/golden/*.npz from the reference itself.
+
+Runs the reference projector library -- oracle/_ref/libprojector.so, built
+from the reference sources for sm_100a by ``make -f oracle/ref.mk`` -- through
+its host-pointer C entries with the argument conventions of its numpy
+wrappers (ct_projector/projector/numpy/*.py), on the seeded cases of
+cases.py, and stores inputs and outputs.  Needs a GPU:
+
+    python tests/golden/make_golden.py --out gpurun_out/golden
+
+This script is test infrastructure; the product never runs the reference.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import os
+import sys
+from ctypes import c_float, c_int, c_ulong, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+import cases  # noqa: E402
+
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libprojector.so")
+
+
+def ptr(a):
+    return c_void_p(a.ctypes.data)
+
+
+def geom(p, nb, img_shape, prj_shape):
+    nz, ny, nx = img_shape
+    nview, nv, nu = prj_shape
+    return [c_ulong(nb), c_ulong(nx), c_ulong(ny), c_ulong(nz), c_float(p.dx), c_float(p.dy), c_float(p.dz),
+            c_float(p.cx), c_float(p.cy), c_float(p.cz), c_ulong(nu), c_ulong(nv), c_ulong(nview)]
+
+
+class Ref:
+    def __init__(self, path):
+        self.L = ctypes.CDLL(path)
+
+    def call(self, name, *args):
+        f = getattr(self.L, name)
+        f.restype = c_int
+        rc = f(*args)
+        if rc != 0:
+            raise RuntimeError(f"{name} returned {rc}")
+
+    # fan_equiangluar.py:241-299
+    def dd_fp(self, p, img, ang, fan, type_=0):
+        prj = np.zeros([img.shape[0], len(ang), p.nv, p.nu], np.float32)
+        if fan:
+            self.call("cDistanceDrivenFanProjection", ptr(prj), ptr(img), ptr(ang),
+                      *geom(p, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du / p.dsd), c_float(p.dv),
+                      c_float(p.off_u), c_float(p.off_v), c_float(p.dsd), c_float(p.dso), c_int(type_))
+        else:
+            self.call("cDistanceDrivenParallelProjection", ptr(prj), ptr(img), ptr(ang),
+                      *geom(p, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv),
+                      c_float(p.off_u), c_float(p.off_v), c_int(type_))
+        return prj
+
+    # fan_equiangluar.py:302-366, parallel.py:192-254
+    def dd_bp(self, p, prj, ang, fan, type_=0):
+        img = np.zeros([prj.shape[0], p.nz, p.ny, p.nx], np.float32)
+        if fan:
+            self.call("cDistanceDrivenFanBackprojection", ptr(img), ptr(prj), ptr(ang),
+                      *geom(p, prj.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du / p.dsd), c_float(p.dv),
+                      c_float(p.off_u), c_float(p.off_v), c_float(p.dsd), c_float(p.dso), c_int(type_))
+        else:
+            self.call("cDistanceDrivenParallelBackprojection", ptr(img), ptr(prj), ptr(ang),
+                      *geom(p, prj.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv),
+                      c_float(p.off_u), c_float(p.off_v), c_int(type_))
+        return img
+
+    # fan_equiangluar.py:19-67, parallel.py:20-71
+    def ramp(self, p, prj, fan, ifilter):
+        out = np.zeros(prj.shape, np.float32)
+        nb, nview, nv, nu = prj.shape
+        if fan:
+            self.call("cfbpFanFilter", ptr(out), ptr(prj), c_int(nb), c_ulong(nu), c_ulong(nv), c_ulong(nview),
+                      c_float(p.du / p.dsd), c_float(p.dv), c_float(p.off_u), c_float(p.off_v), c_float(p.dsd),
+                      c_float(p.dso), c_int(ifilter))
+        else:
+            self.call("cfbpParallelFilter", ptr(out), ptr(prj), c_int(nb), c_ulong(nu), c_ulong(nv), c_ulong(nview),
+                      c_float(p.du), c_float(p.dv), c_float(p.off_u), c_float(p.off_v), c_int(ifilter))
+        return out
+
+    # fan_equiangluar.py:75-123
+    def fbp_bp(self, p, prj, ang):
+        img = np.zeros([prj.shape[0], p.nz, p.ny, p.nx], np.float32)
+        self.call("cfbpFanBackprojection", ptr(img), ptr(prj), ptr(ang),
+                  *geom(p, prj.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du / p.dsd), c_float(p.dv),
+                  c_float(p.off_u), c_float(p.off_v), c_float(p.dsd), c_float(p.dso))
+        return img
+
+    # cone.py:19-93
+    def siddon_fp(self, p, img, dc, du, dv, src):
+        prj = np.zeros([img.shape[0], dc.shape[0], p.nv, p.nu], np.float32)
+        self.call("cSiddonConeProjectionArbitrary", ptr(prj), ptr(img), ptr(dc), ptr(du), ptr(dv), ptr(src),
+                  *geom(p, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv),
+                  c_float(p.off_u), c_float(p.off_v))
+        return prj
+
+    def siddon_bp(self, p, prj, dc, du, dv, src):
+        img = np.zeros([prj.shape[0], p.nz, p.ny, p.nx], np.float32)
+        self.call("cSiddonConeBackprojectionArbitrary", ptr(img), ptr(prj), ptr(dc), ptr(du), ptr(dv), ptr(src),
+                  *geom(p, prj.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv),
+                  c_float(p.off_u), c_float(p.off_v))
+        return img
+
+    # tomo.py:19-164
+    def tomo_fp(self, p, img, dc, src):
+        prj = np.zeros([img.shape[0], dc.shape[0], p.nv, p.nu], np.float32)
+        self.call("cDistanceDrivenTomoProjection", ptr(prj), ptr(img), ptr(dc), ptr(src),
+                  *geom(p, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv),
+                  c_float(p.off_u), c_float(p.off_v), c_int(0))
+        return prj
+
+    def tomo_bp(self, p, prj, dc, src):
+        img = np.zeros([prj.shape[0], p.nz, p.ny, p.nx], np.float32)
+        self.call("cDistanceDrivenTomoBackprojection", ptr(img), ptr(prj), ptr(dc), ptr(src),
+                  *geom(p, prj.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv),
+                  c_float(p.off_u), c_float(p.off_v), c_int(0))
+        return img
+
+
+def run_case(ref: Ref, fn):
+    name, p, inp = fn()
+    out = {}
+    if name in ("fan_basic", "fan_offsets", "par_basic", "par_offsets"):
+        fan = name.startswith("fan")
+        img, ang = inp["img"], inp["angles"]
+        prj = ref.dd_fp(p, img, ang, fan)
+        out["fp"] = prj
+        out["bp"] = ref.dd_bp(p, prj, ang, fan, 0)
+        for fname, code in (("hann", 2), ("hamming", 1), ("cosine", 3), ("ramlak", 0)):
+            out[f"filter_{fname}"] = ref.ramp(p, prj, fan, code)
+        out["bp_fbp"] = ref.dd_bp(p, out["filter_hann"], ang, fan, 1)
+        if fan:
+            out["fbp_bp"] = ref.fbp_bp(p, out["filter_hann"], ang)
+    elif name == "kat":
+        out["fp"] = ref.dd_fp(p, inp["img"], inp["angles"], False)
+        out["bp_fbp"] = ref.dd_bp(p, inp["prj"], inp["angles"], False, 1)
+    elif name == "siddon":
+        a = (inp["det_center"], inp["det_u"], inp["det_v"], inp["src"])
+        prj = ref.siddon_fp(p, inp["img"], *a)
+        out["fp"] = prj
+        out["bp"] = ref.siddon_bp(p, prj, *a)
+    elif name == "tomo":
+        prj = ref.tomo_fp(p, inp["img"], inp["det_center"], inp["src"])
+        out["fp"] = prj
+        out["bp"] = ref.tomo_bp(p, prj, inp["det_center"], inp["src"])
+    geom_attrs = {f"geom_{k}": np.asarray(v) for k, v in p.as_dict().items()}
+    return name, {**{f"in_{k}": v for k, v in inp.items()}, **{f"ref_{k}": v for k, v in out.items()}, **geom_attrs}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    ref = Ref(REF_LIB)
+    for fn in cases.ALL:
+        name, arrays = run_case(ref, fn)
+        path = os.path.join(a.out, f"{name}.npz")
+        np.savez_compressed(path, **arrays)
+        print(f"wrote {path}: " + ", ".join(f"{k}{list(v.shape)}" for k, v in arrays.items() if k.startswith("ref_")))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,91 @@
+"""The C ABI: libctp.so loads and exports every entry point declared in
+include/ctp.h, the ctypes binding covers the same set, and argument checks
+answer without touching a GPU."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "ctp.h")
+
+
+def declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|size_t|const char\s*\*)\s+([A-Za-z_]\w*)\s*\(", src, flags=re.M)))
+
+
+def test_header_declares_reference_entries():
+    names = set(declared())
+    reference = {
+        "SetDevice", "cupyDistanceDrivenFanProjection", "cDistanceDrivenFanProjection",
+        "cupyDistanceDrivenParallelProjection", "cDistanceDrivenParallelProjection",
+        "cupyDistanceDrivenFanBackprojection", "cDistanceDrivenFanBackprojection",
+        "cupyDistanceDrivenParallelBackprojection", "cDistanceDrivenParallelBackprojection",
+        "cupyDistanceDrivenTomoProjection", "cDistanceDrivenTomoProjection",
+        "cupyDistanceDrivenTomoBackprojection", "cDistanceDrivenTomoBackprojection",
+        "cupySiddonConeProjectionArbitrary", "cSiddonConeProjectionArbitrary",
+        "cupySiddonConeBackprojectionArbitrary", "cSiddonConeBackprojectionArbitrary",
+        "cupyfbpFanFilter", "cfbpFanFilter", "cupyfbpParallelFilter", "cfbpParallelFilter",
+        "cupyfbpFanBackprojection", "cfbpFanBackprojection",
+    }
+    assert reference <= names
+
+
+def test_library_exports_every_declared_symbol():
+    from ctprojector_b200._lib import LIB_PATH
+
+    L = ctypes.CDLL(LIB_PATH)
+    missing = [n for n in declared() if not hasattr(L, n)]
+    assert not missing
+
+
+def test_binding_matches_header():
+    from ctprojector_b200._lib import declared_symbols
+
+    assert sorted(declared_symbols()) == declared()
+
+
+def test_version_and_error_string():
+    from ctprojector_b200._lib import last_error_string, lib
+
+    assert b"sm_100a" in lib().ctpVersion()
+    assert isinstance(last_error_string(), str)
+
+
+def test_null_geometry_is_rejected_on_host():
+    from ctprojector_b200._lib import CTP_ERR_INVALID_ARGUMENT, last_error_string, lib
+
+    rc = lib().ctp_dd2d_fp(None, None, None, None, 0, 0, 0, None, 0, None)
+    assert rc == CTP_ERR_INVALID_ARGUMENT
+    assert "geometry" in last_error_string()
+
+
+def test_zero_extent_is_rejected_on_host():
+    from ctprojector_b200._lib import CTP_ERR_INVALID_ARGUMENT, Geometry, lib
+
+    g = Geometry(1, 0, 4, 1, 1, 1, 1, 0, 0, 0, 8, 1, 4, 1, 1, 0, 0, 1000, 500)
+    assert lib().ctp_dd2d_fp(1, 1, 1, ctypes.byref(g), 1, 0, 0, None, 0, None) == CTP_ERR_INVALID_ARGUMENT
+
+
+def test_workspace_queries_need_no_gpu():
+    from ctprojector_b200._lib import Geometry, lib
+
+    g = Geometry(16, 512, 512, 1, 0.8, 0.8, 1, 0, 0, 0, 768, 1, 720, 0.8, 1, 0, 0, 1000, 500)
+    fp = lib().ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0)
+    assert fp >= 16 * 512 * 512 * 4
+    assert lib().ctp_dd2d_bp_workspace(ctypes.byref(g), 1, 0, 0) == 0
+    assert lib().ctp_tomo_bp_workspace(ctypes.byref(g)) >= 16 * 720 * 768 * 4
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    import ctprojector_b200._lib as L
+    from ctprojector_b200.errors import CTProjectorError
+
+    monkeypatch.setattr(L, "_lib", None)
+    monkeypatch.setattr(L, "LIB_PATH", str(tmp_path / "libctp.so"))
+    with pytest.raises(CTProjectorError):
+        L.lib()
