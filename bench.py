@@ -1,0 +1,425 @@
+"""Benchmark of the projector pair on the parallel-beam FBP/SQS workload.
+
+Workload (one step): parallel-beam distance-driven forward projection, the
+normalised back projection, the Hann ramp filter and the FBP-weighted back
+projection of a batch of 16 slices of 512 x 512 pixels at 0.8 mm, 720 views
+over pi, 768 detector cells of 0.8 mm (seeded synthetic ellipse phantoms).
+
+Metric: FP+BP GB/s against the HBM roofline -- the algorithmic bytes of the
+step (per projector: one operand fetch per operator nonzero plus compulsory
+input and output; the filter: its input and output) divided by the step time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank processes its own batch (weak scaling, no
+collective on the data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = ("parallel-beam DD FP + BP + ramp_filter(hann) + FBP BP, 16 x 512 x 512 at 0.8 mm, 720 views over pi, "
+            "768 cells of 0.8 mm")
+METRIC = "FP+BP GB/s vs HBM roofline"
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 512 << 20
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- workload
+def workload_inputs(seed_index: int = 0):
+    from ctprojector_b200 import synthetic as S
+
+    scan, ang, nb = S.config2()
+    rng = np.random.default_rng(S.seed_for(2, seed_index))
+    img = np.stack([S.ellipse_phantom(rng, scan.nx, scan.ny, scan.dx, scan.dy)[None] for _ in range(nb)])
+    return scan, ang, img.astype(np.float32)
+
+
+def algorithmic_bytes(nnz_slice: int, nb: int, scan) -> dict:
+    n_img = nb * scan.nz * scan.ny * scan.nx
+    n_prj = nb * scan.nview * scan.nv * scan.nu
+    proj = 4 * (nnz_slice * nb + n_img + n_prj)
+    return {"fp": proj, "bp": proj, "filter": 4 * 2 * n_prj, "bp_fbp": proj}
+
+
+# ours: launches of our own kernels per step (FP: table, transpose, sweep;
+# BP: gather; filter: pad, spectrum multiply, crop; FBP BP: gather)
+OUR_LAUNCHES_PER_STEP = 3 + 1 + 3 + 1
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from ctprojector_b200.projector import _device as D
+    from ctprojector_b200.projector.cupy import parallel as P
+    from ctprojector_b200.projector.cupy.ct_projector import ct_projector
+    from ctprojector_b200.projector.numpy import parallel as NP
+    from ctprojector_b200.projector.numpy.ct_projector import ct_projector as np_ct_projector
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    scan, ang, img = workload_inputs(rank)
+    nb = img.shape[0]
+    p = scan.projector(ct_projector)
+    timg = torch.tensor(img, device=dev)
+    tang = torch.tensor(ang, device=dev)
+    nnz = D.dd_nnz(p, tang, 1)
+    ab = algorithmic_bytes(nnz, nb, scan)
+    step_bytes = sum(ab.values())
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    ops = ["fp", "bp", "filter", "bp_fbp"]
+    ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for k in ops}
+
+    def step(record):
+        e = ev["fp"]
+        if record:
+            e[0].record()
+        prj = P.distance_driven_fp(p, timg, tang)
+        if record:
+            e[1].record()
+            ev["bp"][0].record()
+        bp = P.distance_driven_bp(p, prj, tang)
+        if record:
+            ev["bp"][1].record()
+            ev["filter"][0].record()
+        fprj = P.ramp_filter(p, prj, "hann")
+        if record:
+            ev["filter"][1].record()
+            ev["bp_fbp"][0].record()
+        rec = P.distance_driven_bp(p, fprj, tang, True)
+        if record:
+            ev["bp_fbp"][1].record()
+        return bp, rec
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    op_ms = {k: [] for k in ops}
+    step_ms = []
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if dist:
+            tdist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the step events)
+            s0.record()
+            step(True)
+            s1.record()
+            torch.cuda.synchronize()
+            step_ms.append(s0.elapsed_time(s1))
+            for k in ops:
+                op_ms[k].append(ev[k][0].elapsed_time(ev[k][1]))
+        torch.cuda.synchronize()
+        if dist:
+            tdist.barrier()
+    ms = float(np.mean(step_ms))
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * step_bytes / (ms * 1e-3) / 1e9
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peak()
+    op_avg = {k: float(np.mean(v)) for k, v in op_ms.items()}
+    proj_ops = ["fp", "bp", "bp_fbp"]
+    dom = max(proj_ops, key=lambda k: op_avg[k])
+    achieved = ab[dom] / (op_avg[dom] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(f"dd2d_{dom}_cfg2")
+
+    # end to end through the host-array API (numpy modules, c* entries)
+    pinned = torch.empty(img.shape, dtype=torch.float32, pin_memory=True)
+    pinned.copy_(torch.from_numpy(img))
+    himg = pinned.numpy()
+    pn = scan.projector(np_ct_projector)
+
+    def e2e_step():
+        prj = NP.distance_driven_fp(pn, himg, ang)
+        bp = NP.distance_driven_bp(pn, prj, ang)
+        fprj = NP.ramp_filter(pn, prj, "hann")
+        rec = NP.distance_driven_bp(pn, fprj, ang, True)
+        return prj, bp, fprj, rec
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if dist:
+        tdist.barrier()
+    e2e_ms = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = float(np.mean(e2e_ms))
+    if dist:
+        t = torch.tensor([e2e], device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e = float(t.item())
+    n_img, n_prj = img.size, nb * scan.nview * scan.nv * scan.nu
+    h2d = 4 * (n_img + n_prj + n_prj + n_prj) + 3 * 4 * len(ang)
+    d2h = 4 * (n_prj + n_img + n_prj + n_img)
+
+    cpu = cpu_baseline(scan, ang, img) if rank == 0 else None
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipse phantoms)",
+        "config": {"workload": WORKLOAD, "batch_per_gpu": nb, "nnz_per_slice": nnz,
+                   "algorithmic_bytes_per_step": step_bytes, "l2": "flushed between steps (512 MiB write)",
+                   "parallelism": f"replicas x{world}", "op_ms": {k: round(v, 4) for k, v in op_avg.items()}},
+        "roofline": {"bound": "hbm", "kernel": f"dd2d_{dom} (table + sweep launches)", "achieved": round(achieved, 2),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic,
+                     "compulsory_gbs": round((ab[dom] - 4 * nnz * nb) / (op_avg[dom] * 1e-3) / 1e9, 2)},
+        "e2e": {"value": round(world * step_bytes / (e2e * 1e-3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(e2e, 3),
+                "api": "ctprojector_b200.projector.numpy.parallel (host arrays, c* entries)",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "cpu_baseline": cpu,
+        "gpu_launches": OUR_LAUNCHES_PER_STEP * args.steps,
+        "clocks": clocks,
+    }
+    return line
+
+
+def cpu_baseline(scan, ang, img):
+    """The FP64 oracle (all host threads) on one slice of the batch: the same
+    four operators, scaled to GB/s with that slice's algorithmic bytes."""
+    from oracle import oracle as O
+
+    O.build()
+    sl = img[:1]
+    t0 = time.perf_counter()
+    prj = O.dd_fp(scan, sl, ang, "parallel")
+    O.dd_bp(scan, prj, ang, "parallel")
+    fprj = O.ramp_filter(scan, prj, "hann", "parallel")
+    O.dd_bp(scan, fprj, ang, "parallel", is_fbp=True)
+    dt = time.perf_counter() - t0
+    nnz = O.dd_nnz(scan, ang, "parallel")
+    b = sum(algorithmic_bytes(nnz, 1, scan).values())
+    return {"value": round(b / dt / 1e9, 4), "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
+            "seconds": round(dt, 2), "sample": "1 of the 16 slices: FP, BP, hann ramp filter, FBP BP (FP64 oracle)"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world, local):
+    """The reference library built from its own sources for sm_100a
+    (oracle/_ref/libprojector.so) through its host-pointer C entries, with the
+    argument conventions of its numpy wrappers, on the same workload."""
+    import ctypes
+    from ctypes import c_float, c_int, c_ulong, c_void_p
+
+    path = os.path.join(ROOT, "oracle", "_ref", "libprojector.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libprojector.so was not built from the reference "
+                "sources (needs the reference tree at build time)"}
+    L = ctypes.CDLL(path)
+    scan, ang, img = workload_inputs(0)
+    nb = img.shape[0]
+    p = scan
+
+    def g(nb_, prj_shape):
+        nview, nv, nu = prj_shape
+        return [c_ulong(nb_), c_ulong(p.nx), c_ulong(p.ny), c_ulong(p.nz), c_float(p.dx), c_float(p.dy),
+                c_float(p.dz), c_float(p.cx), c_float(p.cy), c_float(p.cz), c_ulong(nu), c_ulong(nv),
+                c_ulong(nview)]
+
+    P = lambda a: c_void_p(a.ctypes.data)  # noqa: E731
+    shape = (len(ang), p.nv, p.nu)
+
+    def fp(x):  # parallel.py:133-189
+        out = np.zeros([nb, *shape], np.float32)
+        rc = L.cDistanceDrivenParallelProjection(P(out), P(x), P(ang), *g(nb, shape), c_float(p.du), c_float(p.dv),
+                                                 c_float(p.off_u), c_float(p.off_v), c_int(0))
+        assert rc == 0, rc
+        return out
+
+    def bp(y, fbp):  # parallel.py:192-254
+        out = np.zeros([nb, p.nz, p.ny, p.nx], np.float32)
+        rc = L.cDistanceDrivenParallelBackprojection(P(out), P(y), P(ang), *g(nb, shape), c_float(p.du),
+                                                     c_float(p.dv), c_float(p.off_u), c_float(p.off_v),
+                                                     c_int(1 if fbp else 0))
+        assert rc == 0, rc
+        return out
+
+    def filt(y):  # parallel.py:20-71
+        out = np.zeros(y.shape, np.float32)
+        rc = L.cfbpParallelFilter(P(out), P(y), c_int(nb), c_ulong(p.nu), c_ulong(p.nv), c_ulong(len(ang)),
+                                  c_float(p.du), c_float(p.dv), c_float(p.off_u), c_float(p.off_v), c_int(2))
+        assert rc == 0, rc
+        return out
+
+    import torch
+
+    pinned = torch.empty(img.shape, dtype=torch.float32, pin_memory=True)
+    pinned.copy_(torch.from_numpy(img))
+    himg = pinned.numpy()
+
+    def step():
+        prj = fp(himg)
+        bp(prj, False)
+        fprj = filt(prj)
+        bp(fprj, True)
+
+    for _ in range(args.warmup):
+        step()
+    ts = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            step()
+            ts.append((time.perf_counter() - t0) * 1e3)
+    ms = float(np.mean(ts))
+    from ctprojector_b200.projector import _device as D
+    from ctprojector_b200.projector.cupy.ct_projector import ct_projector
+
+    nnz = D.dd_nnz(scan.projector(ct_projector), torch.tensor(ang, device="cuda"), 1)
+    step_bytes = sum(algorithmic_bytes(nnz, nb, scan).values())
+    value = step_bytes / (ms * 1e-3) / 1e9
+    n_prj = nb * len(ang) * p.nv * p.nu
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipse phantoms)",
+        "config": {"workload": WORKLOAD, "batch_per_gpu": nb, "nnz_per_slice": nnz,
+                   "algorithmic_bytes_per_step": step_bytes,
+                   "implementation": "reference libprojector.so built from its sources for sm_100a, "
+                                     "host-pointer c* entries as called by its numpy modules"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": 1, "kind": "reference",
+                         "sample": "full workload; the reference's only implementation of the path is its CUDA "
+                                   "library, driven from one host thread"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "copies_inside_reference_calls_bytes": 4 * (img.size + 3 * n_prj) + 4 * (2 * n_prj + 2 * img.size)},
+        "clocks": clk.summary(),
+    }
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args(argv)
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args, rank, world, local)), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+    try:
+        line = run_ours(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+
+            tdist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

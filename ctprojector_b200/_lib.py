@@ -29,6 +29,7 @@ FLAG_IN_BF16 = 0x10
 FLAG_IN_FP16 = 0x20
 FLAG_OUT_BF16 = 0x40
 FLAG_OUT_FP16 = 0x80
+FLAG_FILTER_EXACT = 0x100
 
 TYPE_FBP = 0x1
 TYPE_BRANCHLESS = 0x2
@@ -91,7 +92,7 @@ _SIGNATURES = {
     "ctp_dd2d_bp_workspace": [_GP, c_int, c_int, c_uint],
     "ctp_dd2d_nnz": [POINTER(c_ulonglong), _P, _GP, c_int, _P],
     "ctp_ramp_filter": [_P, _P, _GP, c_int, c_int, c_uint, _P, _S, _P],
-    "ctp_ramp_filter_workspace": [_GP, c_int, c_int],
+    "ctp_ramp_filter_workspace": [_GP, c_int, c_int, c_uint],
     "ctp_fbp_fan_bp": [_P, _P, _P, _GP, c_uint, _P],
     "ctp_siddon_fp": [_P, _P, _P, _P, _P, _P, _GP, c_uint, _P],
     "ctp_siddon_bp": [_P, _P, _P, _P, _P, _P, _GP, c_uint, _P],

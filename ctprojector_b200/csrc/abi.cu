@@ -18,7 +18,7 @@ int dd2d_bp(void*, const void*, const float*, const ctp_geometry&, int, int, uns
 size_t dd2d_bp_workspace(const ctp_geometry&, int, int, unsigned);
 int dd2d_nnz(unsigned long long*, const float*, const ctp_geometry&, int, cudaStream_t);
 int ramp_filter(float*, const float*, const ctp_geometry&, int, int, unsigned, void*, size_t, cudaStream_t);
-size_t ramp_filter_workspace(const ctp_geometry&, int, int);
+size_t ramp_filter_workspace(const ctp_geometry&, int, int, unsigned);
 int fbp_fan_bp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 int siddon_fp(void*, const void*, const float*, const float*, const float*, const float*, const ctp_geometry&,
               unsigned, cudaStream_t);
@@ -484,8 +484,8 @@ int ctp_dd2d_fp(void* prj, const void* img, const float* deg, const ctp_geometry
                 unsigned flags, void* workspace, size_t workspace_bytes, void* stream) {
     int rc = check_geometry(g, true, true);
     if (rc) return rc;
-    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     return dd2d_fp(prj, img, deg, *g, geom, typeProjector, flags, workspace, workspace_bytes, as_stream(stream));
 }
 
@@ -497,8 +497,8 @@ int ctp_dd2d_bp(void* img, const void* prj, const float* deg, const ctp_geometry
                 unsigned flags, void* workspace, size_t workspace_bytes, void* stream) {
     int rc = check_geometry(g, true, true);
     if (rc) return rc;
-    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     return dd2d_bp(img, prj, deg, *g, geom, typeProjector, flags, workspace, workspace_bytes, as_stream(stream));
 }
 
@@ -517,21 +517,21 @@ int ctp_ramp_filter(float* fprj, const float* prj, const ctp_geometry* g, int ge
                     void* workspace, size_t workspace_bytes, void* stream) {
     int rc = check_geometry(g, false, true);
     if (rc) return rc;
-    if (!fprj || !prj) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g->nbatch == 0) return CTP_OK;
+    if (!fprj || !prj) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     return ramp_filter(fprj, prj, *g, geom, typeFilter, flags, workspace, workspace_bytes, as_stream(stream));
 }
 
-size_t ctp_ramp_filter_workspace(const ctp_geometry* g, int geom, int typeFilter) {
-    return g ? ramp_filter_workspace(*g, geom, typeFilter) : 0;
+size_t ctp_ramp_filter_workspace(const ctp_geometry* g, int geom, int typeFilter, unsigned flags) {
+    return g ? ramp_filter_workspace(*g, geom, typeFilter, flags) : 0;
 }
 
 int ctp_fbp_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,
                    void* stream) {
     int rc = check_geometry(g, true, true);
     if (rc) return rc;
-    if (!img || !prj || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g->nbatch == 0) return CTP_OK;
+    if (!img || !prj || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     return fbp_fan_bp(img, prj, deg, *g, flags, as_stream(stream));
 }
 
@@ -539,9 +539,9 @@ int ctp_siddon_fp(void* prj, const void* img, const float* detCenter, const floa
                   const float* src, const ctp_geometry* g, unsigned flags, void* stream) {
     int rc = check_geometry(g, true, true);
     if (rc) return rc;
+    if (g->nbatch == 0) return CTP_OK;
     if (!prj || !img || !detCenter || !detU || !detV || !src)
         return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
-    if (g->nbatch == 0) return CTP_OK;
     return siddon_fp(prj, img, detCenter, detU, detV, src, *g, flags, as_stream(stream));
 }
 
@@ -549,9 +549,9 @@ int ctp_siddon_bp(void* img, const void* prj, const float* detCenter, const floa
                   const float* src, const ctp_geometry* g, unsigned flags, void* stream) {
     int rc = check_geometry(g, true, true);
     if (rc) return rc;
+    if (g->nbatch == 0) return CTP_OK;
     if (!prj || !img || !detCenter || !detU || !detV || !src)
         return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
-    if (g->nbatch == 0) return CTP_OK;
     return siddon_bp(img, prj, detCenter, detU, detV, src, *g, flags, as_stream(stream));
 }
 
@@ -567,8 +567,8 @@ int ctp_tomo_fp(float* prj, const float* img, const float* detCenter, const floa
                 unsigned flags, void* stream) {
     int rc = check_geometry(g, true, true);
     if (rc) return rc;
-    if (!prj || !img || !detCenter || !src) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !detCenter || !src) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     return tomo_fp(prj, img, detCenter, src, *g, flags, as_stream(stream));
 }
 
@@ -576,8 +576,8 @@ int ctp_tomo_bp(float* img, const float* prj, const float* detCenter, const floa
                 unsigned flags, void* workspace, size_t workspace_bytes, void* stream) {
     int rc = check_geometry(g, true, true);
     if (rc) return rc;
-    if (!prj || !img || !detCenter || !src) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !detCenter || !src) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     return tomo_bp(img, prj, detCenter, src, *g, flags, workspace, workspace_bytes, as_stream(stream));
 }
 

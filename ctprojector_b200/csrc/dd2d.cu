@@ -14,8 +14,8 @@
 // Design:
 //  * dd_table_kernel evaluates, once per call and in FP64, the footprint edges
 //    of every detector-cell edge ray of every view as lines x(row) = A + B*t in
-//    image coordinates (t = row - anchor), the footprint width per cell as
-//    WA + WB*t, and the ray-length factor L per cell.  The forward projector
+//    image coordinates (t = row - anchor) and the ray-length factor L per
+//    cell.  The forward projector
 //    and its exact transpose read the same FP32 table entries, so both see
 //    bit-identical footprints.
 //  * Forward projection: one thread per ray, rows read with coalesced loads
@@ -30,6 +30,8 @@
 //        image-space overlaps taken from the same edge table.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 
 #include "ctp_common.cuh"
 
@@ -46,8 +48,6 @@ constexpr int kFPThreads = 128;
 struct DDTab {
     const float* eA[2];  // [nview][nu+1] edge position at the anchor row/col
     const float* eB[2];  // [nview][nu+1] edge slope per row/col
-    const float* cWA[2]; // [nview][nu] footprint width at the anchor
-    const float* cWB[2]; // [nview][nu] width slope
     const float* cL[2];  // [nview][nu] ray length factor dy/|cos| or dx/|sin|
     const float* wx;     // [nview] blend weight of the row (y main axis) sweep
     int ym, xm;          // anchor row / column
@@ -56,13 +56,11 @@ struct DDTab {
 struct DDTabW {
     float* eA[2];
     float* eB[2];
-    float* cWA[2];
-    float* cWB[2];
     float* cL[2];
     float* wx;
 };
 
-size_t table_floats(size_t nview, size_t nu) { return 2 * (2 * nview * (nu + 1) + 3 * nview * nu) + nview; }
+size_t table_floats(size_t nview, size_t nu) { return 2 * (2 * nview * (nu + 1) + nview * nu) + nview; }
 
 // Table carve-out in a float buffer; the same layout for readers and writers.
 void carve_table(float* base, size_t nview, size_t nu, DDTabW& w) {
@@ -71,8 +69,6 @@ void carve_table(float* base, size_t nview, size_t nu, DDTabW& w) {
     for (int o = 0; o < 2; ++o) {
         w.eA[o] = p; p += ne;
         w.eB[o] = p; p += ne;
-        w.cWA[o] = p; p += nc;
-        w.cWB[o] = p; p += nc;
         w.cL[o] = p; p += nc;
     }
     w.wx = p;
@@ -82,7 +78,7 @@ DDTab as_read(const DDTabW& w, int ym, int xm) {
     DDTab t;
     for (int o = 0; o < 2; ++o) {
         t.eA[o] = w.eA[o]; t.eB[o] = w.eB[o];
-        t.cWA[o] = w.cWA[o]; t.cWB[o] = w.cWB[o]; t.cL[o] = w.cL[o];
+        t.cL[o] = w.cL[o];
     }
     t.wx = w.wx;
     t.ym = ym;
@@ -135,15 +131,7 @@ __global__ void dd_table_kernel(DDTabW t, const float* __restrict__ deg, int nvi
     t.eA[1][ie] = (float)ax;
     t.eB[1][ie] = (float)bx;
     if (j < d.nu) {
-        double sx2, sy2, ex2, ey2;
-        edge_ray(geom, th, j + 1, g, d, dsd, dso, sx2, sy2, ex2, ey2);
-        double by2 = (ex2 - sx2) / (ey2 - sy2), ay2 = sx2 + by2 * (ym + 0.5 - sy2);
-        double bx2 = (ey2 - sy2) / (ex2 - sx2), ax2 = sy2 + bx2 * (xm + 0.5 - sx2);
         size_t ic = (size_t)view * d.nu + j;
-        t.cWA[0][ic] = (float)(ay2 - ay);
-        t.cWB[0][ic] = (float)(by2 - by);
-        t.cWA[1][ic] = (float)(ax2 - ax);
-        t.cWB[1][ic] = (float)(bx2 - bx);
         double a = geom == 0 ? (-((double)j - 0.5 * (d.nu - 1)) - (double)d.off_u) * (double)d.du : 0.0;
         t.cL[0][ic] = (float)((double)g.dy / fabs(cos(th - a)));
         t.cL[1][ic] = (float)((double)g.dx / fabs(sin(th - a)));
@@ -155,6 +143,14 @@ __global__ void dd_table_kernel(DDTabW t, const float* __restrict__ deg, int nvi
         t.wx[view] = (float)(r < 0 ? 0.0 : (r > 1 ? 1.0 : r));
     }
 }
+
+// The reference decides its hard axis switches (fan back projection,
+// back-projection pre-weights) on |__cosf(deg)| > |__sinf(deg)|
+// (distanceDriven2DBoxInt.cu:362, distanceDriven2DUtils.cu:22,54).  At views
+// within rounding of 45 degrees the outcome depends on those fast intrinsics,
+// so the same comparison is made here; the geometry itself uses accurate
+// trigonometry.
+__device__ __forceinline__ bool ref_y_main(float deg) { return fabsf(__cosf(deg)) > fabsf(__sinf(deg)); }
 
 // [nslice][ny][nx] -> [nslice][nx][ny]
 template <typename T>
@@ -194,8 +190,8 @@ __device__ __forceinline__ void row_z(int iv, const Grid& g, const Det& d, int& 
 // image (n = nx cells per line, nl = ny lines) or rows of the transposed image.
 template <typename Tin, bool COUNT>
 __device__ __forceinline__ float sweep(const Tin* __restrict__ s0, const Tin* __restrict__ s1, float wz, int n,
-                                       int nl, int anchor, float Aa, float Ba, float Ab, float Bb, float WA,
-                                       float WB, unsigned long long& cnt) {
+                                       int nl, int anchor, float Aa, float Ba, float Ab, float Bb,
+                                       unsigned long long& cnt) {
     float sum = 0.f;
     for (int l = 0; l < nl; ++l) {
         float t = (float)(l - anchor);
@@ -209,7 +205,10 @@ __device__ __forceinline__ float sweep(const Tin* __restrict__ s0, const Tin* __
         }
         float v = box_line(s0 + (size_t)l * n, 1, lo, hi, n);
         if (wz != 0.f) v = v * (1.f - wz) + box_line(s1 + (size_t)l * n, 1, lo, hi, n) * wz;
-        sum += __fdividef(v, fabsf(fmaf(WB, t, WA)));
+        // normalised by the width of the rounded footprint, as the reference
+        // does (:63-66): the ratio is the mean of the line over the interval,
+        // which edge rounding only shifts instead of rescaling
+        sum += __fdividef(v, hi - lo);
     }
     return sum;
 }
@@ -238,16 +237,14 @@ __global__ void __launch_bounds__(kFPThreads) dd2d_fp_kernel(Tout* __restrict__ 
             const Tin* s0 = img + ((size_t)b * g.nz + iz) * plane;
             const Tin* s1 = img + ((size_t)b * g.nz + iz1) * plane;
             float sum = sweep<Tin, COUNT>(s0, s1, wz, g.nx, g.ny, tab.ym, tab.eA[0][ie], tab.eB[0][ie],
-                                          tab.eA[0][ie + 1], tab.eB[0][ie + 1], tab.cWA[0][ic], tab.cWB[0][ic],
-                                          cnt);
+                                          tab.eA[0][ie + 1], tab.eB[0][ie + 1], cnt);
             acc += sum * tab.cL[0][ic] * wx;
         }
         if (wx < 1.f) {
             const Tin* s0 = imgT + ((size_t)b * g.nz + iz) * plane;
             const Tin* s1 = imgT + ((size_t)b * g.nz + iz1) * plane;
             float sum = sweep<Tin, COUNT>(s0, s1, wz, g.ny, g.nx, tab.xm, tab.eA[1][ie], tab.eB[1][ie],
-                                          tab.eA[1][ie + 1], tab.eB[1][ie + 1], tab.cWA[1][ic], tab.cWB[1][ic],
-                                          cnt);
+                                          tab.eA[1][ie + 1], tab.eB[1][ie + 1], cnt);
             acc += sum * tab.cL[1][ic] * (1.f - wx);
         }
         if (!COUNT) {
@@ -256,7 +253,7 @@ __global__ void __launch_bounds__(kFPThreads) dd2d_fp_kernel(Tout* __restrict__ 
                 // (ReverseWeightBPParallelKernel, distanceDriven2DUtils.cu:68).
                 float s, c;
                 sincosf(deg[view], &s, &c);
-                acc /= (fabsf(c) > fabsf(s)) ? g.dy / fabsf(c) : g.dx / fabsf(s);
+                acc /= ref_y_main(deg[view]) ? g.dy / fabsf(c) : g.dx / fabsf(s);
             }
             Tout* o = prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu;
             if (accumulate) acc += rdf(o);
@@ -273,6 +270,7 @@ __global__ void __launch_bounds__(kFPThreads) dd2d_fp_kernel(Tout* __restrict__ 
     }
 }
 
+
 // Fan pre-weight of the copied sinogram for the normalised back projection
 // (PreweightBPKernel, distanceDriven2DUtils.cu:8-33): hard switch on the view
 // angle, weight from the ray angle.
@@ -285,10 +283,9 @@ __global__ void fan_preweight_kernel(float* __restrict__ out, const Tin* __restr
     int view = (int)((i / ((size_t)d.nu * d.nv)) % nview);
     float th = deg[view];
     float a = (-((float)iu - (d.nu - 1) / 2.0f) - d.off_u) * d.du;
-    float s, c, sa, ca;
-    sincosf(th, &s, &c);
+    float sa, ca;
     sincosf(th - a, &sa, &ca);
-    float w = (fabsf(c) > fabsf(s)) ? g.dy / fabsf(ca) : g.dx / fabsf(sa);
+    float w = ref_y_main(th) ? g.dy / fabsf(ca) : g.dx / fabsf(sa);
     out[i] = ldf(prj + i) * w;
 }
 
@@ -360,6 +357,7 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
     float* s_sin = s_cos + kBPViews;
     int* s_w0 = (int*)(s_sin + kBPViews);
     int* s_ok = s_w0 + kBPViews;
+    int* s_ym = s_ok + kBPViews;
 
     int tiles_x = (g.nx + kTile - 1) / kTile;
     int tx0 = (blockIdx.x % tiles_x) * kTile, ty0 = (blockIdx.x / tiles_x) * kTile;
@@ -392,6 +390,7 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
             tile_window(FAN, tx0, ty0, g, d, c, s, dso, win, w0, ok);
             s_w0[tid] = w0;
             s_ok[tid] = ok;
+            s_ym[tid] = ref_y_main(deg[v0 + tid]) ? 1 : 0;
         }
         __syncthreads();
         for (int i = tid; i < nvc * win; i += blockDim.x) {
@@ -411,7 +410,7 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
                 const Tp* grow = rows + (size_t)(v0 + vi) * view_stride;
                 if (FAN) {
                     float a1, a2;
-                    if (fabsf(c) > fabsf(s)) {
+                    if (s_ym[vi]) {
                         a1 = det_coord(true, x1, yc, c, s, dso, d);
                         a2 = det_coord(true, x2, yc, c, s, dso, d);
                     } else {
@@ -444,7 +443,7 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
                     }
                     float wx = clampf((fabsf(c) - fabsf(s) + kDDMargin) / (2 * kDDMargin), 0.f, 1.f);
                     float val = valx * wx + valy * (1 - wx);
-                    if (!fbp) val *= (fabsf(c) > fabsf(s)) ? g.dy / fabsf(c) : g.dx / fabsf(s);  // :39-65
+                    if (!fbp) val *= s_ym[vi] ? g.dy / fabsf(c) : g.dx / fabsf(s);  // :39-65
                     acc += val;
                 }
             }
@@ -469,8 +468,8 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
     Tout* __restrict__ img, const Tp* __restrict__ prj, const float* __restrict__ deg, DDTab tab, int nview, Grid g,
     Det d, float dso, int accumulate, int win) {
     extern __shared__ float smem[];
-    // per view: p[win], then per orientation: A[win+1], B[win+1], WA[win], WB[win], L[win]
-    const int per_o = 2 * (win + 1) + 3 * win;
+    // per view: p[win], then per orientation: A[win+1], B[win+1], L[win]
+    const int per_o = 2 * (win + 1) + win;
     const int per_v = win + 2 * per_o;
     float* s_view = smem;                           // [kAdjViews][per_v]
     float* s_cos = s_view + kAdjViews * per_v;      // [kAdjViews]
@@ -535,13 +534,8 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
                                 val = (q < win + 1) ? tab.eA[o][ie] : tab.eB[o][ie];
                             }
                         } else {
-                            q -= 2 * (win + 1);
-                            int which = q / win;
-                            int cell = w0 + (q - which * win);
-                            if (cell >= 0 && cell < d.nu) {
-                                size_t ic = (size_t)view * d.nu + cell;
-                                val = which == 0 ? tab.cWA[o][ic] : (which == 1 ? tab.cWB[o][ic] : tab.cL[o][ic]);
-                            }
+                            int cell = w0 + (q - 2 * (win + 1));
+                            if (cell >= 0 && cell < d.nu) val = tab.cL[o][(size_t)view * d.nu + cell];
                         }
                     }
                 }
@@ -576,24 +570,25 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
                         const float* sp = sv;
                         const float* sA = sv + win + o * per_o;
                         const float* sB = sA + (win + 1);
-                        const float* sWA = sB + (win + 1);
-                        const float* sWB = sWA + win;
-                        const float* sL = sWB + win;
+                        const float* sL = sB + (win + 1);
                         for (int k = kmin; k <= kmax; ++k) {
-                            float Aa, Ba, Ab, Bb, WA, WB, L, p;
+                            float Aa, Ba, Ab, Bb, L, p;
                             int kk = k - w0;
                             if (ok && kk >= 0 && kk < win) {
                                 Aa = sA[kk]; Ba = sB[kk]; Ab = sA[kk + 1]; Bb = sB[kk + 1];
-                                WA = sWA[kk]; WB = sWB[kk]; L = sL[kk]; p = sp[kk];
+                                L = sL[kk]; p = sp[kk];
                             } else {
                                 size_t ie = (size_t)view * (d.nu + 1) + k, ic = (size_t)view * d.nu + k;
                                 Aa = tab.eA[o][ie]; Ba = tab.eB[o][ie]; Ab = tab.eA[o][ie + 1]; Bb = tab.eB[o][ie + 1];
-                                WA = tab.cWA[o][ic]; WB = tab.cWB[o][ic]; L = tab.cL[o][ic];
+                                L = tab.cL[o][ic];
                                 p = ldf(rows + (size_t)view * d.nv * d.nu + k) * om;
                             }
                             float xa = fmaf(Ba, t, Aa), xb = fmaf(Bb, t, Ab);
-                            float ov = fminf(fmaxf(xa, xb), pmin + 1.f) - fmaxf(fminf(xa, xb), pmin);
-                            if (ov > 0.f) sum += p * L * __fdividef(ov, fabsf(fmaf(WB, t, WA)));
+                            float lo = fminf(xa, xb), hi = fmaxf(xa, xb);
+                            float ov = fminf(hi, pmin + 1.f) - fmaxf(lo, pmin);
+                            // the forward projector's coefficient: overlap over the
+                            // width of the same rounded footprint
+                            if (ov > 0.f) sum += p * L * __fdividef(ov, hi - lo);
                         }
                         acc += sum * wo;
                     }
@@ -607,6 +602,368 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
         if (accumulate) acc += rdf(o);
         stf(o, acc);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Forward projection, fast path (fan and parallel, z slices projected one to
+// one onto detector rows).
+//
+// A CTA owns a group of views of one slice and streams the image through
+// shared memory kFRows lines at a time (rows of the image for the views traced
+// along y, rows of the transposed image for those traced along x).  Each staged
+// line is stored as its running integral F in double-float form (hi, lo) plus
+// the pixel value r, so the integral of the line over [a, b] is F(b) - F(a)
+// with no cancellation.  Detector cells share their edges, so each lane of a
+// warp evaluates F at one edge (x = A + B t from the FP64 edge table) and takes
+// its neighbour's value with a shuffle: 31 rays per warp, one table read per
+// ray and line.  The normalisation by the footprint width, the ray-length
+// factor and the blend weight are those of DDFPTracing
+// (distanceDriven2DBoxInt.cu:21-106).
+constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
+
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = a + b;
+    float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+// Stage kFRows lines (length n, stride n between lines) into prefix tables of
+// n+1 entries {hi, lo, r, 0}: entry i holds the integral over cells [0, i).
+template <typename Tin>
+__device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ src, int nlines, int n, int warp,
+                            int lane, int nwarps) {
+    const int E = (n + 1 + 31) / 32;
+    for (int l = warp; l < nlines; l += nwarps) {
+        const Tin* row = src + (size_t)l * n;
+        float4* T = tab + (size_t)l * (n + 1);
+        const int k0 = lane * E;
+        // lane total as a double-float
+        float hi = 0.f, lo = 0.f;
+        for (int q = 0; q < E; ++q) {
+            int k = k0 + q;
+            if (k < n) {
+                float e;
+                two_sum(hi, ldf(row + k), hi, e);
+                lo += e;
+            }
+        }
+        // exclusive scan of (hi, lo) across the warp
+        float ihi = hi, ilo = lo;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            float th = __shfl_up_sync(0xffffffffu, ihi, o), tl = __shfl_up_sync(0xffffffffu, ilo, o);
+            if (lane >= o) {
+                float sh, e;
+                two_sum(ihi, th, sh, e);
+                float sl = ilo + tl + e;
+                ihi = sh + sl;
+                ilo = sl - (ihi - sh);
+            }
+        }
+        float bhi, blo;
+        {
+            float e;
+            two_sum(ihi, -hi, bhi, e);
+            blo = ilo - lo + e;
+            float t = bhi + blo;
+            blo = blo - (t - bhi);
+            bhi = t;
+        }
+        for (int q = 0; q < E; ++q) {
+            int k = k0 + q;
+            if (k <= n) {
+                float r = k < n ? ldf(row + k) : 0.f;
+                T[k] = make_float4(bhi, blo, r, 0.f);
+                float e;
+                two_sum(bhi, r, bhi, e);
+                blo += e;
+            }
+        }
+    }
+}
+
+template <bool FAN, typename Tin, typename Tout>
+__global__ void __launch_bounds__(256) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
+                                                           const Tin* __restrict__ imgT, DDTab tab, Grid g, Det d,
+                                                           int nview, int vgroup, int nrows_chunk,
+                                                           const float* __restrict__ deg, int unweight_par) {
+    extern __shared__ float4 s_lines[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int v0 = blockIdx.x * vgroup;
+    const int nvg = min(vgroup, nview - v0);
+    const int slice = blockIdx.y;  // b * nz + iz, detector row iv = iz
+    const int iz = slice % g.nz, b = slice / g.nz;
+    const int ipv = (d.nu + 30) / 31;  // edge groups per view
+    const int nitems = nvg * ipv;
+
+    float res[kFMaxItems];
+#pragma unroll
+    for (int q = 0; q < kFMaxItems; ++q) res[q] = 0.f;
+
+    for (int o = 0; o < 2; ++o) {
+        const int n = o == 0 ? g.nx : g.ny;       // cells per line
+        const int nl = o == 0 ? g.ny : g.nx;      // lines
+        const int anchor = o == 0 ? tab.ym : tab.xm;
+        const Tin* src = (o == 0 ? img : imgT) + (size_t)slice * g.nx * g.ny;
+        float A[kFMaxItems], B[kFMaxItems], acc[kFMaxItems];
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < kFMaxItems; ++q) {
+            int it = warp + 8 * q;
+            A[q] = B[q] = acc[q] = 0.f;
+            if (it < nitems) {
+                int vi = it / ipv, m = it - vi * ipv;
+                int view = v0 + vi;
+                float wx = tab.wx[view];
+                bool active = o == 0 ? wx > 0.f : wx < 1.f;
+                int j = 31 * m + lane;
+                if (active && j <= d.nu) {
+                    size_t ie = (size_t)view * (d.nu + 1) + j;
+                    A[q] = tab.eA[o][ie];
+                    B[q] = tab.eB[o][ie];
+                    any = true;
+                } else {
+                    // edge beyond the detector or view not traced here: a unit
+                    // spacing keeps the (unused) width of its pair non-zero
+                    A[q] = (float)lane;
+                }
+            }
+        }
+        // every warp must take part in staging whether or not it has work
+        bool cta_any = __syncthreads_or(any);
+        if (!cta_any) continue;
+        const float nf = (float)n;
+        for (int l0 = 0; l0 < nl; l0 += nrows_chunk) {
+            const int nlc = min(nrows_chunk, nl - l0);
+            __syncthreads();
+            stage_lines(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
+            __syncthreads();
+            for (int r = 0; r < nlc; ++r) {
+                const float t = (float)(l0 + r - anchor);
+                const float4* T = s_lines + (size_t)r * (n + 1);
+#pragma unroll
+                for (int q = 0; q < kFMaxItems; ++q) {
+                    if (warp + 8 * q >= nitems) break;
+                    float xr = fmaf(B[q], t, A[q]);
+                    float x = clampf(xr, 0.f, nf);
+                    int i = __float2int_rd(x);
+                    float4 e = T[i];
+                    float hi = e.x, lo = fmaf(e.z, x - (float)i, e.y);
+                    float hin = __shfl_down_sync(0xffffffffu, hi, 1);
+                    float lon = __shfl_down_sync(0xffffffffu, lo, 1);
+                    float xn = __shfl_down_sync(0xffffffffu, xr, 1);
+                    // signed integral over [x_j, x_j+1] divided by the signed
+                    // width of the rounded footprint
+                    acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kFMaxItems; ++q) {
+            int it = warp + 8 * q;
+            if (it >= nitems) break;
+            int vi = it / ipv, m = it - vi * ipv;
+            int view = v0 + vi;
+            int k = 31 * m + lane;
+            float wx = tab.wx[view];
+            bool active = o == 0 ? wx > 0.f : wx < 1.f;
+            if (active && lane < 31 && k < d.nu) {
+                size_t ic = (size_t)view * d.nu + k;
+                res[q] += acc[q] * tab.cL[o][ic] * (o == 0 ? wx : 1.f - wx);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kFMaxItems; ++q) {
+        int it = warp + 8 * q;
+        if (it >= nitems) break;
+        int vi = it / ipv, m = it - vi * ipv;
+        int view = v0 + vi;
+        int k = 31 * m + lane;
+        if (lane < 31 && k < d.nu) {
+            float v = res[q];
+            if (unweight_par) {
+                float sn, cs;
+                sincosf(deg[view], &sn, &cs);
+                v /= ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn);
+            }
+            stf(prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + k, v);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Parallel-beam normalised back projection, fast path.
+//
+// For a parallel beam the detector footprint of a pixel's x-edges (or
+// y-edges) is symmetric about the detector coordinate of the pixel centre,
+// jc = -((x cos + y sin)/du + off_u) + nu/2, which is linear in (ix, iy); the
+// half widths are dx|cos|/2du and dy|sin|/2du.  So the reference's
+// normalised box integral (DDBPParallelKernel, distanceDriven2DBoxInt.cu:
+// 409-497) is F(jc + h) - F(jc - h) over 2h, where F is the running integral
+// of the detector row.  A CTA owns a 32x32 pixel tile; per chunk of views each
+// warp stages, for one view at a time, the window of cells the tile projects
+// onto as a table of (prefix sum, cell value) pairs -- prefix sums local to the
+// window, so they stay small and FP32 keeps them accurate -- and every thread
+// then evaluates 4 pixels x 2 table reads per view.  No atomics, no loops over
+// cells.
+constexpr int kPT = 32;        // tile edge
+constexpr int kPViews = 32;    // views per staged chunk
+constexpr int kPMaxWin = 255;  // staged cells per view (table holds win+1 entries)
+constexpr int kPPar = 9;       // per-view parameters in shared memory
+
+__device__ __forceinline__ float prefix_eval(const float2* __restrict__ T, float x) {
+    int i = __float2int_rd(x);
+    float2 e = T[i];
+    return fmaf(e.y, x - (float)i, e.x);
+}
+
+template <typename Tp, typename Tout>
+__global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ prj,
+                                                               const float* __restrict__ deg, int nview, Grid g,
+                                                               Det d, int fbp, int accumulate, int win) {
+    extern __shared__ float4 smem_f4[];
+    const int stride = win + 1;
+    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                   // [kPViews][stride]
+    float* s_par = reinterpret_cast<float*>(s_tab + kPViews * stride);    // [kPPar][kPViews]
+    int* s_w0 = reinterpret_cast<int*>(s_par + kPPar * kPViews);          // [kPViews], -1 << 30 = not staged
+
+    const int tiles_x = (g.nx + kPT - 1) / kPT;
+    const int tx0 = (blockIdx.x % tiles_x) * kPT, ty0 = (blockIdx.x / tiles_x) * kPT;
+    const int iz = blockIdx.y % g.nz, b = blockIdx.y / g.nz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
+    int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);  // truncation, :383
+    bool row_ok = iv >= 0 && iv < d.nv;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const Tp* rows = prj + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
+    const size_t vstride = (size_t)d.nv * d.nu;
+    const float fwin = (float)win;
+
+    for (int v0 = 0; v0 < nview && row_ok; v0 += kPViews) {
+        const int nvc = min(kPViews, nview - v0);
+        for (int vi = warp; vi < nvc; vi += 8) {
+            const int view = v0 + vi;
+            double s, c;
+            sincos((double)deg[view], &s, &c);
+            const double du = d.du;
+            const double jx = -c * g.dx / du, jy = -s * g.dy / du;
+            const double xc0 = (tx0 + 0.5 - 0.5 * g.nx) * g.dx + g.cx;
+            const double yc0 = (ty0 + 0.5 - 0.5 * g.ny) * g.dy + g.cy;
+            const double j00 = -((xc0 * c + yc0 * s) / du + d.off_u) + 0.5 * d.nu;
+            const double ac = fabs(c), as = fabs(s);
+            const bool ya = ac > as - kDDMarginD, xa = ac < as + kDDMarginD;
+            const double r = (ac - as + kDDMarginD) / (2 * kDDMarginD);
+            const double wx = r < 0 ? 0.0 : (r > 1 ? 1.0 : r);
+            const double hx = 0.5 * g.dx * ac / du, hy = 0.5 * g.dy * as / du;
+            const double hm = fmax(ya ? hx : 0.0, xa ? hy : 0.0);
+            const double pw = fbp ? 1.0 : (ref_y_main(deg[view]) ? g.dy / ac : g.dx / as);  // Utils.cu:39-65
+            const double jmin = j00 + fmin(0.0, (kPT - 1) * jx) + fmin(0.0, (kPT - 1) * jy);
+            const double jmax = j00 + fmax(0.0, (kPT - 1) * jx) + fmax(0.0, (kPT - 1) * jy);
+            bool ok = isfinite(j00) && isfinite(hm);
+            int w0 = 0;
+            if (ok) {
+                w0 = (int)floor(jmin - hm) - 2;
+                ok = ((int)ceil(jmax + hm) + 2 - w0) <= win;
+            }
+            // stage (prefix, value) for window cells w0 .. w0+win-1, entry win = (total, 0)
+            const int per = (stride + 31) / 32;
+            const int k0 = lane * per;
+            float v[8];
+            float run = 0.f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                int k = k0 + q;
+                float x = 0.f;
+                if (ok && q < per && k < win) {
+                    int cell = w0 + k;
+                    if (cell >= 0 && cell < d.nu) x = ldf(rows + (size_t)view * vstride + cell);
+                }
+                v[q] = x;
+                run += x;
+            }
+            float incl = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                float t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            float base = incl - run;
+            float2* T = s_tab + vi * stride;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                int k = k0 + q;
+                if (q < per && k < stride) T[k] = make_float2(base, v[q]);
+                base += v[q];
+            }
+            if (lane == 0) {
+                s_par[0 * kPViews + vi] = (float)(j00 - w0);
+                s_par[1 * kPViews + vi] = (float)jx;
+                s_par[2 * kPViews + vi] = (float)jy;
+                s_par[3 * kPViews + vi] = (float)hx;
+                s_par[4 * kPViews + vi] = (float)hy;
+                s_par[5 * kPViews + vi] = ya ? (float)(pw * wx / (2 * hx)) : 0.f;
+                s_par[6 * kPViews + vi] = xa ? (float)(pw * (1 - wx) / (2 * hy)) : 0.f;
+                s_par[7 * kPViews + vi] = (float)hm;
+                s_par[8 * kPViews + vi] = (float)j00;
+                s_w0[vi] = ok ? w0 : (-1 << 30);
+            }
+        }
+        __syncthreads();
+        for (int vi = 0; vi < nvc; ++vi) {
+            const float jb = s_par[vi], jx = s_par[kPViews + vi], jy = s_par[2 * kPViews + vi];
+            const float hx = s_par[3 * kPViews + vi], hy = s_par[4 * kPViews + vi];
+            const float sx = s_par[5 * kPViews + vi], sy = s_par[6 * kPViews + vi];
+            const float hm = s_par[7 * kPViews + vi];
+            const float2* T = s_tab + vi * stride;
+            const bool staged = s_w0[vi] != (-1 << 30);
+            const float jc0 = fmaf((float)lane, jx, fmaf((float)warp, jy, jb));
+            const float dj = 8.f * jy;
+            if (staged) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    float jc = clampf(fmaf((float)k, dj, jc0), hm, fwin - hm);
+                    float a = 0.f;
+                    if (sx != 0.f) a = fmaf(prefix_eval(T, jc + hx) - prefix_eval(T, jc - hx), sx, a);
+                    if (sy != 0.f) a = fmaf(prefix_eval(T, jc + hy) - prefix_eval(T, jc - hy), sy, a);
+                    acc[k] += a;
+                }
+            } else {
+                // window larger than the staging buffer: integrate the row in global memory
+                const Tp* grow = rows + (size_t)(v0 + vi) * vstride;
+                const float jabs0 = s_par[8 * kPViews + vi] + (float)lane * jx + (float)warp * jy;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    float jc = jabs0 + (float)k * dj;
+                    float a = 0.f;
+                    if (sx != 0.f) a += box_line(grow, 1, jc - hx, jc + hx, d.nu) * sx;
+                    if (sy != 0.f) a += box_line(grow, 1, jc - hy, jc + hy, d.nu) * sy;
+                    acc[k] += a;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const int ix = tx0 + lane;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int iy = ty0 + warp + 8 * k;
+        if (ix < g.nx && iy < g.ny) {
+            Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+            float a = acc[k];
+            if (accumulate) a += rdf(o);
+            stf(o, a);
+        }
+    }
+}
+
+// Staged window for the fast parallel path (cells), or 0 if it does not fit.
+int par_fast_window(const ctp_geometry& g) {
+    double du = fabs((double)g.du);
+    double w = ((kPT - 1) * ((double)g.dx + g.dy) + fmax(g.dx, g.dy)) / du;
+    int win = (int)ceil(w) + 8;
+    return win <= kPMaxWin ? win : 0;
 }
 
 // Staged window (cells) needed by a 16x16 tile, from a conservative bound on
@@ -647,6 +1004,26 @@ int build_table(float* base, const float* deg, const ctp_geometry& g, int geom, 
     return check_launch("dd_table_kernel");
 }
 
+// The fast forward projector handles slices projected one to one onto
+// detector rows (nz == nv and the z interpolation of every row landing exactly
+// on its own slice, as for single-slice and matched stacks) and at most
+// kFMaxItems edge groups per warp.
+bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
+    if (g.nz != g.nv) return false;
+    for (size_t iv = 0; iv < g.nv; ++iv) {
+        double z = ((double)iv - (g.nv - 1) / 2.0 + g.off_v) * g.dv;
+        z = (z - g.cz) / g.dz + g.nz / 2.0 - 0.5;
+        if (fabs(z - (double)iv) > 1e-6) return false;
+    }
+    int ipv = (int)((g.nu + 30) / 31);
+    vgroup = (kFMaxItems * 8) / ipv;
+    if (vgroup < 1) return false;
+    size_t line = (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+    nrows = 8;
+    while (nrows > 1 && nrows * line > 110 * 1024) nrows /= 2;
+    return nrows * line <= 200 * 1024;
+}
+
 template <typename Tin, typename Tout>
 int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
               unsigned flags, char* ws, cudaStream_t s) {
@@ -657,8 +1034,25 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     dim3 tg((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 31) / 32), (unsigned)(g.nbatch * g.nz));
     transpose_kernel<Tin><<<tg, dim3(32, 8), 0, s>>>(imgT, cptr<Tin>(img), (int)g.nx, (int)g.ny);
     if ((rc = check_launch("transpose_kernel"))) return rc;
-    dim3 grid((unsigned)((g.nu + kFPThreads - 1) / kFPThreads), (unsigned)g.nview, (unsigned)(g.nbatch * g.nv));
     int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
+    int vgroup = 0, nrows = 0;
+    if (fp_fast_ok(g, vgroup, nrows)) {
+        size_t shm = (size_t)nrows * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+        dim3 fg((unsigned)((g.nview + vgroup - 1) / vgroup), (unsigned)(g.nbatch * g.nz));
+        if (geom == 0) {
+            auto k = dd2d_fp_fast_kernel<true, Tin, Tout>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k<<<fg, 256, shm, s>>>(mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g),
+                                   (int)g.nview, vgroup, nrows, deg, unweight);
+        } else {
+            auto k = dd2d_fp_fast_kernel<false, Tin, Tout>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k<<<fg, 256, shm, s>>>(mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g),
+                                   (int)g.nview, vgroup, nrows, deg, unweight);
+        }
+        return check_launch("dd2d_fp_fast_kernel");
+    }
+    dim3 grid((unsigned)((g.nu + kFPThreads - 1) / kFPThreads), (unsigned)g.nview, (unsigned)(g.nbatch * g.nv));
     dd2d_fp_kernel<Tin, Tout, false><<<grid, kFPThreads, 0, s>>>(
         mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g), (int)g.nview, deg, unweight,
         (flags & CTP_FLAG_ZERO_OUT) ? 0 : 0, nullptr);
@@ -736,7 +1130,7 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
     if (flags & CTP_FLAG_ADJOINT) {
         DDTab tab;
         if ((rc = build_table(reinterpret_cast<float*>(ws), deg, g, geom, s, tab))) return rc;
-        int per_v = wl + 2 * (2 * (wl + 1) + 3 * wl);
+        int per_v = wl + 2 * (2 * (wl + 1) + wl);
         size_t shm = (size_t)kAdjViews * per_v * 4 + kAdjViews * 5 * 4;
         if (geom == 0) {
             auto k = dd2d_bp_adjoint_kernel<true, Tin, Tout>;
@@ -752,7 +1146,7 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
         return check_launch("dd2d_bp_adjoint_kernel");
     }
     int fbp = (type & (CTP_TYPE_FBP | CTP_TYPE_FORCE_FBP)) ? 1 : 0;
-    size_t shm = (size_t)kBPViews * wl * 4 + kBPViews * 4 * 4;
+    size_t shm = (size_t)kBPViews * wl * 4 + kBPViews * 5 * 4;
     if (geom == 0) {
         if (!fbp) {
             float* wprj = reinterpret_cast<float*>(ws);
@@ -769,6 +1163,16 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
                                                accumulate, win > 0 ? win : 0);
         }
     } else {
+        int pwin = par_fast_window(g);
+        if (pwin > 0) {
+            int tiles_p = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
+            size_t pshm = (size_t)kPViews * (pwin + 1) * sizeof(float2) + kPPar * kPViews * 4 + kPViews * 4;
+            auto kf = dd2d_bp_par_fast_kernel<Tin, Tout>;
+            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
+            kf<<<dim3((unsigned)tiles_p, (unsigned)(g.nbatch * g.nz)), 256, pshm, s>>>(
+                mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin);
+            return check_launch("dd2d_bp_par_fast_kernel");
+        }
         auto k = dd2d_bp_parity_kernel<false, Tin, Tout>;
         k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, fbp,
                                            accumulate, win > 0 ? win : 0);

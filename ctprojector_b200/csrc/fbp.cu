@@ -12,6 +12,9 @@
 // (N = 2^a 3^b), exact because g has support [-(nu-1), nu-1]:
 //   * g is computed once per (nu, da, window, geometry) on the host in FP64
 //     and its N-point spectrum (real: g is even) cached on the device;
+//   * the transforms and the spectrum product run in FP64 (this path is the
+//     accuracy reference; the default path replays the reference's FP32
+//     construction further below);
 //   * one pad/weight kernel writes all rows of the batch into an in-place
 //     R2C layout, cuFFT runs batched R2C and C2R over every row at once, a
 //     multiply kernel scales the spectrum, and a crop kernel writes the first
@@ -102,7 +105,7 @@ std::vector<double> ramp_kernel(int nu, double da, int filter, bool equiangular)
 }
 
 struct Spectrum {
-    float* dev = nullptr;  // N/2+1 real coefficients
+    double* dev = nullptr;  // N/2+1 real coefficients
     int n = 0;
 };
 
@@ -110,7 +113,7 @@ std::mutex g_spec_mu;
 std::map<std::tuple<int, int, long long, int, int, int>, Spectrum> g_spec;
 
 // Device spectrum of g for this (device, nu, da, filter, kind, N); built once.
-int get_spectrum(int nu, double da, int filter, bool equiangular, int N, const float** out) {
+int get_spectrum(int nu, double da, int filter, bool equiangular, int N, const double** out) {
     int dev = 0;
     cudaGetDevice(&dev);
     long long dkey;
@@ -124,7 +127,7 @@ int get_spectrum(int nu, double da, int filter, bool equiangular, int N, const f
     }
     std::vector<double> g = ramp_kernel(nu, da, filter, equiangular);
     int M = N / 2 + 1;
-    std::vector<float> G(M);
+    std::vector<double> G(M);
     std::vector<double> cosN(N);
     for (int i = 0; i < N; ++i) cosN[i] = cos(2 * M_PI * i / N);
     for (int m = 0; m < M; ++m) {
@@ -135,12 +138,12 @@ int get_spectrum(int nu, double da, int filter, bool equiangular, int N, const f
             if (idx >= N) idx -= N;
             acc += 2 * g[k] * cosN[idx];
         }
-        G[m] = (float)acc;
+        G[m] = acc;
     }
     Spectrum sp;
     sp.n = M;
-    cudaError_t e = cudaMalloc(&sp.dev, sizeof(float) * M);  // one-time table, kept for the process
-    if (e == cudaSuccess) e = cudaMemcpy(sp.dev, G.data(), sizeof(float) * M, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMalloc(&sp.dev, sizeof(double) * M);  // one-time table, kept for the process
+    if (e == cudaSuccess) e = cudaMemcpy(sp.dev, G.data(), sizeof(double) * M, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return set_error((int)e, "ramp spectrum upload: %s", cudaGetErrorString(e));
     g_spec[key] = sp;
     *out = sp.dev;
@@ -174,9 +177,9 @@ int get_plan(int N, int batch, Plan** out) {
         return set_error(CTP_ERR_CUFFT, "cufftCreate failed");
     cufftSetAutoAllocation(p->fwd, 0);
     cufftSetAutoAllocation(p->inv, 0);
-    if (cufftMakePlanMany(p->fwd, 1, n, rembed, 1, rembed[0], cembed, 1, cembed[0], CUFFT_R2C, batch, &w1) !=
+    if (cufftMakePlanMany(p->fwd, 1, n, rembed, 1, rembed[0], cembed, 1, cembed[0], CUFFT_D2Z, batch, &w1) !=
             CUFFT_SUCCESS ||
-        cufftMakePlanMany(p->inv, 1, n, cembed, 1, cembed[0], rembed, 1, rembed[0], CUFFT_C2R, batch, &w2) !=
+        cufftMakePlanMany(p->inv, 1, n, cembed, 1, cembed[0], rembed, 1, rembed[0], CUFFT_Z2D, batch, &w2) !=
             CUFFT_SUCCESS)
         return set_error(CTP_ERR_CUFFT, "cufftMakePlanMany failed (N=%d, batch=%d)", N, batch);
     p->work = w1 > w2 ? w1 : w2;
@@ -187,52 +190,276 @@ int get_plan(int N, int batch, Plan** out) {
 
 constexpr int kMaxRowsPerExec = 32768;
 
-// Zero-pad and pre-weight rows into the in-place R2C layout.
-__global__ void pad_kernel(float* __restrict__ buf, const float* __restrict__ prj, int nu, int N, int stride,
-                           size_t rows, int fan, float da, float off_u) {
+// Zero-pad and pre-weight rows (FP64) into the in-place D2Z layout.
+__global__ void pad_kernel(double* __restrict__ buf, const float* __restrict__ prj, int nu, int N, int stride,
+                           size_t rows, int fan, double da, double off_u) {
     size_t r = blockIdx.y + (size_t)blockIdx.z * gridDim.y;
     if (r >= rows) return;
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < stride; n += gridDim.x * blockDim.x) {
-        float v = 0.f;
+        double v = 0.0;
         if (n < nu) {
-            v = prj[r * nu + n];
-            if (fan) v *= cosf(((n - (nu - 1) / 2.f) - off_u) * da);  // fbp.cu:62-66
+            v = (double)prj[r * nu + n];
+            if (fan) v *= cos(((n - (nu - 1) / 2.0) - off_u) * da);  // fbp.cu:62-66
         }
         buf[r * stride + n] = v;
     }
 }
 
-__global__ void spectrum_mul_kernel(float2* __restrict__ spec, const float* __restrict__ G, int M, size_t rows,
-                                    float scale) {
+__global__ void spectrum_mul_kernel(double2* __restrict__ spec, const double* __restrict__ G, int M, size_t rows,
+                                    double scale) {
     size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= rows * M) return;
-    float g = G[i % M] * scale;
-    float2 v = spec[i];
-    spec[i] = make_float2(v.x * g, v.y * g);
+    double g = G[i % M] * scale;
+    double2 v = spec[i];
+    spec[i] = make_double2(v.x * g, v.y * g);
 }
 
-__global__ void crop_kernel(float* __restrict__ out, const float* __restrict__ buf, int nu, int stride, size_t rows) {
+__global__ void crop_kernel(float* __restrict__ out, const double* __restrict__ buf, int nu, int stride, size_t rows) {
     size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= rows * nu) return;
     size_t r = i / nu;
     int n = (int)(i - r * nu);
-    out[i] = buf[r * stride + n];
+    out[i] = (float)buf[r * stride + n];
 }
 
-}  // namespace
+// ------------------------------------------------------------------ reference construction
+// The reference builds the windowed ramp in FP32 (GetRamp, fbpMath.cu:90-241):
+// float spatial ramp on the host, length-L C2C FFT, float window product on
+// the host, inverse C2C, real part / L, length-L R2C.  Rows are then filtered
+// with length-L R2C/C2R transforms in batches of nview rows
+// (fbpParallel.cu:44-86, fbp.cu:81-134).  Replaying those steps in the same
+// float operation order keeps the output within FP32 rounding of the
+// reference.
+struct RefFilter {
+    cufftComplex* spec = nullptr;  // [nu] frequency kernel
+    float* weight = nullptr;       // [nu] fan pre-weight (cos), or null
+};
 
-size_t ramp_filter_workspace(const ctp_geometry& g, int, int) {
+std::mutex g_ref_mu;
+std::map<std::tuple<int, int, unsigned, int, int, unsigned>, RefFilter> g_ref;
+
+int build_ref_filter(int nu, float da, int filter, bool fan, float off_u, RefFilter* out) {
+    const int L = 2 * nu - 1;
+    const float PIf = 3.141592657f;  // projector.h:5
+    std::vector<cufftComplex> ramp(L), win(L);
+    for (int i = 0; i < L; i++) {
+        int k = i - (nu - 1);
+        if (k == 0)
+            ramp[i].x = 1 / (4 * da * da);
+        else if (k % 2 != 0)
+            ramp[i].x = fan ? -1 / (PIf * PIf * sinf(k * da) * sinf(k * da)) : -1 / (PIf * PIf * k * k * da * da);
+        else
+            ramp[i].x = 0;
+        ramp[i].y = 0;
+        switch (filter) {
+            case 1: win[i].x = 0.54f + 0.46f * cosf(2 * PIf * i / (float)L); break;
+            case 2: win[i].x = 0.5f + 0.5f * cosf(2 * PIf * i / (float)L); break;
+            case 3: win[i].x = fabsf(cosf(PIf * i / (float)L)); break;
+            default: win[i].x = 1;
+        }
+        win[i].y = 0;
+    }
+    cufftHandle c2c = 0, r2c = 0;
+    cufftComplex* d = nullptr;
+    float* dk = nullptr;
+    int rc = CTP_OK;
+    // one-time table construction for this geometry; kept for the process
+    if (cudaMalloc(&d, sizeof(cufftComplex) * L) != cudaSuccess || cudaMalloc(&dk, sizeof(float) * L) != cudaSuccess ||
+        cudaMalloc(&out->spec, sizeof(cufftComplex) * nu) != cudaSuccess)
+        rc = set_error(cudaErrorMemoryAllocation, "ramp table allocation failed");
+    if (!rc && (cufftPlan1d(&c2c, L, CUFFT_C2C, 1) != CUFFT_SUCCESS || cufftPlan1d(&r2c, L, CUFFT_R2C, 1) != CUFFT_SUCCESS))
+        rc = set_error(CTP_ERR_CUFFT, "ramp table plan failed");
+    if (!rc) {
+        cudaMemcpy(d, ramp.data(), sizeof(cufftComplex) * L, cudaMemcpyHostToDevice);
+        cufftExecC2C(c2c, d, d, CUFFT_FORWARD);
+        cudaMemcpy(ramp.data(), d, sizeof(cufftComplex) * L, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < L; i++) {
+            float re = ramp[i].x * win[i].x - ramp[i].y * win[i].y;
+            float im = ramp[i].x * win[i].y + ramp[i].y * win[i].x;
+            ramp[i].x = re;
+            ramp[i].y = im;
+        }
+        cudaMemcpy(d, ramp.data(), sizeof(cufftComplex) * L, cudaMemcpyHostToDevice);
+        cufftExecC2C(c2c, d, d, CUFFT_INVERSE);
+        cudaMemcpy(ramp.data(), d, sizeof(cufftComplex) * L, cudaMemcpyDeviceToHost);
+        std::vector<float> k(L);
+        for (int i = 0; i < L; i++) k[i] = ramp[i].x / L;
+        cudaMemcpy(dk, k.data(), sizeof(float) * L, cudaMemcpyHostToDevice);
+        if (cufftExecR2C(r2c, dk, out->spec) != CUFFT_SUCCESS) rc = set_error(CTP_ERR_CUFFT, "ramp R2C failed");
+        cudaError_t e = cudaDeviceSynchronize();
+        if (!rc && e != cudaSuccess) rc = set_error((int)e, "ramp table: %s", cudaGetErrorString(e));
+    }
+    if (!rc && fan) {
+        std::vector<float> w(nu);
+        for (int i = 0; i < nu; i++) w[i] = cosf(((i - (nu - 1) / 2.f) - off_u) * da);  // fbp.cu:62-66
+        if (cudaMalloc(&out->weight, sizeof(float) * nu) != cudaSuccess)
+            rc = set_error(cudaErrorMemoryAllocation, "ramp weight allocation failed");
+        else
+            cudaMemcpy(out->weight, w.data(), sizeof(float) * nu, cudaMemcpyHostToDevice);
+    }
+    if (c2c) cufftDestroy(c2c);
+    if (r2c) cufftDestroy(r2c);
+    if (d) cudaFree(d);
+    if (dk) cudaFree(dk);
+    return rc;
+}
+
+int get_ref_filter(int nu, float da, int filter, bool fan, float off_u, RefFilter* out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    unsigned dbits, obits;
+    memcpy(&dbits, &da, 4);
+    memcpy(&obits, &off_u, 4);
+    auto key = std::make_tuple(dev, nu, dbits, filter, (int)fan, fan ? obits : 0u);
+    std::lock_guard<std::mutex> lk(g_ref_mu);
+    auto it = g_ref.find(key);
+    if (it != g_ref.end()) {
+        *out = it->second;
+        return CTP_OK;
+    }
+    RefFilter f;
+    int rc = build_ref_filter(nu, da, filter, fan, off_u, &f);
+    if (rc) return rc;
+    g_ref[key] = f;
+    *out = f;
+    return CTP_OK;
+}
+
+struct RefPlan {
+    cufftHandle fwd = 0, inv = 0;
+    size_t work = 0;
+    std::mutex mu;
+};
+std::mutex g_rplan_mu;
+std::map<std::tuple<int, int, int>, std::unique_ptr<RefPlan>> g_rplans;
+
+// cufftPlanMany with the reference's layout: real rows of length L (idist L),
+// complex rows of nu bins (odist nu), batch nview.
+int get_ref_plan(int L, int nu, int batch, RefPlan** out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    auto key = std::make_tuple(dev, L, batch);
+    std::lock_guard<std::mutex> lk(g_rplan_mu);
+    auto it = g_rplans.find(key);
+    if (it != g_rplans.end()) {
+        *out = it->second.get();
+        return CTP_OK;
+    }
+    std::unique_ptr<RefPlan> p(new RefPlan());
+    int n[1] = {L};
+    size_t w1 = 0, w2 = 0;
+    if (cufftCreate(&p->fwd) != CUFFT_SUCCESS || cufftCreate(&p->inv) != CUFFT_SUCCESS)
+        return set_error(CTP_ERR_CUFFT, "cufftCreate failed");
+    cufftSetAutoAllocation(p->fwd, 0);
+    cufftSetAutoAllocation(p->inv, 0);
+    if (cufftMakePlanMany(p->fwd, 1, n, nullptr, 1, L, nullptr, 1, nu, CUFFT_R2C, batch, &w1) != CUFFT_SUCCESS ||
+        cufftMakePlanMany(p->inv, 1, n, nullptr, 1, nu, nullptr, 1, L, CUFFT_C2R, batch, &w2) != CUFFT_SUCCESS)
+        return set_error(CTP_ERR_CUFFT, "cufftMakePlanMany failed (L=%d, batch=%d)", L, batch);
+    p->work = w1 > w2 ? w1 : w2;
+    *out = p.get();
+    g_rplans[key] = std::move(p);
+    return CTP_OK;
+}
+
+// CopyPrjToPad + Multiply2D (fbpMath.cu:59-72, cudaMath.cu:28-49): one pass over all rows.
+__global__ void ref_pad_kernel(float* __restrict__ pad, const float* __restrict__ prj, const float* __restrict__ w,
+                               int nu, int L, size_t rows) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= rows * L) return;
+    size_t r = i / L;
+    int n = (int)(i - r * L);
+    float v = 0.f;
+    if (n < nu) {
+        v = prj[r * nu + n];
+        if (w) v = v * w[n];
+    }
+    pad[i] = v;
+}
+
+// ComplexMultiply2D (fbpMath.cu:12-33) against the kernel replicated over rows.
+__global__ void ref_cmul_kernel(cufftComplex* __restrict__ f, const cufftComplex* __restrict__ k, int nu,
+                                size_t rows) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= rows * nu) return;
+    cufftComplex val1 = f[i];
+    cufftComplex val2 = k[i % nu];
+    cufftComplex val;
+    val.x = val1.x * val2.x - val1.y * val2.y;
+    val.y = val1.x * val2.y + val1.y * val2.x;
+    f[i] = val;
+}
+
+// Scale2D + CopyPadToPrj (cudaMath.cu:76-97, fbpMath.cu:74-87).
+__global__ void ref_crop_kernel(float* __restrict__ out, const float* __restrict__ pad, int nu, int L, size_t rows,
+                                float scale) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= rows * nu) return;
+    size_t r = i / nu;
+    int n = (int)(i - r * nu);
+    out[i] = pad[r * L + nu - 1 + n] * scale;
+}
+
+size_t ref_workspace(const ctp_geometry& g) {
+    size_t nu = g.nu, L = 2 * nu - 1, rows = g.nbatch * g.nview * g.nv;
+    RefPlan* p = nullptr;
+    if (get_ref_plan((int)L, (int)nu, (int)g.nview, &p)) return 0;
+    return align_up(rows * L * sizeof(float)) + align_up(rows * nu * sizeof(cufftComplex)) + align_up(p->work);
+}
+
+int ramp_filter_reference(float* fprj, const float* prj, const ctp_geometry& g, int geom, int filter,
+                          void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    int nu = (int)g.nu, L = 2 * nu - 1, nview = (int)g.nview;
+    size_t rows = g.nbatch * g.nview * g.nv;
+    bool fan = geom == 0;
+    RefFilter rf;
+    int rc = get_ref_filter(nu, g.du, filter, fan, g.off_u, &rf);
+    if (rc) return rc;
+    RefPlan* plan = nullptr;
+    if ((rc = get_ref_plan(L, nu, nview, &plan))) return rc;
+    Scratch scr;
+    size_t pad_b = align_up(rows * L * sizeof(float)), frq_b = align_up(rows * nu * sizeof(cufftComplex));
+    if ((rc = scr.acquire(workspace, workspace_bytes, pad_b + frq_b + align_up(plan->work), s))) return rc;
+    float* pad = reinterpret_cast<float*>(scr.base());
+    cufftComplex* frq = reinterpret_cast<cufftComplex*>(scr.base() + pad_b);
+    void* work = scr.base() + pad_b + frq_b;
+    const float PIf = 3.141592657f;
+    // fbpParallel.cu:59, fbp.cu:103 (float arithmetic)
+    float scale = fan ? PIf / g.nview * g.du / g.dso / L : PIf / g.nview * g.du / L;
+    size_t np = rows * L;
+    ref_pad_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(pad, prj, fan ? rf.weight : nullptr, nu, L, rows);
+    if ((rc = check_launch("ref_pad_kernel"))) return rc;
+    {
+        std::lock_guard<std::mutex> lk(plan->mu);
+        cufftSetStream(plan->fwd, s);
+        cufftSetStream(plan->inv, s);
+        cufftSetWorkArea(plan->fwd, work);
+        cufftSetWorkArea(plan->inv, work);
+        for (size_t r0 = 0; r0 < rows; r0 += nview)
+            if (cufftExecR2C(plan->fwd, pad + r0 * L, frq + r0 * nu) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecR2C failed");
+        size_t nf = rows * nu;
+        ref_cmul_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(frq, rf.spec, nu, rows);
+        if ((rc = check_launch("ref_cmul_kernel"))) return rc;
+        for (size_t r0 = 0; r0 < rows; r0 += nview)
+            if (cufftExecC2R(plan->inv, frq + r0 * nu, pad + r0 * L) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecC2R failed");
+    }
+    size_t no = rows * nu;
+    ref_crop_kernel<<<(unsigned)((no + 255) / 256), 256, 0, s>>>(fprj, pad, nu, L, rows, scale);
+    return check_launch("ref_crop_kernel");
+}
+
+size_t exact_workspace(const ctp_geometry& g) {
     size_t rows = g.nbatch * g.nview * g.nv;
     int N = fft_size((int)g.nu);
     size_t chunk = rows < (size_t)kMaxRowsPerExec ? rows : (size_t)kMaxRowsPerExec;
     Plan* p = nullptr;
     if (chunk == 0 || get_plan(N, (int)chunk, &p)) return 0;
-    return align_up(chunk * 2 * (N / 2 + 1) * sizeof(float)) + align_up(p->work);
+    return align_up(chunk * 2 * (N / 2 + 1) * sizeof(double)) + align_up(p->work);
 }
 
-int ramp_filter(float* fprj, const float* prj, const ctp_geometry& g, int geom, int filter, unsigned,
-                void* workspace, size_t workspace_bytes, cudaStream_t s) {
-    if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
+int ramp_filter_exact(float* fprj, const float* prj, const ctp_geometry& g, int geom, int filter, void* workspace,
+                      size_t workspace_bytes, cudaStream_t s) {
     int nu = (int)g.nu;
     size_t rows = g.nbatch * g.nview * g.nv;
     int N = fft_size(nu), M = N / 2 + 1, stride = 2 * M;
@@ -240,21 +467,21 @@ int ramp_filter(float* fprj, const float* prj, const ctp_geometry& g, int geom, 
     Plan* plan = nullptr;
     int rc = get_plan(N, (int)chunk, &plan);
     if (rc) return rc;
-    const float* G = nullptr;
+    const double* G = nullptr;
     bool fan = geom == 0;
     if ((rc = get_spectrum(nu, (double)g.du, filter, fan, N, &G))) return rc;
     Scratch scr;
-    size_t buf_bytes = align_up(chunk * stride * sizeof(float));
+    size_t buf_bytes = align_up(chunk * stride * sizeof(double));
     if ((rc = scr.acquire(workspace, workspace_bytes, buf_bytes + align_up(plan->work), s))) return rc;
-    float* buf = reinterpret_cast<float*>(scr.base());
+    double* buf = reinterpret_cast<double*>(scr.base());
     void* work = scr.base() + buf_bytes;
-    // fbpParallel.cu:59 / fbp.cu:103 scale, with the 1/N of the unnormalised C2R
     double scale = M_PI / (double)g.nview * (double)g.du / (fan ? (double)g.dso : 1.0) / N;
     for (size_t r0 = 0; r0 < rows; r0 += chunk) {
         size_t nr = rows - r0 < chunk ? rows - r0 : chunk;
         dim3 pg((unsigned)((stride + 255) / 256 > 8 ? 8 : (stride + 255) / 256), (unsigned)(nr < 65535 ? nr : 65535),
                 (unsigned)((nr + 65534) / 65535));
-        pad_kernel<<<pg, 256, 0, s>>>(buf, prj + r0 * nu, nu, N, stride, nr, fan ? 1 : 0, g.du, g.off_u);
+        pad_kernel<<<pg, 256, 0, s>>>(buf, prj + r0 * nu, nu, N, stride, nr, fan ? 1 : 0, (double)g.du,
+                                      (double)g.off_u);
         if ((rc = check_launch("pad_kernel"))) return rc;
         {
             std::lock_guard<std::mutex> lk(plan->mu);
@@ -262,25 +489,35 @@ int ramp_filter(float* fprj, const float* prj, const ctp_geometry& g, int geom, 
             cufftSetStream(plan->inv, s);
             cufftSetWorkArea(plan->fwd, work);
             cufftSetWorkArea(plan->inv, work);
-            if (nr != chunk) {
-                // last partial chunk: zero the tail rows so the fixed-batch plan
-                // transforms defined data
-                cudaMemsetAsync(buf + nr * stride, 0, (chunk - nr) * stride * sizeof(float), s);
-            }
-            if (cufftExecR2C(plan->fwd, buf, reinterpret_cast<cufftComplex*>(buf)) != CUFFT_SUCCESS)
-                return set_error(CTP_ERR_CUFFT, "cufftExecR2C failed");
+            if (nr != chunk) cudaMemsetAsync(buf + nr * stride, 0, (chunk - nr) * stride * sizeof(double), s);
+            if (cufftExecD2Z(plan->fwd, buf, reinterpret_cast<cufftDoubleComplex*>(buf)) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecD2Z failed");
             size_t ns = nr * (size_t)M;
-            spectrum_mul_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(reinterpret_cast<float2*>(buf), G, M,
-                                                                           nr, (float)scale);
+            spectrum_mul_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(reinterpret_cast<double2*>(buf), G, M,
+                                                                           nr, scale);
             if ((rc = check_launch("spectrum_mul_kernel"))) return rc;
-            if (cufftExecC2R(plan->inv, reinterpret_cast<cufftComplex*>(buf), buf) != CUFFT_SUCCESS)
-                return set_error(CTP_ERR_CUFFT, "cufftExecC2R failed");
+            if (cufftExecZ2D(plan->inv, reinterpret_cast<cufftDoubleComplex*>(buf), buf) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecZ2D failed");
         }
         size_t no = nr * (size_t)nu;
         crop_kernel<<<(unsigned)((no + 255) / 256), 256, 0, s>>>(fprj + r0 * nu, buf, nu, stride, nr);
         if ((rc = check_launch("crop_kernel"))) return rc;
     }
     return CTP_OK;
+}
+
+}  // namespace
+
+size_t ramp_filter_workspace(const ctp_geometry& g, int, int, unsigned flags) {
+    return (flags & CTP_FLAG_FILTER_EXACT) ? exact_workspace(g) : ref_workspace(g);
+}
+
+int ramp_filter(float* fprj, const float* prj, const ctp_geometry& g, int geom, int filter, unsigned flags,
+                void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
+    if (flags & CTP_FLAG_FILTER_EXACT)
+        return ramp_filter_exact(fprj, prj, g, geom, filter, workspace, workspace_bytes, s);
+    return ramp_filter_reference(fprj, prj, g, geom, filter, workspace, workspace_bytes, s);
 }
 
 // ------------------------------------------------------------------ fbp_bp

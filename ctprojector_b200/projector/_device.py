@@ -155,15 +155,16 @@ def dd_nnz(p, angles, geom: int, image_shape=None) -> int:
 
 
 # --------------------------------------------------------------------------- filters
-def ramp_filter(p, prj, filter_type: str, geom: int, out=None, stream=None):
+def ramp_filter(p, prj, filter_type: str, geom: int, out=None, stream=None, exact=False):
     t = as_tensor(prj, lowp_ok=False)
     nb, nview, nv, nu = t.shape
     du = fan_da(p) if geom == _lib.GEOM_FAN else float(p.du)
     g = make_geometry(p, nb, (1, 1, 1), nu, nv, nview, du, float(p.dsd), float(p.dso))
     fprj = _out(list(t.shape), torch.float32, t.device, out)
     ifilter = filter_code(filter_type)
-    ws, wp, wn = workspace(lib().ctp_ramp_filter_workspace(byref(g), geom, ifilter), t.device)
-    check(lib().ctp_ramp_filter(ptr(fprj), ptr(t), byref(g), geom, ifilter, 0, wp, wn,
+    flags = _lib.FLAG_FILTER_EXACT if exact else 0
+    ws, wp, wn = workspace(lib().ctp_ramp_filter_workspace(byref(g), geom, ifilter, flags), t.device)
+    check(lib().ctp_ramp_filter(ptr(fprj), ptr(t), byref(g), geom, ifilter, flags, wp, wn,
                                 stream_handle(stream, t.device)), "ramp_filter")
     return fprj
 

@@ -15,9 +15,11 @@ from .. import _device as D
 from .ct_projector import ct_projector
 
 
-def ramp_filter(projector: ct_projector, prj, filter_type: str = "hann", *, out=None, stream=None):
+def ramp_filter(projector: ct_projector, prj, filter_type: str = "hann", *, exact: bool = False, out=None,
+                stream=None):
     """Filter the projection for equiangular geometry; 'hamming', 'hann', 'cosine', else RL."""
-    return D.like_input(D.ramp_filter(projector, prj, filter_type, _lib.GEOM_FAN, out=out, stream=stream), prj)
+    return D.like_input(D.ramp_filter(projector, prj, filter_type, _lib.GEOM_FAN, out=out, stream=stream,
+                                      exact=exact), prj)
 
 
 def fbp_bp(projector: ct_projector, prj, angles, *, out=None, accumulate=False, stream=None):

@@ -21,13 +21,13 @@ def seed_for(config: int, index: int = 0) -> int:
 
 def ellipse_phantom(rng: np.random.Generator, nx: int, ny: int, dx: float, dy: float, n_ellipses: int = 10,
                     supersample: int = 4) -> np.ndarray:
-    """[ny, nx] float32 phantom in 1/mm."""
+    """[ny, nx] float32 phantom in 1/mm (each shape rasterised inside its
+    bounding box on the super-sampled grid)."""
     R = 0.45 * nx * dx
     ss = supersample
-    xs = (np.arange(nx * ss) + 0.5) / ss * dx - nx * dx / 2
-    ys = (np.arange(ny * ss) + 0.5) / ss * dy - ny * dy / 2
-    X, Y = np.meshgrid(xs, ys)
-    img = np.where(X * X + Y * Y <= R * R, 0.019, 0.0)
+    xs = ((np.arange(nx * ss) + 0.5) / ss * dx - nx * dx / 2).astype(np.float32)
+    ys = ((np.arange(ny * ss) + 0.5) / ss * dy - ny * dy / 2).astype(np.float32)
+    img = np.where(xs[None, :] ** 2 + ys[:, None] ** 2 <= R * R, np.float32(0.019), np.float32(0.0))
     for _ in range(n_ellipses):
         r = 0.6 * R * math.sqrt(rng.uniform())
         t = rng.uniform(0, 2 * math.pi)
@@ -36,9 +36,15 @@ def ellipse_phantom(rng: np.random.Generator, nx: int, ny: int, dx: float, dy: f
         phi = rng.uniform(0, math.pi)
         mu = rng.uniform(0.01, 0.03)
         c, s = math.cos(phi), math.sin(phi)
-        u = (X - x0) * c + (Y - y0) * s
-        v = -(X - x0) * s + (Y - y0) * c
-        img = np.where((u / a) ** 2 + (v / b) ** 2 <= 1, mu, img)
+        ext = max(a, b)
+        i0, i1 = np.searchsorted(xs, x0 - ext), np.searchsorted(xs, x0 + ext)
+        j0, j1 = np.searchsorted(ys, y0 - ext), np.searchsorted(ys, y0 + ext)
+        X = xs[None, i0:i1] - x0
+        Y = ys[j0:j1, None] - y0
+        u = X * c + Y * s
+        v = -X * s + Y * c
+        sub = img[j0:j1, i0:i1]
+        sub[(u / a) ** 2 + (v / b) ** 2 <= 1] = mu
     img = img.reshape(ny, ss, nx, ss).mean(axis=(1, 3))
     return img.astype(np.float32)
 

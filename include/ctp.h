@@ -57,6 +57,8 @@ extern "C" {
 #define CTP_FLAG_IN_FP16 0x20  /* the input array is float16 */
 #define CTP_FLAG_OUT_BF16 0x40 /* the output array is bfloat16 */
 #define CTP_FLAG_OUT_FP16 0x80 /* the output array is float16 */
+#define CTP_FLAG_FILTER_EXACT 0x100 /* ramp filter: FP64 windowed kernel, smooth FFT size
+                                       (default: the reference's FP32 construction) */
 
 /* typeProjector bits of the DD 2D entries, as in the reference
  * (distanceDriven2D.cu:12-25): bit0 FBP weighting, bit1 branchless,
@@ -230,10 +232,14 @@ size_t ctp_dd2d_bp_workspace(const ctp_geometry* g, int geom, int typeProjector,
 int ctp_dd2d_nnz(unsigned long long* nnz_host, const float* deg, const ctp_geometry* g, int geom, void* stream);
 
 /* Ramp filter (fbp.cu:15-162 fan, fbpParallel.cu:14-109 parallel); overwrites
- * fprj.  geom 0 = fan (g->du angular), 1 = parallel. */
+ * fprj.  geom 0 = fan (g->du angular), 1 = parallel.  By default the windowed
+ * ramp is built and applied in FP32 with transforms of length 2nu-1, the
+ * construction of the reference (fbpMath.cu:90-241), which keeps the result
+ * within FP32 rounding of the reference; CTP_FLAG_FILTER_EXACT builds the
+ * kernel in FP64 and filters with a smooth transform size (more accurate). */
 int ctp_ramp_filter(float* fprj, const float* prj, const ctp_geometry* g, int geom, int typeFilter, unsigned flags,
                     void* workspace, size_t workspace_bytes, void* stream);
-size_t ctp_ramp_filter_workspace(const ctp_geometry* g, int geom, int typeFilter);
+size_t ctp_ramp_filter_workspace(const ctp_geometry* g, int geom, int typeFilter, unsigned flags);
 
 /* Pixel-driven fan FBP back projection (fbp.cu:265-359); img += BP. */
 int ctp_fbp_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,

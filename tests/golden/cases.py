@@ -100,4 +100,36 @@ def case_tomo():
     return "tomo", p, dict(img=img, det_center=dc, src=src)
 
 
-ALL = [case_fan_basic, case_fan_offsets, case_par_basic, case_par_offsets, case_kat, case_siddon, case_tomo]
+def case_par_wide():
+    """Full detector width of the parallel benchmark workload (768 cells of
+    0.8 mm) with a coarse image covering it, 24 views."""
+    p = Proj(nx=256, ny=256, nz=1, dx=2.4, dy=2.4, nu=768, nv=1, du=0.8, dv=1.0, nview=24)
+    rng = np.random.default_rng(S.seed_for(107))
+    ang = S.angles(24, np.pi)
+    img = _phantom_stack(rng, 1, 1, 256, 256, 2.4, 2.4)
+    return "par_wide", p, dict(img=img, angles=ang)
+
+
+def case_fan_45():
+    """Full detector width of the fan workload (736 cells of 1.2858 mm), 24
+    views on multiples of 15 degrees -- four of them exactly on 45-degree
+    diagonals, where the reference's hard axis switch follows its fast
+    intrinsic cos/sin (compared with the reference only)."""
+    p = Proj(nx=128, ny=128, nz=1, dx=3.0, dy=3.0, nu=736, nv=1, du=1.2858, dv=1.0, nview=24)
+    rng = np.random.default_rng(S.seed_for(108))
+    ang = S.angles(24, 2 * np.pi)
+    img = _phantom_stack(rng, 1, 1, 128, 128, 3.0, 3.0)
+    return "fan_45", p, dict(img=img, angles=ang)
+
+
+def case_fan_wide():
+    """As fan_45 with the views offset by 0.3 degrees (no exact diagonals)."""
+    p = Proj(nx=128, ny=128, nz=1, dx=3.0, dy=3.0, nu=736, nv=1, du=1.2858, dv=1.0, nview=24)
+    rng = np.random.default_rng(S.seed_for(109))
+    ang = (S.angles(24, 2 * np.pi) + np.float32(np.deg2rad(0.3))).astype(np.float32)
+    img = _phantom_stack(rng, 1, 1, 128, 128, 3.0, 3.0)
+    return "fan_wide", p, dict(img=img, angles=ang)
+
+
+ALL = [case_fan_basic, case_fan_offsets, case_par_basic, case_par_offsets, case_kat, case_siddon, case_tomo,
+       case_par_wide, case_fan_45, case_fan_wide]

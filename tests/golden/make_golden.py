@@ -133,7 +133,7 @@ class Ref:
 def run_case(ref: Ref, fn):
     name, p, inp = fn()
     out = {}
-    if name in ("fan_basic", "fan_offsets", "par_basic", "par_offsets"):
+    if name in ("fan_basic", "fan_offsets", "par_basic", "par_offsets", "par_wide", "fan_45", "fan_wide"):
         fan = name.startswith("fan")
         img, ang = inp["img"], inp["angles"]
         prj = ref.dd_fp(p, img, ang, fan)
@@ -163,10 +163,13 @@ def run_case(ref: Ref, fn):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--only", nargs="*", default=None, help="case names to (re)generate")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     ref = Ref(REF_LIB)
     for fn in cases.ALL:
+        if a.only and fn.__name__[5:] not in a.only:
+            continue
         name, arrays = run_case(ref, fn)
         path = os.path.join(a.out, f"{name}.npz")
         np.savez_compressed(path, **arrays)

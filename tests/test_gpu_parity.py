@@ -102,7 +102,14 @@ def test_dd_adjoint_identity(name):
     assert abs(lhs - rhs) / (np.linalg.norm(Ax) * np.linalg.norm(y)) <= ADJ_TOL
 
 
-@pytest.mark.parametrize("name", DD_CASES)
+# The default filter replays the reference's FP32 construction of the windowed
+# ramp (length 2nu-1 transforms); its distance to the exact FP64 filter is the
+# reference's own rounding, up to REF_FILTER_TOL on these cases.  The exact
+# mode (FP64 kernel) meets TOL against the oracle.
+REF_FILTER_TOL = 1e-4
+
+
+@pytest.mark.parametrize("name", DD_CASES + ["par_wide", "fan_wide"])
 @pytest.mark.parametrize("ftype", ["hann", "hamming", "cosine", "ramlak"])
 def test_ramp_filter_matches_oracle(name, ftype, oracle):
     p, inp = _case(name)
@@ -110,9 +117,9 @@ def test_ramp_filter_matches_oracle(name, ftype, oracle):
     M = mods(fan)
     geom = "fan" if fan else "parallel"
     prj = oracle.dd_fp(p, inp["img"], inp["angles"], geom)
-    out = host(M.ramp_filter(p, dev(prj), ftype))
     ref = oracle.ramp_filter(p, prj, ftype, geom)
-    assert rel_l2(out, ref) <= TOL
+    assert rel_l2(host(M.ramp_filter(p, dev(prj), ftype, exact=True)), ref) <= TOL
+    assert rel_l2(host(M.ramp_filter(p, dev(prj), ftype)), ref) <= REF_FILTER_TOL
 
 
 @pytest.mark.parametrize("name", ["fan_basic", "fan_offsets"])
@@ -164,7 +171,7 @@ def test_tomo_matches_oracle(oracle):
 
 
 # ----------------------------------------------------------------- vs the reference itself
-@pytest.mark.parametrize("name", DD_CASES + ["kat"])
+@pytest.mark.parametrize("name", DD_CASES + ["kat", "par_wide", "fan_wide", "fan_45"])
 def test_dd_matches_reference_golden(name):
     p, inp, ref = load_golden(name)
     fan = name.startswith("fan")
