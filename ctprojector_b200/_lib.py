@@ -91,6 +91,8 @@ _SIGNATURES = {
     "ctp_dd2d_bp": [_P, _P, _P, _GP, c_int, c_int, c_uint, _P, _S, _P],
     "ctp_dd2d_bp_workspace": [_GP, c_int, c_int, c_uint],
     "ctp_dd2d_nnz": [POINTER(c_ulonglong), _P, _GP, c_int, _P],
+    "ctp_dd2d_fp_noalloc": [_P, _P, _P, _GP, c_int, c_int, c_uint, _P],
+    "ctp_dd2d_fp_noalloc_capacity": [],
     "ctp_ramp_filter": [_P, _P, _GP, c_int, c_int, c_uint, _P, _S, _P],
     "ctp_ramp_filter_workspace": [_GP, c_int, c_int, c_uint],
     "ctp_fbp_fan_bp": [_P, _P, _P, _GP, c_uint, _P],
@@ -106,6 +108,7 @@ _RESTYPE = {
     "ctpVersion": c_char_p,
     "ctp_dd2d_fp_workspace": c_size_t,
     "ctp_dd2d_bp_workspace": c_size_t,
+    "ctp_dd2d_fp_noalloc_capacity": c_size_t,
     "ctp_ramp_filter_workspace": c_size_t,
     "ctp_tomo_bp_workspace": c_size_t,
 }

@@ -17,6 +17,8 @@ size_t dd2d_fp_workspace(const ctp_geometry&, int, int, unsigned);
 int dd2d_bp(void*, const void*, const float*, const ctp_geometry&, int, int, unsigned, void*, size_t, cudaStream_t);
 size_t dd2d_bp_workspace(const ctp_geometry&, int, int, unsigned);
 int dd2d_nnz(unsigned long long*, const float*, const ctp_geometry&, int, cudaStream_t);
+int dd2d_fp_noalloc(void*, const void*, const float*, const ctp_geometry&, int, int, unsigned, cudaStream_t);
+size_t dd2d_fp_noalloc_capacity();
 int ramp_filter(float*, const float*, const ctp_geometry&, int, int, unsigned, void*, size_t, cudaStream_t);
 size_t ramp_filter_workspace(const ctp_geometry&, int, int, unsigned);
 int fbp_fan_bp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
@@ -505,6 +507,17 @@ int ctp_dd2d_bp(void* img, const void* prj, const float* deg, const ctp_geometry
 size_t ctp_dd2d_bp_workspace(const ctp_geometry* g, int geom, int typeProjector, unsigned flags) {
     return g ? dd2d_bp_workspace(*g, geom, typeProjector, flags) : 0;
 }
+
+int ctp_dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geometry* g, int geom,
+                        int typeProjector, unsigned flags, void* stream) {
+    int rc = check_geometry(g, true, true);
+    if (rc) return rc;
+    if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    return dd2d_fp_noalloc(prj, img, deg, *g, geom, typeProjector, flags, as_stream(stream));
+}
+
+size_t ctp_dd2d_fp_noalloc_capacity(void) { return dd2d_fp_noalloc_capacity(); }
 
 int ctp_dd2d_nnz(unsigned long long* nnz_host, const float* deg, const ctp_geometry* g, int geom, void* stream) {
     int rc = check_geometry(g, true, true);

@@ -32,6 +32,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "ctp_common.cuh"
 
@@ -1206,5 +1207,64 @@ int dd2d_bp(void* img, const void* prj, const float* deg, const ctp_geometry& g,
         return launch_bp<__half, float>(img, prj, deg, g, geom, type, flags, scr.base(), s);
     return set_error(CTP_ERR_UNSUPPORTED, "dd2d_bp: unsupported storage type combination (flags 0x%x)", flags);
 }
+
+// ---------------------------------------------------------------------------
+// Forward projection without any allocation.
+//
+// Some callers cannot allocate device memory at call time: a process whose GPU
+// memory is owned by another allocator (frameworks that reserve most of the
+// device at start-up, so a cudaMalloc from inside their custom ops fails or
+// fragments their pool), or an acquisition/reconstruction service that
+// forbids allocation once it is running.  For them, this variant of the DD
+// forward projector takes its scratch (the edge table and the transposed
+// image) from a fixed array in the library's device memory instead of the
+// caller's workspace or the stream-ordered pool.  Every GPU that loads the
+// library holds the array until the process exits.  All calls on a device
+// share it, so calls that overlap on that GPU (for example from two streams)
+// race and must be ordered by the caller; nothing in it needs to start at
+// zero, because every call rewrites all the scratch it reads.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+
+static __device__ __align__(256) unsigned char g_fp_scratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_fp_scratch_mu;
+void* g_fp_scratch_addr[256] = {nullptr};
+}  // namespace
+
+// Device address of g_fp_scratch on the current device, looked up once per
+// device (the host-side symbol is only a stand-in, not a device address).
+static int fp_scratch_address(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error((int)e, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= 256) return set_error(CTP_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_fp_scratch_mu);
+    if (!g_fp_scratch_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_fp_scratch);
+        if (e != cudaSuccess)
+            return set_error((int)e, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+        g_fp_scratch_addr[dev] = p;
+    }
+    *out = g_fp_scratch_addr[dev];
+    return CTP_OK;
+}
+
+int dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
+                    unsigned flags, cudaStream_t s) {
+    size_t need = fp_workspace(g);
+    if (need > kNoAllocScratchBytes)
+        return set_error(CTP_ERR_TOO_LARGE,
+                         "ctp_dd2d_fp_noalloc needs %zu bytes of scratch; its fixed buffer holds %zu "
+                         "(use ctp_dd2d_fp with a workspace)",
+                         need, kNoAllocScratchBytes);
+    void* scratch = nullptr;
+    int rc = fp_scratch_address(&scratch);
+    if (rc) return rc;
+    return dd2d_fp(prj, img, deg, g, geom, type, flags, scratch, kNoAllocScratchBytes, s);
+}
+
+size_t dd2d_fp_noalloc_capacity() { return kNoAllocScratchBytes; }
 
 }  // namespace ctp

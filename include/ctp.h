@@ -227,6 +227,21 @@ int ctp_dd2d_bp(void* img, const void* prj, const float* deg, const ctp_geometry
                 unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
 size_t ctp_dd2d_bp_workspace(const ctp_geometry* g, int geom, int typeProjector, unsigned flags);
 
+/* The DD forward projection of ctp_dd2d_fp for callers that cannot allocate
+ * device memory at call time (their GPU memory is owned by another allocator,
+ * or allocation is not allowed once their service runs).  It allocates
+ * nothing: its scratch is a fixed 32 MiB array inside the library's device
+ * memory, held by every GPU that loads the library until the process exits
+ * (ctp_dd2d_fp_noalloc_capacity() returns the size).  Requests needing more
+ * scratch return CTP_ERR_TOO_LARGE.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU race,
+ * so the caller must order them (one stream, or events).  Output semantics and
+ * flags as ctp_dd2d_fp.  This entry has no counterpart in the reference. */
+int ctp_dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geometry* g, int geom,
+                        int typeProjector, unsigned flags, void* stream);
+size_t ctp_dd2d_fp_noalloc_capacity(void);
+
 /* Number of operator nonzeros of the DD forward projector for one batch
  * item (the pixel count of every ray footprint on every main-axis line). */
 int ctp_dd2d_nnz(unsigned long long* nnz_host, const float* deg, const ctp_geometry* g, int geom, void* stream);
