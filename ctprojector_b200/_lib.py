@@ -102,6 +102,9 @@ _SIGNATURES = {
     "ctp_tomo_fp": [_P, _P, _P, _P, _GP, c_uint, _P],
     "ctp_tomo_bp": [_P, _P, _P, _P, _GP, c_uint, _P, _S, _P],
     "ctp_tomo_bp_workspace": [_GP],
+    "cupyTVSQS3D": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F],
+    "cTVSQS3D": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F],
+    "ctp_tv_sqs": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F, _P],
 }
 _RESTYPE = {
     "ctpGetLastErrorString": c_char_p,

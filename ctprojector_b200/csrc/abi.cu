@@ -32,6 +32,8 @@ int tomo_fp(float*, const float*, const float*, const float*, const ctp_geometry
 int tomo_bp(float*, const float*, const float*, const float*, const ctp_geometry&, unsigned, void*, size_t,
             cudaStream_t);
 size_t tomo_bp_workspace(const ctp_geometry&);
+int tv_sqs(float*, float*, float*, const float*, float, float, float, size_t, size_t, size_t, size_t, float,
+           cudaStream_t);
 
 static thread_local char t_err[512] = "";
 
@@ -595,5 +597,33 @@ int ctp_tomo_bp(float* img, const float* prj, const float* detCenter, const floa
 }
 
 size_t ctp_tomo_bp_workspace(const ctp_geometry* g) { return g ? tomo_bp_workspace(*g) : 0; }
+
+// ------------------------------------------------------------ TV prior
+int cupyTVSQS3D(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nBatches,
+                size_t nx, size_t ny, size_t nz, float eps) {
+    return finish_sync(tv_sqs(s1, s2, var, img, wx, wy, wz, nBatches, nx, ny, nz, eps, 0), 0);
+}
+
+int cTVSQS3D(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nBatches,
+             size_t nx, size_t ny, size_t nz, float eps) {
+    if (nBatches == 0) return CTP_OK;
+    if (!s1 || !s2 || !var || !img) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    HostCall hc;
+    size_t n = nBatches * nx * ny * nz;
+    float* dimg = hc.upload(img, n);
+    float* d1 = hc.dev<float>(n);
+    float* d2 = hc.dev<float>(n);
+    float* dv = hc.dev<float>(n);
+    if (!hc.rc) hc.rc = tv_sqs(d1, d2, dv, dimg, wx, wy, wz, nBatches, nx, ny, nz, eps, hc.s);
+    hc.download(s1, d1, n);
+    hc.download(s2, d2, n);
+    hc.download(var, dv, n);
+    return hc.finish();
+}
+
+int ctp_tv_sqs(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nbatch,
+               size_t nx, size_t ny, size_t nz, float eps, void* stream) {
+    return tv_sqs(s1, s2, var, img, wx, wy, wz, nbatch, nx, ny, nz, eps, as_stream(stream));
+}
 
 }  // extern "C"

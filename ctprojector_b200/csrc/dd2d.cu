@@ -32,6 +32,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <climits>
 #include <mutex>
 
 #include "ctp_common.cuh"
@@ -622,14 +623,30 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
 // (distanceDriven2DBoxInt.cu:21-106).
 constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
 
+// Running integral at x' + 1/2 from a midpoint table: entry i holds
+// (C_i + r_i / 2, r_i) with C_i the integral up to cell i, so
+// F(x) = entry.x + r_i (x - 1/2 - i) for the cell i nearest x - 1/2.  The
+// nearest integer comes from the float adder (x' + 1.5*2^23 rounds x' to an
+// integer in the low mantissa bits), which keeps the lookup off the
+// conversion pipe.  x' = x - 1/2 must lie in [-1/2, n - 1/2].
+constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr int kRoundMagicBits = 0x4B400000;
+
+__device__ __forceinline__ float prefix_eval_mid(const float2* __restrict__ T, float xs) {
+    float t = xs + kRoundMagic;
+    int i = __float_as_int(t) - kRoundMagicBits;
+    float2 e = T[i];
+    return fmaf(e.y, xs - (t - kRoundMagic), e.x);
+}
+
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = a + b;
     float bb = s - a;
     e = (a - (s - bb)) + (b - bb);
 }
 
-// Stage kFRows lines (length n, stride n between lines) into prefix tables of
-// n+1 entries {hi, lo, r, 0}: entry i holds the integral over cells [0, i).
+// Stage lines (length n, stride n between lines) into midpoint tables of n+1
+// entries {hi, lo, r, 0}: hi + lo = integral over cells [0, i) plus r_i / 2.
 template <typename Tin>
 __device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ src, int nlines, int n, int warp,
                             int lane, int nwarps) {
@@ -674,7 +691,7 @@ __device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ sr
             int k = k0 + q;
             if (k <= n) {
                 float r = k < n ? ldf(row + k) : 0.f;
-                T[k] = make_float4(bhi, blo, r, 0.f);
+                T[k] = make_float4(bhi, fmaf(0.5f, r, blo), r, 0.f);  // midpoint table
                 float e;
                 two_sum(bhi, r, bhi, e);
                 blo += e;
@@ -683,8 +700,11 @@ __device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ sr
     }
 }
 
-template <bool FAN, typename Tin, typename Tout>
-__global__ void __launch_bounds__(256) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
+// NI = edge groups per warp (compile time, so the group loop is straight-line
+// code with independent dependency chains); groups beyond the CTA's views are
+// harmless dummies whose results are dropped.
+template <bool FAN, int NI, typename Tin, typename Tout>
+__global__ void __launch_bounds__(256, 3) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
                                                            const Tin* __restrict__ imgT, DDTab tab, Grid g, Det d,
                                                            int nview, int vgroup, int nrows_chunk,
                                                            const float* __restrict__ deg, int unweight_par) {
@@ -697,43 +717,37 @@ __global__ void __launch_bounds__(256) dd2d_fp_fast_kernel(Tout* __restrict__ pr
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
     const int nitems = nvg * ipv;
 
-    float res[kFMaxItems];
-#pragma unroll
-    for (int q = 0; q < kFMaxItems; ++q) res[q] = 0.f;
-
     for (int o = 0; o < 2; ++o) {
-        const int n = o == 0 ? g.nx : g.ny;       // cells per line
-        const int nl = o == 0 ? g.ny : g.nx;      // lines
+        const int n = o == 0 ? g.nx : g.ny;   // cells per line
+        const int nl = o == 0 ? g.ny : g.nx;  // lines
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const Tin* src = (o == 0 ? img : imgT) + (size_t)slice * g.nx * g.ny;
-        float A[kFMaxItems], B[kFMaxItems], acc[kFMaxItems];
+        float A[NI], B[NI], acc[NI];
         bool any = false;
 #pragma unroll
-        for (int q = 0; q < kFMaxItems; ++q) {
-            int it = warp + 8 * q;
-            A[q] = B[q] = acc[q] = 0.f;
+        for (int q = 0; q < NI; ++q) {
+            const int it = warp + 8 * q;
+            // dummy edge positions keep every width non-zero
+            A[q] = (float)lane - 0.5f;
+            B[q] = 0.f;
+            acc[q] = 0.f;
             if (it < nitems) {
-                int vi = it / ipv, m = it - vi * ipv;
-                int view = v0 + vi;
-                float wx = tab.wx[view];
-                bool active = o == 0 ? wx > 0.f : wx < 1.f;
-                int j = 31 * m + lane;
+                const int vi = it / ipv, m = it - vi * ipv;
+                const int view = v0 + vi;
+                const float wx = tab.wx[view];
+                const bool active = o == 0 ? wx > 0.f : wx < 1.f;
+                const int j = 31 * m + lane;
                 if (active && j <= d.nu) {
-                    size_t ie = (size_t)view * (d.nu + 1) + j;
-                    A[q] = tab.eA[o][ie];
+                    const size_t ie = (size_t)view * (d.nu + 1) + j;
+                    A[q] = tab.eA[o][ie] - 0.5f;  // shifted for the midpoint tables
                     B[q] = tab.eB[o][ie];
                     any = true;
-                } else {
-                    // edge beyond the detector or view not traced here: a unit
-                    // spacing keeps the (unused) width of its pair non-zero
-                    A[q] = (float)lane;
                 }
             }
         }
-        // every warp must take part in staging whether or not it has work
-        bool cta_any = __syncthreads_or(any);
-        if (!cta_any) continue;
-        const float nf = (float)n;
+        // every warp takes part in staging whether or not it has work
+        if (!__syncthreads_or(any)) continue;
+        const float lo_lim = -0.5f, hi_lim = (float)n - 0.5f;
         for (int l0 = 0; l0 < nl; l0 += nrows_chunk) {
             const int nlc = min(nrows_chunk, nl - l0);
             __syncthreads();
@@ -743,52 +757,51 @@ __global__ void __launch_bounds__(256) dd2d_fp_fast_kernel(Tout* __restrict__ pr
                 const float t = (float)(l0 + r - anchor);
                 const float4* T = s_lines + (size_t)r * (n + 1);
 #pragma unroll
-                for (int q = 0; q < kFMaxItems; ++q) {
-                    if (warp + 8 * q >= nitems) break;
-                    float xr = fmaf(B[q], t, A[q]);
-                    float x = clampf(xr, 0.f, nf);
-                    int i = __float2int_rd(x);
-                    float4 e = T[i];
-                    float hi = e.x, lo = fmaf(e.z, x - (float)i, e.y);
-                    float hin = __shfl_down_sync(0xffffffffu, hi, 1);
-                    float lon = __shfl_down_sync(0xffffffffu, lo, 1);
-                    float xn = __shfl_down_sync(0xffffffffu, xr, 1);
-                    // signed integral over [x_j, x_j+1] divided by the signed
-                    // width of the rounded footprint
+                for (int q = 0; q < NI; ++q) {
+                    const float xr = fmaf(B[q], t, A[q]);  // edge position - 1/2
+                    const float xs = clampf(xr, lo_lim, hi_lim);
+                    const float tt = xs + kRoundMagic;
+                    const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
+                    const float hi = e.x, lo = fmaf(e.z, xs - (tt - kRoundMagic), e.y);
+                    const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
+                    const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
+                    const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
+                    // signed integral over [x_j, x_j+1] over the signed width of
+                    // the rounded footprint
                     acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
                 }
             }
         }
 #pragma unroll
-        for (int q = 0; q < kFMaxItems; ++q) {
-            int it = warp + 8 * q;
-            if (it >= nitems) break;
-            int vi = it / ipv, m = it - vi * ipv;
-            int view = v0 + vi;
-            int k = 31 * m + lane;
-            float wx = tab.wx[view];
-            bool active = o == 0 ? wx > 0.f : wx < 1.f;
-            if (active && lane < 31 && k < d.nu) {
-                size_t ic = (size_t)view * d.nu + k;
-                res[q] += acc[q] * tab.cL[o][ic] * (o == 0 ? wx : 1.f - wx);
-            }
+        for (int q = 0; q < NI; ++q) {
+            const int it = warp + 8 * q;
+            if (it >= nitems) continue;
+            const int vi = it / ipv, m = it - vi * ipv;
+            const int view = v0 + vi;
+            const int k = 31 * m + lane;
+            const float wx = tab.wx[view];
+            const bool active = o == 0 ? wx > 0.f : wx < 1.f;
+            if (!active || lane >= 31 || k >= d.nu) continue;
+            float v = acc[q] * tab.cL[o][(size_t)view * d.nu + k] * (o == 0 ? wx : 1.f - wx);
+            Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + k;
+            if (o == 1 && wx > 0.f) v += rdf(dst);  // the row sweep of this view wrote first
+            stf(dst, v);
         }
     }
-#pragma unroll
-    for (int q = 0; q < kFMaxItems; ++q) {
-        int it = warp + 8 * q;
-        if (it >= nitems) break;
-        int vi = it / ipv, m = it - vi * ipv;
-        int view = v0 + vi;
-        int k = 31 * m + lane;
-        if (lane < 31 && k < d.nu) {
-            float v = res[q];
-            if (unweight_par) {
-                float sn, cs;
-                sincosf(deg[view], &sn, &cs);
-                v /= ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn);
-            }
-            stf(prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + k, v);
+    if (unweight_par) {
+        // FORCE_FBP on parallel FP: cancel the ray-length weight
+        // (ReverseWeightBPParallelKernel, distanceDriven2DUtils.cu:68-94)
+        for (int q = 0; q < NI; ++q) {
+            const int it = warp + 8 * q;
+            if (it >= nitems) continue;
+            const int vi = it / ipv, m = it - vi * ipv;
+            const int view = v0 + vi;
+            const int k = 31 * m + lane;
+            if (lane >= 31 || k >= d.nu) continue;
+            float sn, cs;
+            sincosf(deg[view], &sn, &cs);
+            Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + k;
+            stf(dst, rdf(dst) / (ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn)));
         }
     }
 }
@@ -813,11 +826,6 @@ constexpr int kPViews = 32;    // views per staged chunk
 constexpr int kPMaxWin = 255;  // staged cells per view (table holds win+1 entries)
 constexpr int kPPar = 9;       // per-view parameters in shared memory
 
-__device__ __forceinline__ float prefix_eval(const float2* __restrict__ T, float x) {
-    int i = __float2int_rd(x);
-    float2 e = T[i];
-    return fmaf(e.y, x - (float)i, e.x);
-}
 
 template <typename Tp, typename Tout>
 __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ prj,
@@ -895,11 +903,11 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 int k = k0 + q;
-                if (q < per && k < stride) T[k] = make_float2(base, v[q]);
+                if (q < per && k < stride) T[k] = make_float2(fmaf(0.5f, v[q], base), v[q]);
                 base += v[q];
             }
             if (lane == 0) {
-                s_par[0 * kPViews + vi] = (float)(j00 - w0);
+                s_par[0 * kPViews + vi] = (float)(j00 - w0 - 0.5);  // shifted for prefix_eval_mid
                 s_par[1 * kPViews + vi] = (float)jx;
                 s_par[2 * kPViews + vi] = (float)jy;
                 s_par[3 * kPViews + vi] = (float)hx;
@@ -924,10 +932,10 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
             if (staged) {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    float jc = clampf(fmaf((float)k, dj, jc0), hm, fwin - hm);
+                    float jc = clampf(fmaf((float)k, dj, jc0), hm - 0.5f, fwin - hm - 0.5f);
                     float a = 0.f;
-                    if (sx != 0.f) a = fmaf(prefix_eval(T, jc + hx) - prefix_eval(T, jc - hx), sx, a);
-                    if (sy != 0.f) a = fmaf(prefix_eval(T, jc + hy) - prefix_eval(T, jc - hy), sy, a);
+                    if (sx != 0.f) a = fmaf(prefix_eval_mid(T, jc + hx) - prefix_eval_mid(T, jc - hx), sx, a);
+                    if (sy != 0.f) a = fmaf(prefix_eval_mid(T, jc + hy) - prefix_eval_mid(T, jc - hy), sy, a);
                     acc[k] += a;
                 }
             } else {
@@ -957,6 +965,166 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
             stf(o, a);
         }
     }
+}
+
+// Fan-beam normalised back projection (and FBP weighting), fast path.
+// DDBPFanKernel (distanceDriven2DBoxInt.cu:319-396): per pixel and view, the
+// pixel's x-edges at its centre row (or y-edges at its centre column, by the
+// reference's intrinsic axis switch) are mapped to the detector with
+// atan(rx / (ry + dso)) (distanceDriven2DUtils.cu:96-101) and the pre-weighted
+// row is integrated between them and normalised.  Same tiling and window
+// tables as the parallel fast path; src is the pre-weighted sinogram (or the
+// plain one in FBP mode).
+template <typename Tp, typename Tout>
+__global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ src,
+                                                               const float* __restrict__ deg, int nview, Grid g,
+                                                               Det d, float dso, int fbp, int accumulate, int win) {
+    extern __shared__ float4 smem_f4[];
+    const int stride = win + 1;
+    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                 // [kPViews][stride]
+    float* s_c = reinterpret_cast<float*>(s_tab + kPViews * stride);    // [kPViews]
+    float* s_s = s_c + kPViews;
+    int* s_w0 = reinterpret_cast<int*>(s_s + kPViews);                  // window start, or INT_MIN
+    int* s_ym = s_w0 + kPViews;
+
+    const int tiles_x = (g.nx + kPT - 1) / kPT;
+    const int tx0 = (blockIdx.x % tiles_x) * kPT, ty0 = (blockIdx.x / tiles_x) * kPT;
+    const int iz = blockIdx.y % g.nz, b = blockIdx.y / g.nz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
+    int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);
+    bool row_ok = iv >= 0 && iv < d.nv;
+    const Tp* rows = src + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
+    const size_t vstride = (size_t)d.nv * d.nu;
+    const int ix = tx0 + lane;
+    const float xc = ((float)ix - g.nx / 2.f) * g.dx + g.cx + g.dx / 2;
+    float yc[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) yc[k] = ((float)(ty0 + warp + 8 * k) - g.ny / 2.f) * g.dy + g.cy + g.dy / 2;
+    const float hdx = g.dx / 2.0f, hdy = g.dy / 2.0f;
+    const float jscale = -1.f / d.du, joff = -d.off_u + d.nu / 2.0f;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+
+    for (int v0 = 0; v0 < nview && row_ok; v0 += kPViews) {
+        const int nvc = min(kPViews, nview - v0);
+        for (int vi = warp; vi < nvc; vi += 8) {
+            const int view = v0 + vi;
+            double s, c;
+            sincos((double)deg[view], &s, &c);
+            // window: detector coordinates of the tile's corner edges
+            double xs[2] = {(tx0 - 0.5 * g.nx) * g.dx + g.cx, (tx0 + kPT - 0.5 * g.nx) * g.dx + g.cx};
+            double ys[2] = {(ty0 - 0.5 * g.ny) * g.dy + g.cy, (ty0 + kPT - 0.5 * g.ny) * g.dy + g.cy};
+            double jmin = 1e300, jmax = -1e300;
+            bool ok = true;
+            for (int a = 0; a < 2; ++a)
+                for (int q = 0; q < 2; ++q) {
+                    double ry = -xs[a] * s + ys[q] * c + dso;
+                    if (!(ry > 0)) ok = false;
+                    double j = -(atan((xs[a] * c + ys[q] * s) / ry) / d.du + (double)d.off_u) + 0.5 * d.nu;
+                    jmin = fmin(jmin, j);
+                    jmax = fmax(jmax, j);
+                }
+            int w0 = 0;
+            if (ok && isfinite(jmin) && isfinite(jmax)) {
+                w0 = (int)floor(jmin) - 2;
+                ok = ((int)ceil(jmax) + 2 - w0) <= win;
+            } else {
+                ok = false;
+            }
+            const int per = (stride + 31) / 32;
+            const int k0 = lane * per;
+            float v[8];
+            float run = 0.f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                int k = k0 + q;
+                float x = 0.f;
+                if (ok && q < per && k < win) {
+                    int cell = w0 + k;
+                    if (cell >= 0 && cell < d.nu) x = ldf(rows + (size_t)view * vstride + cell);
+                }
+                v[q] = x;
+                run += x;
+            }
+            float incl = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                float t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            float base = incl - run;
+            float2* T = s_tab + vi * stride;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                int k = k0 + q;
+                if (q < per && k < stride) T[k] = make_float2(fmaf(0.5f, v[q], base), v[q]);
+                base += v[q];
+            }
+            if (lane == 0) {
+                s_c[vi] = (float)c;
+                s_s[vi] = (float)s;
+                s_w0[vi] = ok ? w0 : INT_MIN;
+                s_ym[vi] = ref_y_main(deg[view]) ? 1 : 0;
+            }
+        }
+        __syncthreads();
+        for (int vi = 0; vi < nvc; ++vi) {
+            const float c = s_c[vi], sn = s_s[vi];
+            const int w0 = s_w0[vi];
+            const bool ym = s_ym[vi] != 0;
+            const float2* T = s_tab + vi * stride;
+            const Tp* grow = rows + (size_t)(v0 + vi) * vstride;
+            const float fw0 = (float)w0 + 0.5f;  // window origin, shifted for prefix_eval_mid
+            const float lim = (float)win - 0.5f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float rxc = xc * c + yc[k] * sn;
+                const float ryc = -xc * sn + yc[k] * c;
+                // edge points: x-edges at the centre row, or y-edges at the centre column
+                const float ex = ym ? hdx * c : hdy * sn;
+                const float ey = ym ? -hdx * sn : hdy * c;
+                float a1 = atanf((rxc - ex) / ((ryc - ey) + dso));
+                float a2 = atanf((rxc + ex) / ((ryc + ey) + dso));
+                float j1 = fmaf(a1, jscale, joff), j2 = fmaf(a2, jscale, joff);
+                float lo = fminf(j1, j2), hi = fmaxf(j1, j2);
+                float val;
+                if (w0 != INT_MIN) {
+                    float l = clampf(lo - fw0, -0.5f, lim), h = clampf(hi - fw0, -0.5f, lim);
+                    val = prefix_eval_mid(T, h) - prefix_eval_mid(T, l);
+                } else {
+                    val = box_line(grow, 1, lo, hi, d.nu);
+                }
+                val = __fdividef(val, hi - lo);
+                if (fbp) val *= dso * dso / (rxc * rxc + (dso + ryc) * (dso + ryc));
+                acc[k] += val;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int iy = ty0 + warp + 8 * k;
+        if (ix < g.nx && iy < g.ny) {
+            Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+            float a = acc[k];
+            if (accumulate) a += rdf(o);
+            stf(o, a);
+        }
+    }
+}
+
+// Staged window for the fast fan path: angular size of a 32x32 tile seen from
+// the nearest source position, in cells, or 0 if it does not fit.
+int fan_fast_window(const ctp_geometry& g) {
+    double hx = 0.5 * g.nx * g.dx, hy = 0.5 * g.ny * g.dy;
+    double rmax = sqrt((fabs(g.cx) + hx) * (fabs(g.cx) + hx) + (fabs(g.cy) + hy) * (fabs(g.cy) + hy));
+    double diag = kPT * sqrt((double)g.dx * g.dx + (double)g.dy * g.dy);
+    double near = (double)g.dso - rmax;
+    if (near <= diag) return 0;
+    double cells = 2 * atan(0.5 * diag / near) / fabs((double)g.du);
+    int win = (int)ceil(cells) + 8;
+    return win <= kPMaxWin ? win : 0;
 }
 
 // Staged window for the fast parallel path (cells), or 0 if it does not fit.
@@ -1017,7 +1185,19 @@ bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
         if (fabs(z - (double)iv) > 1e-6) return false;
     }
     int ipv = (int)((g.nu + 30) / 31);
-    vgroup = (kFMaxItems * 8) / ipv;
+    // views per CTA: the largest count whose edge groups fill the warps of one
+    // of the compiled group counts (4, 8, 12, 16 per warp) with the least waste
+    vgroup = 0;
+    double best = 1e30;
+    for (int v = 1; v * ipv <= kFMaxItems * 8; ++v) {
+        int per_warp = (v * ipv + 7) / 8;
+        int ni = per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : per_warp <= 12 ? 12 : 16;
+        double waste = (double)(ni * 8) / (v * ipv) + 0.05 / v;  // prefer more views per staged image
+        if (waste < best) {
+            best = waste;
+            vgroup = v;
+        }
+    }
     if (vgroup < 1) return false;
     size_t line = (std::max(g.nx, g.ny) + 1) * sizeof(float4);
     nrows = 8;
@@ -1040,16 +1220,23 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     if (fp_fast_ok(g, vgroup, nrows)) {
         size_t shm = (size_t)nrows * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
         dim3 fg((unsigned)((g.nview + vgroup - 1) / vgroup), (unsigned)(g.nbatch * g.nz));
-        if (geom == 0) {
-            auto k = dd2d_fp_fast_kernel<true, Tin, Tout>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-            k<<<fg, 256, shm, s>>>(mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g),
-                                   (int)g.nview, vgroup, nrows, deg, unweight);
+        int ipv = (int)((g.nu + 30) / 31);
+        int per_warp = (vgroup * ipv + 7) / 8;
+        auto launch = [&](auto kern) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g),
+                                      (int)g.nview, vgroup, nrows, deg, unweight);
+        };
+        bool fan = geom == 0;
+        if (per_warp <= 4) {
+            if (fan) launch(dd2d_fp_fast_kernel<true, 4, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 4, Tin, Tout>);
+        } else if (per_warp <= 8) {
+            if (fan) launch(dd2d_fp_fast_kernel<true, 8, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 8, Tin, Tout>);
+        } else if (per_warp <= 12) {
+            if (fan) launch(dd2d_fp_fast_kernel<true, 12, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 12, Tin, Tout>);
         } else {
-            auto k = dd2d_fp_fast_kernel<false, Tin, Tout>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-            k<<<fg, 256, shm, s>>>(mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g),
-                                   (int)g.nview, vgroup, nrows, deg, unweight);
+            if (fan) launch(dd2d_fp_fast_kernel<true, 16, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 16, Tin, Tout>);
         }
         return check_launch("dd2d_fp_fast_kernel");
     }
@@ -1149,6 +1336,28 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
     int fbp = (type & (CTP_TYPE_FBP | CTP_TYPE_FORCE_FBP)) ? 1 : 0;
     size_t shm = (size_t)kBPViews * wl * 4 + kBPViews * 5 * 4;
     if (geom == 0) {
+        int fwin = fan_fast_window(g);
+        int tiles_f = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
+        size_t fshm = (size_t)kPViews * (fwin + 1) * sizeof(float2) + 4 * kPViews * 4;
+        dim3 fgrid((unsigned)tiles_f, (unsigned)(g.nbatch * g.nz));
+        if (fwin > 0 && !fbp) {
+            float* wprj = reinterpret_cast<float*>(ws);
+            size_t total = g.nbatch * g.nview * g.nv * g.nu;
+            fan_preweight_kernel<Tin><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(wprj, cptr<Tin>(prj), deg,
+                                                                                    nview, dt, gr, total);
+            if ((rc = check_launch("fan_preweight_kernel"))) return rc;
+            auto kf = dd2d_bp_fan_fast_kernel<float, Tout>;
+            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
+            kf<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), wprj, deg, nview, gr, dt, dso, 0, accumulate, fwin);
+            return check_launch("dd2d_bp_fan_fast_kernel");
+        }
+        if (fwin > 0) {
+            auto kf = dd2d_bp_fan_fast_kernel<Tin, Tout>;
+            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
+            kf<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, 1, accumulate,
+                                        fwin);
+            return check_launch("dd2d_bp_fan_fast_kernel");
+        }
         if (!fbp) {
             float* wprj = reinterpret_cast<float*>(ws);
             size_t total = g.nbatch * g.nview * g.nv * g.nu;

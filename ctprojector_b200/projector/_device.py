@@ -86,7 +86,7 @@ def make_geometry(p, nbatch, image_shape, nu, nv, nview, du, dsd=0.0, dso=0.0) -
 
 def fan_da(p) -> float:
     """Angular cell size passed by the reference fan wrappers (du / dsd)."""
-    return float(np.float32(p.du) / np.float32(p.dsd))
+    return float(np.float32(p.du / p.dsd))
 
 
 def _out(shape, dtype, device, out):

@@ -210,6 +210,16 @@ int cfbpFanBackprojection(float* pImg, const float* pPrj, const float* pDeg, siz
                           size_t nv, size_t nview, float da, float dv, float off_a, float off_v, float dsd,
                           float dso);
 
+/* TotalVariation.cu:185 (cupy*) / :213 (c*) of the reference prior library
+ * (libprior.so): SQS surrogate terms of the anisotropic TV prior.  s1, s2 and
+ * var are [nBatches][nz][ny][nx]; wx, wy, wz weight the x, y, z differences.
+ * (The reference host entry sizes its buffers for one batch item; this one
+ * handles every item.) */
+int cupyTVSQS3D(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nBatches,
+                size_t nx, size_t ny, size_t nz, float eps);
+int cTVSQS3D(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nBatches,
+             size_t nx, size_t ny, size_t nz, float eps);
+
 /* ======================================================================== */
 /* 2. Extended entries: explicit stream, workspace and flags                */
 /* ======================================================================== */
@@ -274,6 +284,10 @@ int ctp_tomo_fp(float* prj, const float* img, const float* detCenter, const floa
 int ctp_tomo_bp(float* img, const float* prj, const float* detCenter, const float* src, const ctp_geometry* g,
                 unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
 size_t ctp_tomo_bp_workspace(const ctp_geometry* g);
+
+/* TV-SQS surrogate terms (TotalVariation.cu:21-149) on a stream. */
+int ctp_tv_sqs(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nbatch,
+               size_t nx, size_t ny, size_t nz, float eps, void* stream);
 
 #ifdef __cplusplus
 }

@@ -104,8 +104,8 @@ def _ptr(a, t=c_double):
 
 
 def _fan_da(p):
-    # The reference wrappers pass the angular cell size du / dsd in float32.
-    return float(np.float32(np.float32(p.du) / np.float32(p.dsd)))
+    # The reference wrappers pass c_float(projector.du / projector.dsd).
+    return float(np.float32(p.du / p.dsd))
 
 
 # --------------------------------------------------------------------------- DD 2D
@@ -281,3 +281,33 @@ def ramp_filter(p, prj, filter_type: str = "hann", geom: str = "parallel"):
     G = np.fft.rfft(g, n=n)
     full = np.fft.irfft(X * G, n=n, axis=-1)
     return full[..., nu - 1: 2 * nu - 1] * scale
+
+
+# --------------------------------------------------------------------------- TV prior
+def tv_sqs(img, weights, eps=1e-8):
+    """SQS terms of the anisotropic TV prior, kernel/prior/cuda/TotalVariation.cu:21-149
+    of the reference.  weights along (z, y, x); img [batch, nz, ny, nx]."""
+    x = _d(img)
+    wz, wy, wx = (float(np.float32(w)) for w in weights)
+    dx = np.zeros_like(x)
+    dy = np.zeros_like(x)
+    dz = np.zeros_like(x)
+    dx[..., 1:] = x[..., 1:] - x[..., :-1]
+    dy[..., 1:, :] = x[..., 1:, :] - x[..., :-1, :]
+    dz[..., 1:, :, :] = x[..., 1:, :, :] - x[..., :-1, :, :]
+    var = np.sqrt(wx * dx * dx + wy * dy * dy + wz * dz * dz + float(np.float32(eps)))
+    dx1 = np.zeros_like(x)
+    dy1 = np.zeros_like(x)
+    dz1 = np.zeros_like(x)
+    dx1[..., :-1] = x[..., :-1] - x[..., 1:]
+    dy1[..., :-1, :] = x[..., :-1, :] - x[..., 1:, :]
+    dz1[..., :-1, :, :] = x[..., :-1, :, :] - x[..., 1:, :, :]
+    varx = var.copy()
+    vary = var.copy()
+    varz = var.copy()
+    varx[..., :-1] = var[..., 1:]
+    vary[..., :-1, :] = var[..., 1:, :]
+    varz[..., :-1, :, :] = var[..., 1:, :, :]
+    s1 = (wx * dx + wy * dy + wz * dz) / var + wx * dx1 / varx + wy * dy1 / vary + wz * dz1 / varz
+    s2 = (wx + wy + wz) / var + wx / varx + wy / vary + wz / varz
+    return s1, s2, var
