@@ -32,6 +32,8 @@ int tomo_fp(float*, const float*, const float*, const float*, const ctp_geometry
 int tomo_bp(float*, const float*, const float*, const float*, const ctp_geometry&, unsigned, void*, size_t,
             cudaStream_t);
 size_t tomo_bp_workspace(const ctp_geometry&);
+int sqs_tv_update(float*, void*, const float*, const float*, const float*, size_t, const unsigned char*, float, float,
+                  float, float, float, size_t, size_t, size_t, unsigned, cudaStream_t);
 int tv_sqs(float*, float*, float*, const float*, float, float, float, size_t, size_t, size_t, size_t, float,
            cudaStream_t);
 
@@ -624,6 +626,13 @@ int cTVSQS3D(float* s1, float* s2, float* var, const float* img, float wx, float
 int ctp_tv_sqs(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nbatch,
                size_t nx, size_t ny, size_t nz, float eps, void* stream) {
     return tv_sqs(s1, s2, var, img, wx, wy, wz, nbatch, nx, ny, nz, eps, as_stream(stream));
+}
+
+int ctp_sqs_tv_update(float* x_out, void* x_lp, const float* x, const float* bp, const float* norm,
+                      size_t norm_slices, const unsigned char* zlink, float wx, float wy, float wz, float beta,
+                      float eps, size_t nx, size_t ny, size_t nslices, unsigned flags, void* stream) {
+    return sqs_tv_update(x_out, x_lp, x, bp, norm, norm_slices, zlink, wx, wy, wz, beta, eps, nx, ny, nslices, flags,
+                         as_stream(stream));
 }
 
 }  // extern "C"

@@ -809,23 +809,39 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_fast_kernel(Tout* __restrict__
 // ---------------------------------------------------------------------------
 // Parallel-beam normalised back projection, fast path.
 //
-// For a parallel beam the detector footprint of a pixel's x-edges (or
-// y-edges) is symmetric about the detector coordinate of the pixel centre,
-// jc = -((x cos + y sin)/du + off_u) + nu/2, which is linear in (ix, iy); the
-// half widths are dx|cos|/2du and dy|sin|/2du.  So the reference's
-// normalised box integral (DDBPParallelKernel, distanceDriven2DBoxInt.cu:
-// 409-497) is F(jc + h) - F(jc - h) over 2h, where F is the running integral
-// of the detector row.  A CTA owns a 32x32 pixel tile; per chunk of views each
-// warp stages, for one view at a time, the window of cells the tile projects
-// onto as a table of (prefix sum, cell value) pairs -- prefix sums local to the
-// window, so they stay small and FP32 keeps them accurate -- and every thread
-// then evaluates 4 pixels x 2 table reads per view.  No atomics, no loops over
-// cells.
+// For a parallel beam the detector coordinate of a pixel centre,
+// jc = -((x cos + y sin)/du + off_u) + nu/2, is linear in (ix, iy) with steps
+// jx = -dx cos/du and jy = -dy sin/du, and the footprint of the pixel's
+// x-edges is [jc - |jx|/2, jc + |jx|/2] (of its y-edges, jc -+ |jy|/2).  The
+// reference's normalised box integral (DDBPParallelKernel,
+// distanceDriven2DBoxInt.cu:409-497) is then (F(e1) - F(e0)) / (e1 - e0) with
+// F the running integral of the detector row, and neighbouring pixels share
+// footprint edges: pixels ix and ix+1 meet at jc + jx/2.  So a thread that
+// owns 4 consecutive pixels along x evaluates F at 5 edges for the x-edge
+// term, and one that owns 4 consecutive pixels along y does the same for the
+// y-edge term.  Each thread holds one pixel run of each kind (x-layout and
+// y-layout accumulators) and the two are added through shared memory at the
+// end.
+//
+// A CTA owns a 32x32 tile of one slice.  Per chunk of 32 views: one thread per
+// view computes the view's constants in FP64 (tile-origin coordinate, steps,
+// blend weights, staged window); each warp then stages, for its views, the
+// window of cells the tile projects onto as a midpoint table of window-local
+// running sums (small, so FP32 keeps them accurate); then every thread adds
+// the views to its 8 pixels with table lookups only.  No atomics.
 constexpr int kPT = 32;        // tile edge
 constexpr int kPViews = 32;    // views per staged chunk
 constexpr int kPMaxWin = 255;  // staged cells per view (table holds win+1 entries)
-constexpr int kPPar = 9;       // per-view parameters in shared memory
 
+struct ParView {
+    float jb, jx, jy, sx;  // jb: window coordinate - 1/2 of the tile's first pixel centre
+    float sy, jc, hx, hy;  // sx, sy: signed normalisations (0 = term inactive); jc: absolute coordinate
+};
+
+inline size_t par_fast_smem(int win) {
+    return (size_t)kPViews * (win + 1) * sizeof(float2) + kPViews * sizeof(ParView) + kPViews * sizeof(int) +
+           kPT * (kPT + 1) * sizeof(float);
+}
 
 template <typename Tp, typename Tout>
 __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ prj,
@@ -833,27 +849,32 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
                                                                Det d, int fbp, int accumulate, int win) {
     extern __shared__ float4 smem_f4[];
     const int stride = win + 1;
-    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                   // [kPViews][stride]
-    float* s_par = reinterpret_cast<float*>(s_tab + kPViews * stride);    // [kPPar][kPViews]
-    int* s_w0 = reinterpret_cast<int*>(s_par + kPPar * kPViews);          // [kPViews], -1 << 30 = not staged
+    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                  // [kPViews][stride]
+    ParView* s_par = reinterpret_cast<ParView*>(s_tab + kPViews * stride);  // 16-byte aligned: 256 * stride bytes before
+    int* s_w0 = reinterpret_cast<int*>(s_par + kPViews);                 // window start, INT_MIN = not staged
+    float* s_acc = reinterpret_cast<float*>(s_w0 + kPViews);             // [kPT][kPT + 1] merge buffer
 
     const int tiles_x = (g.nx + kPT - 1) / kPT;
     const int tx0 = (blockIdx.x % tiles_x) * kPT, ty0 = (blockIdx.x / tiles_x) * kPT;
     const int iz = blockIdx.y % g.nz, b = blockIdx.y / g.nz;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // x-layout: 4 pixels along x; a half warp spans 16 columns x 4 rows, so its
+    // table reads fall on distinct banks.  y-layout: 4 pixels along y, lane = column.
+    const int xl_row = warp * 4 + ((lane >> 2) & 3);
+    const int xl_col = ((lane >> 4) * 4 + (lane & 3)) * 4;
+    const int yl_col = lane, yl_row = warp * 4;
 
     float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
     int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);  // truncation, :383
     bool row_ok = iv >= 0 && iv < d.nv;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
     const Tp* rows = prj + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
     const size_t vstride = (size_t)d.nv * d.nu;
-    const float fwin = (float)win;
 
     for (int v0 = 0; v0 < nview && row_ok; v0 += kPViews) {
         const int nvc = min(kPViews, nview - v0);
-        for (int vi = warp; vi < nvc; vi += 8) {
-            const int view = v0 + vi;
+        if (threadIdx.x < nvc) {
+            const int vi = threadIdx.x, view = v0 + vi;
             double s, c;
             sincos((double)deg[view], &s, &c);
             const double du = d.du;
@@ -873,10 +894,28 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
             bool ok = isfinite(j00) && isfinite(hm);
             int w0 = 0;
             if (ok) {
+                // two spare cells on each side: every edge lookup lands in [1.5, win - 2.5]
                 w0 = (int)floor(jmin - hm) - 2;
                 ok = ((int)ceil(jmax + hm) + 2 - w0) <= win;
             }
-            // stage (prefix, value) for window cells w0 .. w0+win-1, entry win = (total, 0)
+            ParView P;
+            P.jb = (float)(j00 - w0 - 0.5);
+            P.jx = (float)jx;
+            P.jy = (float)jy;
+            P.sx = ya ? (float)(pw * wx / jx) : 0.f;
+            P.sy = xa ? (float)(pw * (1 - wx) / jy) : 0.f;
+            P.jc = (float)j00;
+            P.hx = (float)hx;
+            P.hy = (float)hy;
+            s_par[vi] = P;
+            s_w0[vi] = ok ? w0 : INT_MIN;
+        }
+        __syncthreads();
+        // stage (running sum + value/2, value) for window cells w0 .. w0+win-1; entry win = (total, 0)
+        for (int vi = warp; vi < nvc; vi += 8) {
+            const int w0 = s_w0[vi];
+            const bool ok = w0 != INT_MIN;
+            const int view = v0 + vi;
             const int per = (stride + 31) / 32;
             const int k0 = lane * per;
             float v[8];
@@ -906,61 +945,60 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
                 if (q < per && k < stride) T[k] = make_float2(fmaf(0.5f, v[q], base), v[q]);
                 base += v[q];
             }
-            if (lane == 0) {
-                s_par[0 * kPViews + vi] = (float)(j00 - w0 - 0.5);  // shifted for prefix_eval_mid
-                s_par[1 * kPViews + vi] = (float)jx;
-                s_par[2 * kPViews + vi] = (float)jy;
-                s_par[3 * kPViews + vi] = (float)hx;
-                s_par[4 * kPViews + vi] = (float)hy;
-                s_par[5 * kPViews + vi] = ya ? (float)(pw * wx / (2 * hx)) : 0.f;
-                s_par[6 * kPViews + vi] = xa ? (float)(pw * (1 - wx) / (2 * hy)) : 0.f;
-                s_par[7 * kPViews + vi] = (float)hm;
-                s_par[8 * kPViews + vi] = (float)j00;
-                s_w0[vi] = ok ? w0 : (-1 << 30);
-            }
         }
         __syncthreads();
         for (int vi = 0; vi < nvc; ++vi) {
-            const float jb = s_par[vi], jx = s_par[kPViews + vi], jy = s_par[2 * kPViews + vi];
-            const float hx = s_par[3 * kPViews + vi], hy = s_par[4 * kPViews + vi];
-            const float sx = s_par[5 * kPViews + vi], sy = s_par[6 * kPViews + vi];
-            const float hm = s_par[7 * kPViews + vi];
+            const ParView P = s_par[vi];
             const float2* T = s_tab + vi * stride;
-            const bool staged = s_w0[vi] != (-1 << 30);
-            const float jc0 = fmaf((float)lane, jx, fmaf((float)warp, jy, jb));
-            const float dj = 8.f * jy;
-            if (staged) {
+            if (s_w0[vi] != INT_MIN) {
+                if (P.sx != 0.f) {
+                    const float e0 = fmaf((float)xl_col - 0.5f, P.jx, fmaf((float)xl_row, P.jy, P.jb));
+                    float f[5];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    float jc = clampf(fmaf((float)k, dj, jc0), hm - 0.5f, fwin - hm - 0.5f);
-                    float a = 0.f;
-                    if (sx != 0.f) a = fmaf(prefix_eval_mid(T, jc + hx) - prefix_eval_mid(T, jc - hx), sx, a);
-                    if (sy != 0.f) a = fmaf(prefix_eval_mid(T, jc + hy) - prefix_eval_mid(T, jc - hy), sy, a);
-                    acc[k] += a;
+                    for (int k = 0; k < 5; ++k) f[k] = prefix_eval_mid(T, fmaf((float)k, P.jx, e0));
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) ax[k] = fmaf(f[k + 1] - f[k], P.sx, ax[k]);
+                }
+                if (P.sy != 0.f) {
+                    const float e0 = fmaf((float)yl_row - 0.5f, P.jy, fmaf((float)yl_col, P.jx, P.jb));
+                    float f[5];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) f[k] = prefix_eval_mid(T, fmaf((float)k, P.jy, e0));
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) ay[k] = fmaf(f[k + 1] - f[k], P.sy, ay[k]);
                 }
             } else {
                 // window larger than the staging buffer: integrate the row in global memory
                 const Tp* grow = rows + (size_t)(v0 + vi) * vstride;
-                const float jabs0 = s_par[8 * kPViews + vi] + (float)lane * jx + (float)warp * jy;
+                if (P.sx != 0.f) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    float jc = jabs0 + (float)k * dj;
-                    float a = 0.f;
-                    if (sx != 0.f) a += box_line(grow, 1, jc - hx, jc + hx, d.nu) * sx;
-                    if (sy != 0.f) a += box_line(grow, 1, jc - hy, jc + hy, d.nu) * sy;
-                    acc[k] += a;
+                    for (int k = 0; k < 4; ++k) {
+                        float jc = P.jc + (float)(xl_col + k) * P.jx + (float)xl_row * P.jy;
+                        ax[k] += box_line(grow, 1, jc - P.hx, jc + P.hx, d.nu) * fabsf(P.sx);
+                    }
+                }
+                if (P.sy != 0.f) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        float jc = P.jc + (float)yl_col * P.jx + (float)(yl_row + k) * P.jy;
+                        ay[k] += box_line(grow, 1, jc - P.hy, jc + P.hy, d.nu) * fabsf(P.sy);
+                    }
                 }
             }
         }
         __syncthreads();
     }
-    const int ix = tx0 + lane;
+    // add the x-layout sums to the y-layout ones and store rows coalesced
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s_acc[xl_row * (kPT + 1) + xl_col + k] = ax[k];
+    __syncthreads();
+    const int ix = tx0 + yl_col;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        int iy = ty0 + warp + 8 * k;
+        int iy = ty0 + yl_row + k;
         if (ix < g.nx && iy < g.ny) {
             Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
-            float a = acc[k];
+            float a = ay[k] + s_acc[(yl_row + k) * (kPT + 1) + yl_col];
             if (accumulate) a += rdf(o);
             stf(o, a);
         }
@@ -972,44 +1010,60 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
 // pixel's x-edges at its centre row (or y-edges at its centre column, by the
 // reference's intrinsic axis switch) are mapped to the detector with
 // atan(rx / (ry + dso)) (distanceDriven2DUtils.cu:96-101) and the pre-weighted
-// row is integrated between them and normalised.  Same tiling and window
+// row is integrated between them and normalised by the mapped width.  Pixels
+// next to each other along the switched axis share an edge point, so a thread
+// owning 4 consecutive pixels along that axis maps 5 edge points, not 8: the
+// x-layout of the parallel path for x-edge views, the y-layout for y-edge
+// views, merged through shared memory at the end.  Same tiling and window
 // tables as the parallel fast path; src is the pre-weighted sinogram (or the
 // plain one in FBP mode).
+struct FanView {
+    float c, s;
+    int w0;  // window start, INT_MIN = not staged
+    int ym;  // x-edges at the centre row (1) or y-edges at the centre column (0)
+};
+
+inline size_t fan_fast_smem(int win) {
+    return (size_t)kPViews * (win + 1) * sizeof(float2) + kPViews * sizeof(FanView) + kPT * (kPT + 1) * sizeof(float);
+}
+
 template <typename Tp, typename Tout>
 __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ src,
                                                                const float* __restrict__ deg, int nview, Grid g,
                                                                Det d, float dso, int fbp, int accumulate, int win) {
     extern __shared__ float4 smem_f4[];
     const int stride = win + 1;
-    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                 // [kPViews][stride]
-    float* s_c = reinterpret_cast<float*>(s_tab + kPViews * stride);    // [kPViews]
-    float* s_s = s_c + kPViews;
-    int* s_w0 = reinterpret_cast<int*>(s_s + kPViews);                  // window start, or INT_MIN
-    int* s_ym = s_w0 + kPViews;
+    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                    // [kPViews][stride]
+    FanView* s_view = reinterpret_cast<FanView*>(s_tab + kPViews * stride);
+    float* s_acc = reinterpret_cast<float*>(s_view + kPViews);             // [kPT][kPT + 1] merge buffer
 
     const int tiles_x = (g.nx + kPT - 1) / kPT;
     const int tx0 = (blockIdx.x % tiles_x) * kPT, ty0 = (blockIdx.x / tiles_x) * kPT;
     const int iz = blockIdx.y % g.nz, b = blockIdx.y / g.nz;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int xl_row = warp * 4 + ((lane >> 2) & 3);
+    const int xl_col = ((lane >> 4) * 4 + (lane & 3)) * 4;
+    const int yl_col = lane, yl_row = warp * 4;
 
     float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
     int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);
     bool row_ok = iv >= 0 && iv < d.nv;
     const Tp* rows = src + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
     const size_t vstride = (size_t)d.nv * d.nu;
-    const int ix = tx0 + lane;
-    const float xc = ((float)ix - g.nx / 2.f) * g.dx + g.cx + g.dx / 2;
-    float yc[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) yc[k] = ((float)(ty0 + warp + 8 * k) - g.ny / 2.f) * g.dy + g.cy + g.dy / 2;
     const float hdx = g.dx / 2.0f, hdy = g.dy / 2.0f;
+    // x-layout: pixel centres (xs0 + k dx, ysx); y-layout: (xsy, ys0 + k dy)
+    const float xs0 = ((float)(tx0 + xl_col) - g.nx / 2.f) * g.dx + g.cx + hdx;
+    const float ysx = ((float)(ty0 + xl_row) - g.ny / 2.f) * g.dy + g.cy + hdy;
+    const float xsy = ((float)(tx0 + yl_col) - g.nx / 2.f) * g.dx + g.cx + hdx;
+    const float ys0 = ((float)(ty0 + yl_row) - g.ny / 2.f) * g.dy + g.cy + hdy;
     const float jscale = -1.f / d.du, joff = -d.off_u + d.nu / 2.0f;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const float dso2 = dso * dso;
+    float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
 
     for (int v0 = 0; v0 < nview && row_ok; v0 += kPViews) {
         const int nvc = min(kPViews, nview - v0);
-        for (int vi = warp; vi < nvc; vi += 8) {
-            const int view = v0 + vi;
+        if (threadIdx.x < nvc) {
+            const int vi = threadIdx.x, view = v0 + vi;
             double s, c;
             sincos((double)deg[view], &s, &c);
             // window: detector coordinates of the tile's corner edges
@@ -1032,6 +1086,18 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
             } else {
                 ok = false;
             }
+            FanView V;
+            V.c = (float)c;
+            V.s = (float)s;
+            V.w0 = ok ? w0 : INT_MIN;
+            V.ym = ref_y_main(deg[view]) ? 1 : 0;
+            s_view[vi] = V;
+        }
+        __syncthreads();
+        for (int vi = warp; vi < nvc; vi += 8) {
+            const int w0 = s_view[vi].w0;
+            const bool ok = w0 != INT_MIN;
+            const int view = v0 + vi;
             const int per = (stride + 31) / 32;
             const int k0 = lane * per;
             float v[8];
@@ -1061,53 +1127,69 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
                 if (q < per && k < stride) T[k] = make_float2(fmaf(0.5f, v[q], base), v[q]);
                 base += v[q];
             }
-            if (lane == 0) {
-                s_c[vi] = (float)c;
-                s_s[vi] = (float)s;
-                s_w0[vi] = ok ? w0 : INT_MIN;
-                s_ym[vi] = ref_y_main(deg[view]) ? 1 : 0;
-            }
         }
         __syncthreads();
         for (int vi = 0; vi < nvc; ++vi) {
-            const float c = s_c[vi], sn = s_s[vi];
-            const int w0 = s_w0[vi];
-            const bool ym = s_ym[vi] != 0;
+            const FanView V = s_view[vi];
             const float2* T = s_tab + vi * stride;
             const Tp* grow = rows + (size_t)(v0 + vi) * vstride;
-            const float fw0 = (float)w0 + 0.5f;  // window origin, shifted for prefix_eval_mid
-            const float lim = (float)win - 0.5f;
+            const float fw0 = (float)V.w0 + 0.5f;  // window origin, shifted for prefix_eval_mid
+            // edge points p_k = p_0 + k * step, k = 0..4, rotated: (rx, ry)
+            float px, py, sx, sy;
+            if (V.ym) {
+                px = xs0 - hdx; py = ysx; sx = g.dx; sy = 0.f;
+            } else {
+                px = xsy; py = ys0 - hdy; sx = 0.f; sy = g.dy;
+            }
+            const float rx0 = px * V.c + py * V.s, ry0 = -px * V.s + py * V.c;
+            const float drx = sx * V.c + sy * V.s, dry = -sx * V.s + sy * V.c;
+            float j[5];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const float rxc = xc * c + yc[k] * sn;
-                const float ryc = -xc * sn + yc[k] * c;
-                // edge points: x-edges at the centre row, or y-edges at the centre column
-                const float ex = ym ? hdx * c : hdy * sn;
-                const float ey = ym ? -hdx * sn : hdy * c;
-                float a1 = atanf((rxc - ex) / ((ryc - ey) + dso));
-                float a2 = atanf((rxc + ex) / ((ryc + ey) + dso));
-                float j1 = fmaf(a1, jscale, joff), j2 = fmaf(a2, jscale, joff);
-                float lo = fminf(j1, j2), hi = fmaxf(j1, j2);
-                float val;
-                if (w0 != INT_MIN) {
-                    float l = clampf(lo - fw0, -0.5f, lim), h = clampf(hi - fw0, -0.5f, lim);
-                    val = prefix_eval_mid(T, h) - prefix_eval_mid(T, l);
-                } else {
-                    val = box_line(grow, 1, lo, hi, d.nu);
+            for (int k = 0; k < 5; ++k) {
+                const float rx = fmaf((float)k, drx, rx0), ry = fmaf((float)k, dry, ry0);
+                j[k] = fmaf(atanf(rx / (ry + dso)), jscale, joff);
+            }
+            float val[4];
+            if (V.w0 != INT_MIN) {
+                float f[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) f[k] = prefix_eval_mid(T, j[k] - fw0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) val[k] = __fdividef(f[k + 1] - f[k], j[k + 1] - j[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float lo = fminf(j[k], j[k + 1]), hi = fmaxf(j[k], j[k + 1]);
+                    val[k] = __fdividef(box_line(grow, 1, lo, hi, d.nu), hi - lo);
                 }
-                val = __fdividef(val, hi - lo);
-                if (fbp) val *= dso * dso / (rxc * rxc + (dso + ryc) * (dso + ryc));
-                acc[k] += val;
+            }
+            if (fbp) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float rxc = fmaf((float)k + 0.5f, drx, rx0), ryc = fmaf((float)k + 0.5f, dry, ry0);
+                    val[k] *= dso2 / (rxc * rxc + (dso + ryc) * (dso + ryc));
+                }
+            }
+            if (V.ym) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) ax[k] += val[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) ay[k] += val[k];
             }
         }
         __syncthreads();
     }
 #pragma unroll
+    for (int k = 0; k < 4; ++k) s_acc[xl_row * (kPT + 1) + xl_col + k] = ax[k];
+    __syncthreads();
+    const int ix = tx0 + yl_col;
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-        int iy = ty0 + warp + 8 * k;
+        int iy = ty0 + yl_row + k;
         if (ix < g.nx && iy < g.ny) {
             Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
-            float a = acc[k];
+            float a = ay[k] + s_acc[(yl_row + k) * (kPT + 1) + yl_col];
             if (accumulate) a += rdf(o);
             stf(o, a);
         }
@@ -1338,7 +1420,7 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
     if (geom == 0) {
         int fwin = fan_fast_window(g);
         int tiles_f = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
-        size_t fshm = (size_t)kPViews * (fwin + 1) * sizeof(float2) + 4 * kPViews * 4;
+        size_t fshm = fan_fast_smem(fwin);
         dim3 fgrid((unsigned)tiles_f, (unsigned)(g.nbatch * g.nz));
         if (fwin > 0 && !fbp) {
             float* wprj = reinterpret_cast<float*>(ws);
@@ -1376,7 +1458,7 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
         int pwin = par_fast_window(g);
         if (pwin > 0) {
             int tiles_p = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
-            size_t pshm = (size_t)kPViews * (pwin + 1) * sizeof(float2) + kPPar * kPViews * 4 + kPViews * 4;
+            size_t pshm = par_fast_smem(pwin);
             auto kf = dd2d_bp_par_fast_kernel<Tin, Tout>;
             cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
             kf<<<dim3((unsigned)tiles_p, (unsigned)(g.nbatch * g.nz)), 256, pshm, s>>>(

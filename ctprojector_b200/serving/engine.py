@@ -1,0 +1,524 @@
+"""Continuous-batching reconstruction server on one GPU.
+
+Jobs (an FBP or an SQS-TV reconstruction of one scan) arrive over time.  Jobs
+whose scan protocol (geometry + algorithm) is the same share a *lane*: one set
+of device-resident buffers with a fixed number of slots (image slices for the
+fan/parallel protocols, volumes for cone), its own CUDA stream and captured
+CUDA graphs.  Each pass of the server loop
+
+1. moves arrived jobs to the arrival queue,
+2. admits queued jobs into free slots (creating a lane if the HBM budget
+   allows it, after tearing down idle lanes), uploading their sinograms on the
+   lane's stream,
+3. advances every lane with work by one step (one SQS iteration over all its
+   live slots, or one batched FBP), unless its previous-but-one step is still
+   running, so lanes run concurrently on the GPU and stay at most two steps
+   ahead of the host,
+4. retires finished jobs: a device-to-host copy of their slots into pinned
+   memory, then the slots are freed and the live ones packed to the front.
+
+So a job that arrives while others are on the GPU joins its lane at the next
+iteration boundary instead of waiting for the batch to drain.  Slots of one
+lane are independent in every kernel (projections are per slice or per
+volume; the TV prior stops at each job's own z borders through the per-slice
+z links), so a job's result does not depend on what else is in the lane.
+
+The SQS iteration is the reference's sqs_one_step with the TV prior
+(recon/cupy/sqs_algorithms.py:22-57, prior/cupy/recon_prior.py:85-135), with
+weight 1, x0 = 0 and the projector normalisation folded into beta:
+
+    x <- x - (A^T (A x - y) + beta s1(x)) / (A^T A 1 + beta s2(x))
+
+Storage precision: the measured sinogram is held on the device in the job's
+storage type (float32, bfloat16 or float16); the iterate, the projections of
+each iteration and every sum are float32.  Optionally the forward projector
+reads a low-precision copy of the iterate written by the fused update
+(``image_storage``).
+"""
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ..projector import _device as D
+from ..recon import sqs_tv_update
+from .scheduler import ArrivalQueue, LatencyStats, MemoryBudget, Pending, SlotPool, bucket
+
+DTYPES = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float16": torch.float16}
+
+
+@dataclass(eq=False)
+class Protocol:
+    """Scan geometry and reconstruction shared by the jobs of one lane.
+
+    ``scan`` carries the attributes of the reference ct_projector (nx, ny, nz,
+    dx, dy, dz, cx, cy, cz, nu, nv, du, dv, off_u, off_v, dsd, dso); ``nz`` is
+    the volume depth for cone protocols and ignored for fan/parallel, whose
+    jobs bring 1..capacity slices each."""
+
+    name: str
+    kind: str  # "fan", "parallel" or "cone"
+    algo: str  # "fbp" or "sqs"
+    scan: object
+    angles: Optional[np.ndarray] = None  # fan / parallel, float32 radians
+    cone: Optional[Tuple[np.ndarray, ...]] = None  # (det_center, det_u, det_v, src), each [nview, 3]
+    n_iter: int = 20
+    beta: float = 0.0
+    tv_weights: Tuple[float, float, float] = (1.0, 1.0, 1.0)  # (z, y, x)
+    eps: float = 1e-8
+    filter: str = "hann"
+    storage: str = "float32"  # sinogram on the device
+    image_storage: str = "float32"  # iterate as read by the forward projector
+
+    def __post_init__(self):
+        if self.kind not in ("fan", "parallel", "cone"):
+            raise ValueError(f"unknown geometry kind {self.kind!r}")
+        if self.algo not in ("fbp", "sqs"):
+            raise ValueError(f"unknown algorithm {self.algo!r}")
+        if self.kind == "cone" and self.algo != "sqs":
+            raise ValueError("cone protocols reconstruct with SQS (there is no cone FBP)")
+        if self.storage not in DTYPES or self.image_storage not in DTYPES:
+            raise ValueError("storage must be float32, bfloat16 or float16")
+
+    @property
+    def nview(self) -> int:
+        return len(self.angles) if self.kind != "cone" else int(self.cone[0].shape[0])
+
+    @property
+    def slices_per_unit(self) -> int:
+        return int(self.scan.nz) if self.kind == "cone" else 1
+
+    def sinogram_shape(self, nz: int) -> Tuple[int, int, int, int]:
+        """Host sinogram layout of a job with nz slices."""
+        if self.kind == "cone":
+            return (1, self.nview, int(self.scan.nv), int(self.scan.nu))
+        return (nz, self.nview, 1, int(self.scan.nu))
+
+
+@dataclass(eq=False)
+class Job:
+    """One reconstruction request.  ``sinogram`` is a host tensor of
+    ``protocol.sinogram_shape(nz)`` in any float type (it is stored in the
+    protocol's storage type on the device); ``arrival`` is in seconds from the
+    start of the stream.  The server fills ``result`` ([nz, ny, nx] float32,
+    host) and ``t_done``."""
+
+    job_id: int
+    protocol: Protocol
+    sinogram: torch.Tensor
+    arrival: float = 0.0
+    nz: int = 1
+    result: Optional[torch.Tensor] = None
+    t_admit: float = float("nan")
+    t_done: float = float("nan")
+    done_event: Optional[torch.cuda.Event] = field(default=None, repr=False)
+
+    @property
+    def units(self) -> int:
+        return 1 if self.protocol.kind == "cone" else self.nz
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.arrival
+
+
+def _zlink_pattern(n: int) -> torch.Tensor:
+    z = torch.zeros(n, dtype=torch.uint8)
+    if n > 1:
+        z[1:] |= 1
+        z[:-1] |= 2
+    return z
+
+
+def _set_zlinks(z: torch.Tensor) -> None:
+    """Device-side z links of one volume of len(z) slices (no host copy, so the
+    lane's stream is not synchronised)."""
+    n = z.numel()
+    if n == 1:
+        z.zero_()
+        return
+    z.fill_(3)
+    z[:1].fill_(2)
+    z[-1:].fill_(1)
+
+
+# --------------------------------------------------------------------------- lanes
+class Lane:
+    """Device buffers, stream and slot pool of one protocol."""
+
+    def __init__(self, engine: "Engine", protocol: Protocol, capacity: int):
+        self.engine = engine
+        self.p = protocol
+        self.capacity = int(capacity)
+        self.pool = SlotPool(self.capacity)
+        self.dev = engine.device
+        self.stream = torch.cuda.Stream(self.dev)
+        self.jobs: Dict[int, List] = {}  # job id -> [job, steps left]
+        self.events: deque = deque()
+        self.last_used = time.perf_counter()
+        s = protocol.scan
+        self.ny, self.nx = int(s.ny), int(s.nx)
+        if protocol.kind == "cone":
+            self.geo = [torch.tensor(np.ascontiguousarray(a, dtype=np.float32), device=self.dev)
+                        for a in protocol.cone]
+        else:
+            self.ang = torch.tensor(np.ascontiguousarray(protocol.angles, dtype=np.float32), device=self.dev)
+            self.geom = _lib.GEOM_FAN if protocol.kind == "fan" else _lib.GEOM_PARALLEL
+
+    @staticmethod
+    def bytes_per_unit(p: Protocol) -> int:
+        raise NotImplementedError
+
+    @property
+    def active(self) -> bool:
+        return bool(self.jobs)
+
+    def ready(self) -> bool:
+        while self.events and self.events[0].query():
+            self.events.popleft()
+        return len(self.events) < 2
+
+    def can_admit(self, job: Job) -> bool:
+        return self.pool.fits(job.units)
+
+    def _record(self):
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self.events.append(ev)
+
+    def release(self):
+        self.stream.synchronize()
+
+
+class SQSLane(Lane):
+    """SQS-TV lane: slots are slices (fan/parallel) or volumes (cone)."""
+
+    def __init__(self, engine, protocol, capacity):
+        super().__init__(engine, protocol, capacity)
+        p, s = protocol, protocol.scan
+        C, U = self.capacity, p.slices_per_unit
+        nview = p.nview
+        nv = int(s.nv) if p.kind == "cone" else 1
+        sdt, idt = DTYPES[p.storage], DTYPES[p.image_storage]
+        with torch.cuda.stream(self.stream):
+            self.y = torch.zeros(C, nview, nv, int(s.nu), dtype=sdt, device=self.dev)
+            self.fp = torch.zeros(C, nview, nv, int(s.nu), device=self.dev)
+            self.x = [torch.zeros(C, U, self.ny, self.nx, device=self.dev) for _ in range(2)]
+            self.bp = torch.zeros(C, U, self.ny, self.nx, device=self.dev)
+            self.xlp = ([torch.zeros(C, U, self.ny, self.nx, dtype=idt, device=self.dev) for _ in range(2)]
+                        if idt != torch.float32 else None)
+            if p.kind == "cone":
+                self.zlink = _zlink_pattern(U).repeat(C).to(self.dev)
+            else:
+                self.zlink = torch.zeros(C, dtype=torch.uint8, device=self.dev)
+            one = torch.ones(1, U, self.ny, self.nx, device=self.dev)
+            self.norm = self._bp(self._fp(one)).reshape(U, self.ny, self.nx).contiguous()
+        self.cur = 0
+        self.graphs: Dict[Tuple[int, int], torch.cuda.CUDAGraph] = {}
+        self.graph_pool = torch.cuda.graph_pool_handle() if engine.use_graphs else None
+
+    @staticmethod
+    def bytes_per_unit(p: Protocol) -> int:
+        s = p.scan
+        nv = int(s.nv) if p.kind == "cone" else 1
+        sino = p.nview * nv * int(s.nu)
+        img = p.slices_per_unit * int(s.ny) * int(s.nx)
+        lp = 2 * DTYPES[p.image_storage].itemsize * img if p.image_storage != "float32" else 0
+        # y, fp; x (2), bp, fp workspace (transposed image); captured graphs' workspaces
+        return sino * (DTYPES[p.storage].itemsize + 4) + img * 4 * 4 + lp + sino * 4
+
+    # projector calls on the lane stream (current stream inside the lane's context)
+    def _fp(self, x, out=None):
+        if self.p.kind == "cone":
+            return D.siddon_fp(self.p.scan, x, *self.geo, out=out)
+        return D.dd_fp(self.p.scan, x, self.ang, self.geom, out=out)
+
+    def _bp(self, y, out=None):
+        if self.p.kind == "cone":
+            return D.siddon_bp(self.p.scan, y, *self.geo, out=out)
+        return D.dd_bp(self.p.scan, y, self.ang, self.geom, out=out)
+
+    def _iterate(self, b: int, src: int, dst: int):
+        p = self.p
+        xin = self.xlp[src][:b] if self.xlp is not None else self.x[src][:b]
+        self._fp(xin, out=self.fp[:b])
+        self.fp[:b].sub_(self.y[:b])
+        self._bp(self.fp[:b], out=self.bp[:b])
+        sqs_tv_update(self.x[src][:b], self.bp[:b], self.norm, p.beta, p.tv_weights, p.eps,
+                      zlink=self.zlink[:b * p.slices_per_unit], out=self.x[dst][:b],
+                      x_lp=self.xlp[dst][:b] if self.xlp is not None else None)
+
+    def _run_step(self, b: int):
+        src, dst = self.cur, 1 - self.cur
+        key = (b, src)
+        g = self.graphs.get(key)
+        if g is not None:
+            g.replay()
+        else:
+            # first step at this size runs eagerly (first-use allocations, kernel
+            # attributes), then the same step is captured for the next time
+            self._iterate(b, src, dst)
+            if self.engine.use_graphs:
+                g = torch.cuda.CUDAGraph()
+                g.capture_begin(pool=self.graph_pool)
+                try:
+                    self._iterate(b, src, dst)
+                finally:
+                    g.capture_end()
+                self.graphs[key] = g
+        self.cur = dst
+
+    def admit(self, job: Job) -> None:
+        p = self.p
+        start = self.pool.alloc(job.job_id, job.units)
+        if start is None:  # fits only after packing
+            self._apply_moves(self.pool.compact())
+            start = self.pool.alloc(job.job_id, job.units)
+        n = job.units
+        with torch.cuda.stream(self.stream):
+            self.y[start:start + n].copy_(job.sinogram.reshape(self.y[start:start + n].shape), non_blocking=True)
+            self.x[self.cur][start:start + n].zero_()
+            if self.xlp is not None:
+                self.xlp[self.cur][start:start + n].zero_()
+            if p.kind != "cone":
+                _set_zlinks(self.zlink[start:start + n])
+        self.jobs[job.job_id] = [job, p.n_iter]
+
+    def _apply_moves(self, moves):
+        if not moves:
+            return
+        with torch.cuda.stream(self.stream):
+            bufs = [self.y, self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else [])
+            for m in moves:
+                for t in bufs:
+                    t[m.dst:m.dst + m.n].copy_(t[m.src:m.src + m.n].clone())
+                if self.p.kind != "cone":
+                    self.zlink[m.dst:m.dst + m.n].copy_(self.zlink[m.src:m.src + m.n].clone())
+
+    def step(self) -> List[Job]:
+        hw = self.pool.high_water
+        b = bucket(hw, self.capacity)
+        with torch.cuda.stream(self.stream):
+            self._run_step(b)
+        done = []
+        for jid in list(self.jobs):
+            rec = self.jobs[jid]
+            rec[1] -= 1
+            if rec[1] == 0:
+                done.append(rec[0])
+        if done:
+            with torch.cuda.stream(self.stream):
+                for job in done:
+                    start, n = self.pool.free(job.job_id)
+                    del self.jobs[job.job_id]
+                    job.result = torch.empty((n * self.p.slices_per_unit, self.ny, self.nx), pin_memory=True)
+                    job.result.copy_(self.x[self.cur][start:start + n].reshape(job.result.shape), non_blocking=True)
+                    job.done_event = torch.cuda.Event()
+                    job.done_event.record(self.stream)
+                old_hw = hw
+                self._apply_moves(self.pool.compact())
+                new_hw = self.pool.high_water
+                if new_hw < old_hw:
+                    for t in [self.y, self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else []):
+                        t[new_hw:old_hw].zero_()
+                    if self.p.kind != "cone":
+                        self.zlink[new_hw:old_hw].zero_()
+        self._record()
+        self.last_used = time.perf_counter()
+        return done
+
+
+class FBPLane(Lane):
+    """FBP lane (fan or parallel): each step filters and back projects every
+    job admitted since the previous step as one batch of slices."""
+
+    def __init__(self, engine, protocol, capacity):
+        super().__init__(engine, protocol, capacity)
+        p, s = protocol, protocol.scan
+        C = self.capacity
+        with torch.cuda.stream(self.stream):
+            self.y = torch.zeros(C, p.nview, 1, int(s.nu), dtype=DTYPES[p.storage], device=self.dev)
+            self.img = torch.zeros(C, 1, self.ny, self.nx, device=self.dev)
+
+    @staticmethod
+    def bytes_per_unit(p: Protocol) -> int:
+        s = p.scan
+        sino = p.nview * int(s.nu)
+        return sino * (DTYPES[p.storage].itemsize + 8) + int(s.ny) * int(s.nx) * 4
+
+    def admit(self, job: Job) -> None:
+        start = self.pool.alloc(job.job_id, job.units)
+        if start is None:
+            raise RuntimeError("FBP lane slots are freed every step; admission checked can_admit first")
+        with torch.cuda.stream(self.stream):
+            self.y[start:start + job.units].copy_(job.sinogram.reshape(self.y[start:start + job.units].shape),
+                                                  non_blocking=True)
+        self.jobs[job.job_id] = [job, 1]
+
+    def step(self) -> List[Job]:
+        p = self.p
+        b = self.pool.high_water
+        done = []
+        with torch.cuda.stream(self.stream):
+            y = self.y[:b] if self.y.dtype == torch.float32 else self.y[:b].float()
+            f = D.ramp_filter(p.scan, y, p.filter, self.geom)
+            D.dd_bp(p.scan, f, self.ang, self.geom, is_fbp=True, out=self.img[:b])
+            for jid in list(self.jobs):
+                job = self.jobs.pop(jid)[0]
+                start, n = self.pool.free(jid)
+                job.result = torch.empty((n, self.ny, self.nx), pin_memory=True)
+                job.result.copy_(self.img[start:start + n].reshape(job.result.shape), non_blocking=True)
+                job.done_event = torch.cuda.Event()
+                job.done_event.record(self.stream)
+                done.append(job)
+        self._record()
+        self.last_used = time.perf_counter()
+        return done
+
+
+# --------------------------------------------------------------------------- engine
+class Engine:
+    """The server loop.  ``hbm_bytes`` bounds the lanes' buffers (default: 80%
+    of the device memory free at start); ``capacity`` maps a protocol name to
+    its lane's slot count (default 64 slices for fan/parallel lanes, as many
+    cone volumes as a quarter of the budget holds, at most 4)."""
+
+    def __init__(self, device=None, hbm_bytes: Optional[int] = None, max_wait: float = 1.0,
+                 use_graphs: bool = True, capacity: Optional[Dict[str, int]] = None, slices_per_lane: int = 64):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the reconstruction server needs a CUDA device")
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        _lib.lib()  # fail now, not at the first job, if the CUDA library is missing
+        free, _ = torch.cuda.mem_get_info(self.device)
+        self.budget = MemoryBudget(int(hbm_bytes) if hbm_bytes is not None else int(0.8 * free))
+        self.queue = ArrivalQueue(max_wait)
+        self.use_graphs = use_graphs
+        self.capacity = dict(capacity or {})
+        self.slices_per_lane = int(slices_per_lane)
+        self.lanes: Dict[str, Lane] = {}
+        self.jobs: Dict[int, Job] = {}
+        self.retiring: List[Job] = []
+        self.completed: List[Job] = []
+        self.stats = LatencyStats()
+        self.t0 = 0.0
+        self.evictions = 0  # lanes torn down to make room for another protocol
+        self.peak_reserved = 0
+
+    # lanes ---------------------------------------------------------------
+    def _lane_class(self, p: Protocol):
+        return SQSLane if p.algo == "sqs" else FBPLane
+
+    def _lane_capacity(self, p: Protocol) -> int:
+        if p.name in self.capacity:
+            return int(self.capacity[p.name])
+        if p.kind == "cone":
+            per = self._lane_class(p).bytes_per_unit(p)
+            return int(max(1, min(4, self.budget.total // 4 // max(per, 1))))
+        return self.slices_per_lane
+
+    def lane_for(self, p: Protocol, units: int) -> Optional[Lane]:
+        lane = self.lanes.get(p.name)
+        if lane is not None:
+            return lane
+        cls = self._lane_class(p)
+        cap = max(self._lane_capacity(p), units)
+        need = cls.bytes_per_unit(p) * cap
+        if need > self.budget.free:
+            # tear down idle lanes, least recently used first
+            for name, l in sorted(self.lanes.items(), key=lambda kv: kv[1].last_used):
+                if need <= self.budget.free:
+                    break
+                if not l.active and all(e.query() for e in l.events):
+                    l.release()
+                    del self.lanes[name]
+                    self.budget.release(name)
+                    self.evictions += 1
+        if not self.budget.try_reserve(p.name, need):
+            return None
+        self.peak_reserved = max(self.peak_reserved, self.budget.reserved)
+        lane = cls(self, p, cap)
+        self.lanes[p.name] = lane
+        return lane
+
+    def warmup(self, protocols: Sequence[Protocol]) -> None:
+        """Create the lanes of ``protocols`` ahead of the stream (projector
+        tables, normalisation images, cuFFT plans) so the first jobs do not
+        pay for them."""
+        for p in protocols:
+            self.lane_for(p, 1)
+        torch.cuda.synchronize(self.device)
+
+    # loop ----------------------------------------------------------------
+    def submit(self, job: Job) -> None:
+        self.jobs[job.job_id] = job
+        self.queue.push(Pending(job.arrival, job.job_id, job.protocol.name, job.units))
+
+    def _admit(self, now: float) -> bool:
+        admitted = False
+        for item in self.queue.candidates(now, self.lanes.keys()):
+            job = self.jobs[item.job_id]
+            lane = self.lane_for(job.protocol, job.units)
+            if lane is None or not lane.can_admit(job):
+                continue
+            lane.admit(job)
+            job.t_admit = now
+            self.queue.remove(item)
+            admitted = True
+        return admitted
+
+    def _step(self) -> bool:
+        stepped = False
+        for lane in list(self.lanes.values()):
+            if lane.active and lane.ready():
+                self.retiring.extend(lane.step())
+                stepped = True
+        return stepped
+
+    def _poll(self, now_fn) -> bool:
+        finished = False
+        still = []
+        for job in self.retiring:
+            if job.done_event.query():
+                job.t_done = now_fn()
+                self.stats.add(job.latency, job.t_done)
+                self.completed.append(job)
+                del self.jobs[job.job_id]
+                finished = True
+            else:
+                still.append(job)
+        self.retiring = still
+        return finished
+
+    def busy(self) -> bool:
+        return bool(self.jobs)
+
+    def run(self, jobs: Sequence[Job], realtime: bool = True, idle_sleep: float = 1e-4) -> dict:
+        """Serve ``jobs`` (sorted by arrival).  With ``realtime`` a job is
+        offered only once its arrival time has passed on the wall clock;
+        otherwise all are offered at once.  Returns the latency summary."""
+        pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        self.t0 = time.perf_counter()
+        now_fn = lambda: time.perf_counter() - self.t0  # noqa: E731
+        while pending or self.busy():
+            now = now_fn()
+            while pending and (not realtime or pending[0].arrival <= now):
+                self.submit(pending.popleft())
+            progressed = self._admit(now)
+            progressed |= self._step()
+            progressed |= self._poll(now_fn)
+            if not progressed:
+                time.sleep(idle_sleep)
+        torch.cuda.synchronize(self.device)
+        return self.stats.summary(0.0)
+
+    def close(self) -> None:
+        for name, lane in list(self.lanes.items()):
+            lane.release()
+            self.budget.release(name)
+        self.lanes.clear()

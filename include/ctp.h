@@ -289,6 +289,20 @@ size_t ctp_tomo_bp_workspace(const ctp_geometry* g);
 int ctp_tv_sqs(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nbatch,
                size_t nx, size_t ny, size_t nz, float eps, void* stream);
 
+/* One SQS iteration with the TV prior, fused into one pass (no counterpart
+   entry in the reference: there it is sqs_one_step, recon/cupy/sqs_algorithms.py
+   :22-57, calling the TV-SQS terms of TotalVariation.cu:21-149, in several
+   array operations):
+       x_out = x - (bp + beta s1(x)) / (norm + beta s2(x))
+   over nslices slices of ny x nx.  zlink[i] (may be NULL: no z coupling) bit 0
+   says slice i has its z neighbour i-1 in the same volume, bit 1 the
+   neighbour i+1.  norm holds norm_slices slices, read at slice i % norm_slices.
+   x_out must not alias x.  x_lp (may be NULL) also receives x_out in bf16
+   (flags CTP_FLAG_OUT_BF16) or fp16 (CTP_FLAG_OUT_FP16). */
+int ctp_sqs_tv_update(float* x_out, void* x_lp, const float* x, const float* bp, const float* norm,
+                      size_t norm_slices, const unsigned char* zlink, float wx, float wy, float wz, float beta,
+                      float eps, size_t nx, size_t ny, size_t nslices, unsigned flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

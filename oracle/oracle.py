@@ -311,3 +311,34 @@ def tv_sqs(img, weights, eps=1e-8):
     s1 = (wx * dx + wy * dy + wz * dz) / var + wx * dx1 / varx + wy * dy1 / vary + wz * dz1 / varz
     s2 = (wx + wy + wz) / var + wx / varx + wy / vary + wz / varz
     return s1, s2, var
+
+
+def split_volumes(zlink):
+    """Slice ranges [a, b) of the volumes packed in a flat slice array, from the
+    per-slice z links (bit 0: neighbour below in the same volume, bit 1: above)."""
+    zl = np.asarray(zlink, dtype=np.uint8)
+    out, a = [], 0
+    for i in range(len(zl)):
+        if not (zl[i] & 2):
+            out.append((a, i + 1))
+            a = i + 1
+    return out
+
+
+def sqs_tv_update(x, bp, norm, zlink, weights, beta, eps=1e-8):
+    """x - (bp + beta s1(x)) / (norm + beta s2(x)) in FP64 on a flat slice array
+    [nslices, ny, nx]: one SQS iteration with the TV prior (sqs_one_step,
+    recon/cupy/sqs_algorithms.py:22-57 of the reference), TV terms per packed
+    volume as in tv_sqs.  norm has norm_slices slices, read at i % norm_slices."""
+    x = _d(x)
+    n = x.shape[0]
+    norm = _d(norm)
+    idx = np.arange(n) % norm.shape[0]
+    s1 = np.zeros_like(x)
+    s2 = np.zeros_like(x)
+    vols = split_volumes(zlink) if zlink is not None else [(i, i + 1) for i in range(n)]
+    for a, b in vols:
+        t1, t2, _ = tv_sqs(x[None, a:b], weights, eps)
+        s1[a:b], s2[a:b] = t1[0], t2[0]
+    beta = float(np.float32(beta))
+    return x - (_d(bp) + beta * s1) / (norm[idx] + beta * s2)
