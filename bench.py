@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = ("parallel-beam DD FP + BP + ramp_filter(hann) + FBP BP, 16 x 512 x 512 at 0.8 mm, 720 views over pi, "
             "768 cells of 0.8 mm")
-METRIC = "FP+BP GB/s vs HBM roofline"
+METRIC = "FP+BP GB/s vs HBM roofline; served recons/s, p50/p99 latency at <=1e-4 rel L2"
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 512 << 20
 
@@ -44,6 +44,19 @@ def measured_peak():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def max_over_ranks(x: float, device) -> float:
+    """The largest of every rank's ``x`` (the step time of the slowest rank);
+    ``x`` itself without an initialised process group."""
+    import torch
+    import torch.distributed as tdist
+
+    if not (tdist.is_available() and tdist.is_initialized()) or tdist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def dist_env():
@@ -124,9 +137,15 @@ def algorithmic_bytes(nnz_slice: int, nb: int, scan) -> dict:
     return {"fp": proj, "bp": proj, "filter": 4 * 2 * n_prj, "bp_fbp": proj}
 
 
-# ours: launches of our own kernels per step (FP: table, transpose, sweep;
-# BP: gather; filter: pad, spectrum multiply, crop; FBP BP: gather)
-OUR_LAUNCHES_PER_STEP = 3 + 1 + 3 + 1
+# ours: launches of our own kernels per step (FP: edge table, transpose, row
+# and column line tables, streamed sweep; BP: gather; filter: pad, spectrum
+# multiply, crop; FBP BP: gather)
+OUR_LAUNCHES_PER_STEP = 5 + 1 + 3 + 1
+
+# served stream: seeded Poisson arrivals of 2D reconstruction jobs
+SERVED_JOBS = 150
+SERVED_RATE_HZ = 50.0
+SERVED_SEED = 5
 
 
 def run_ours(args, rank, world, local):
@@ -200,11 +219,7 @@ def run_ours(args, rank, world, local):
         torch.cuda.synchronize()
         if dist:
             tdist.barrier()
-    ms = float(np.mean(step_ms))
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(float(np.mean(step_ms)), dev)
     value = world * step_bytes / (ms * 1e-3) / 1e9
 
     # roofline of the dominant kernel
@@ -243,17 +258,14 @@ def run_ours(args, rank, world, local):
         t0 = time.perf_counter()
         e2e_step()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e = float(np.mean(e2e_ms))
-    if dist:
-        t = torch.tensor([e2e], device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e = max_over_ranks(float(np.mean(e2e_ms)), dev)
     n_img, n_prj = img.size, nb * scan.nview * scan.nv * scan.nu
     h2d = 4 * (n_img + n_prj + n_prj + n_prj) + 3 * 4 * len(ang)
     d2h = 4 * (n_prj + n_img + n_prj + n_img)
 
     cpu = cpu_baseline(scan, ang, img) if rank == 0 else None
     clocks = clk.summary()
+    served = run_served(dev) if (rank == 0 and not args.no_served) else None
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
@@ -271,8 +283,62 @@ def run_ours(args, rank, world, local):
         "cpu_baseline": cpu,
         "gpu_launches": OUR_LAUNCHES_PER_STEP * args.steps,
         "clocks": clocks,
+        "served": served,
     }
     return line
+
+
+def run_served(dev):
+    """The reconstruction server on a seeded stream of 2D jobs (fan 256^2 and
+    512^2, parallel 512^2; FBP or 20 SQS-TV iterations; 1-16 slices) arriving
+    at SERVED_RATE_HZ, sinograms stored in bf16 on the device, iterate and sums
+    in FP32; then the same jobs, same arrivals, through the plain FP32 per-call
+    path (one public-API call per operation, one job at a time).  Latency is
+    arrival to result on the host; recons/s is jobs over the time to the last
+    result."""
+    import torch
+
+    from ctprojector_b200.serving import Engine
+    from ctprojector_b200.serving import workload as W
+    from ctprojector_b200.serving.per_call import reconstruct, run_per_call
+
+    p32 = W.catalog(storage="float32")
+    plp = W.catalog(storage="bfloat16")
+    stream = W.arrivals(SERVED_JOBS, SERVED_RATE_HZ, SERVED_SEED, W.MIX_2D)
+    names = sorted({n for _, n, _ in stream})
+    pools32 = {n: W.sinogram_pool(p32[n], 2, 16, seed=i) for i, n in enumerate(names)}
+    poolslp = {n: [t.to(torch.bfloat16).pin_memory() for t in v] for n, v in pools32.items()}
+    jobs = W.make_jobs(plp, stream, poolslp)
+    eng = Engine(device=dev)
+    t0 = time.perf_counter()
+    eng.warmup([plp[n] for n in names])
+    warm = time.perf_counter() - t0
+    served = eng.run(jobs, realtime=True)
+    eng.close()
+    del eng
+    jobs32 = W.same_jobs(jobs, p32, pools32)
+    for n in names:  # first-call costs (filter plans, kernel attributes) outside the stream
+        reconstruct(next(j for j in jobs32 if j.protocol.name == n))
+    torch.cuda.synchronize()
+    per_call = run_per_call(jobs32, realtime=True)
+    by = {}
+    for j in jobs:
+        by.setdefault(j.protocol.name, []).append(j.latency)
+    r = lambda x: round(x, 3)  # noqa: E731
+    return {
+        "recons_per_s": r(served["recons_per_s"]), "p50_ms": r(served["p50_ms"]), "p99_ms": r(served["p99_ms"]),
+        "jobs": served["jobs"], "arrival_rate_hz": SERVED_RATE_HZ,
+        "per_call_fp32": {"recons_per_s": r(per_call["recons_per_s"]), "p50_ms": r(per_call["p50_ms"]),
+                          "p99_ms": r(per_call["p99_ms"])},
+        "served_over_per_call": r(served["recons_per_s"] / per_call["recons_per_s"]),
+        "p50_ms_by_protocol": {k: r(1e3 * float(np.median(v))) for k, v in sorted(by.items())},
+        "storage": "sinograms bf16 on the device; iterate, projections and sums fp32",
+        "mix": "2D: fan 256^2 (360 views) and 512^2 (984 views), parallel 512^2 (720 views); FBP or 20 SQS-TV "
+               "iterations; 1-16 slices; Poisson arrivals, seed %d" % SERVED_SEED,
+        "accuracy": "served results vs the FP64 oracle reconstruction within 1e-4 relative L2: "
+                    "tests/test_gpu_serving.py",
+        "warmup_s": r(warm),
+    }
 
 
 def cpu_baseline(scan, ang, img):
@@ -393,6 +459,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
     if args.impl == "reference":

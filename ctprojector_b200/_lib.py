@@ -105,6 +105,7 @@ _SIGNATURES = {
     "cupyTVSQS3D": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F],
     "cTVSQS3D": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F],
     "ctp_tv_sqs": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F, _P],
+    "ctp_wait_timeouts": [_P],
     "ctp_sqs_tv_update": [_P, _P, _P, _P, _P, _S, _P, _F, _F, _F, _F, _F, _S, _S, _S, c_uint, _P],
 }
 _RESTYPE = {

@@ -32,6 +32,7 @@ int tomo_fp(float*, const float*, const float*, const float*, const ctp_geometry
 int tomo_bp(float*, const float*, const float*, const float*, const ctp_geometry&, unsigned, void*, size_t,
             cudaStream_t);
 size_t tomo_bp_workspace(const ctp_geometry&);
+int wait_timeouts(unsigned*);
 int sqs_tv_update(float*, void*, const float*, const float*, const float*, size_t, const unsigned char*, float, float,
                   float, float, float, size_t, size_t, size_t, unsigned, cudaStream_t);
 int tv_sqs(float*, float*, float*, const float*, float, float, float, size_t, size_t, size_t, size_t, float,
@@ -634,5 +635,7 @@ int ctp_sqs_tv_update(float* x_out, void* x_lp, const float* x, const float* bp,
     return sqs_tv_update(x_out, x_lp, x, bp, norm, norm_slices, zlink, wx, wy, wz, beta, eps, nx, ny, nslices, flags,
                          as_stream(stream));
 }
+
+int ctp_wait_timeouts(unsigned int* count) { return wait_timeouts(count); }
 
 }  // extern "C"

@@ -645,59 +645,73 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     e = (a - (s - bb)) + (b - bb);
 }
 
-// Stage lines (length n, stride n between lines) into midpoint tables of n+1
-// entries {hi, lo, r, 0}: hi + lo = integral over cells [0, i) plus r_i / 2.
+// Midpoint table of one line of n cells, built by one warp: n+1 entries
+// {hi, lo, r, 0} with hi + lo = integral over cells [0, i) plus r_i / 2 in
+// double-float form and r_i the cell value (0 past the end).
+template <typename Tin>
+__device__ __forceinline__ void stage_line(float4* __restrict__ T, const Tin* __restrict__ row, int n, int lane) {
+    const int E = (n + 1 + 31) / 32;
+    const int k0 = lane * E;
+    // lane total as a double-float
+    float hi = 0.f, lo = 0.f;
+    for (int q = 0; q < E; ++q) {
+        int k = k0 + q;
+        if (k < n) {
+            float e;
+            two_sum(hi, ldf(row + k), hi, e);
+            lo += e;
+        }
+    }
+    // exclusive scan of (hi, lo) across the warp
+    float ihi = hi, ilo = lo;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        float th = __shfl_up_sync(0xffffffffu, ihi, o), tl = __shfl_up_sync(0xffffffffu, ilo, o);
+        if (lane >= o) {
+            float sh, e;
+            two_sum(ihi, th, sh, e);
+            float sl = ilo + tl + e;
+            ihi = sh + sl;
+            ilo = sl - (ihi - sh);
+        }
+    }
+    float bhi, blo;
+    {
+        float e;
+        two_sum(ihi, -hi, bhi, e);
+        blo = ilo - lo + e;
+        float t = bhi + blo;
+        blo = blo - (t - bhi);
+        bhi = t;
+    }
+    for (int q = 0; q < E; ++q) {
+        int k = k0 + q;
+        if (k <= n) {
+            float r = k < n ? ldf(row + k) : 0.f;
+            T[k] = make_float4(bhi, fmaf(0.5f, r, blo), r, 0.f);  // midpoint table
+            float e;
+            two_sum(bhi, r, bhi, e);
+            blo += e;
+        }
+    }
+}
+
+// Stage lines (length n, stride n between lines) into consecutive tables.
 template <typename Tin>
 __device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ src, int nlines, int n, int warp,
                             int lane, int nwarps) {
-    const int E = (n + 1 + 31) / 32;
-    for (int l = warp; l < nlines; l += nwarps) {
-        const Tin* row = src + (size_t)l * n;
-        float4* T = tab + (size_t)l * (n + 1);
-        const int k0 = lane * E;
-        // lane total as a double-float
-        float hi = 0.f, lo = 0.f;
-        for (int q = 0; q < E; ++q) {
-            int k = k0 + q;
-            if (k < n) {
-                float e;
-                two_sum(hi, ldf(row + k), hi, e);
-                lo += e;
-            }
-        }
-        // exclusive scan of (hi, lo) across the warp
-        float ihi = hi, ilo = lo;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            float th = __shfl_up_sync(0xffffffffu, ihi, o), tl = __shfl_up_sync(0xffffffffu, ilo, o);
-            if (lane >= o) {
-                float sh, e;
-                two_sum(ihi, th, sh, e);
-                float sl = ilo + tl + e;
-                ihi = sh + sl;
-                ilo = sl - (ihi - sh);
-            }
-        }
-        float bhi, blo;
-        {
-            float e;
-            two_sum(ihi, -hi, bhi, e);
-            blo = ilo - lo + e;
-            float t = bhi + blo;
-            blo = blo - (t - bhi);
-            bhi = t;
-        }
-        for (int q = 0; q < E; ++q) {
-            int k = k0 + q;
-            if (k <= n) {
-                float r = k < n ? ldf(row + k) : 0.f;
-                T[k] = make_float4(bhi, fmaf(0.5f, r, blo), r, 0.f);  // midpoint table
-                float e;
-                two_sum(bhi, r, bhi, e);
-                blo += e;
-            }
-        }
-    }
+    for (int l = warp; l < nlines; l += nwarps) stage_line(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
+}
+
+// The tables of every line of a stack of slices (one warp per line), for the
+// forward projector that streams them into shared memory.
+template <typename Tin>
+__global__ void __launch_bounds__(256) line_tables_kernel(float4* __restrict__ out, const Tin* __restrict__ src,
+                                                          long long nlines, int n) {
+    const int lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long l = w0; l < nlines; l += nw) stage_line(out + l * (n + 1), src + l * n, n, lane);
 }
 
 // NI = edge groups per warp (compile time, so the group loop is straight-line
@@ -801,6 +815,208 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_fast_kernel(Tout* __restrict__
             float sn, cs;
             sincosf(deg[view], &sn, &cs);
             Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + k;
+            stf(dst, rdf(dst) / (ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn)));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Forward projection, streamed-table path.  Same arithmetic as
+// dd2d_fp_fast_kernel, but the midpoint tables of every image line are built
+// once per slice by line_tables_kernel and streamed into a two-buffer ring in
+// shared memory with bulk asynchronous copies (cp.async.bulk, completion on an
+// mbarrier): while the warps integrate one chunk of lines, the copy of the
+// next chunk is in flight, and no warp spends instructions on staging.
+__device__ unsigned int g_wait_timeouts;  // bounded waits that gave up (read by ctp_wait_timeouts)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bytes and both addresses are multiples of 16
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of `bar`, giving up (and counting it) after a bounded
+// number of polls instead of spinning forever.
+constexpr unsigned kWaitPolls = 1u << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (unsigned i = 0; i < kWaitPolls; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicAdd(&g_wait_timeouts, 1u);
+    return false;
+}
+
+template <bool FAN, int NI, typename Tout>
+__global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
+                                                             const float4* __restrict__ ltab1, DDTab tab, Grid g,
+                                                             Det d, int nview, int vgroup, int rchunk,
+                                                             const float* __restrict__ deg, int unweight_par) {
+    extern __shared__ float4 s_ring[];  // [2][rchunk * (max(nx, ny) + 1)]
+    __shared__ __align__(8) unsigned long long s_bar[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int v0 = blockIdx.x * vgroup;
+    const int nvg = min(vgroup, nview - v0);
+    const int slice = blockIdx.y;  // b * nz + iz, detector row iv = iz
+    const int iz = slice % g.nz, b = slice / g.nz;
+    const int ipv = (d.nu + 30) / 31;  // edge groups per view
+    const int nitems = nvg * ipv;
+    const size_t ring = (size_t)rchunk * (max(g.nx, g.ny) + 1);
+
+    // orientations with work in this CTA: rows (o = 0) for views traced along
+    // y, columns (o = 1) for views traced along x, both in the blend band
+    bool act0 = false, act1 = false;
+    for (int vi = threadIdx.x; vi < nvg; vi += blockDim.x) {
+        const float wx = tab.wx[v0 + vi];
+        act0 |= wx > 0.f;
+        act1 |= wx < 1.f;
+    }
+    act0 = __syncthreads_or(act0);
+    act1 = __syncthreads_or(act1);
+    const int nc0 = act0 ? (g.ny + rchunk - 1) / rchunk : 0;
+    const int nc1 = act1 ? (g.nx + rchunk - 1) / rchunk : 0;
+    const int K = nc0 + nc1;
+    const float4* src0 = ltab0 + (size_t)slice * g.ny * (g.nx + 1);
+    const float4* src1 = ltab1 + (size_t)slice * g.nx * (g.ny + 1);
+
+    auto issue = [&](int k) {
+        const int o = k < nc0 ? 0 : 1;
+        const int c = o == 0 ? k : k - nc0;
+        const int n = o == 0 ? g.nx : g.ny, nl = o == 0 ? g.ny : g.nx;
+        const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
+        const unsigned bytes = (unsigned)((size_t)nlc * (n + 1) * sizeof(float4));
+        unsigned long long* bar = &s_bar[k & 1];
+        mbar_expect_tx(bar, bytes);
+        bulk_copy_g2s(s_ring + (k & 1) * ring, (o == 0 ? src0 : src1) + (size_t)l0 * (n + 1), bytes, bar);
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (K > 0) issue(0);
+        if (K > 1) issue(1);
+    }
+
+    float A[NI], B[NI], acc[NI];
+    bool failed = false;
+    int k = 0;
+    for (; k < K; ++k) {
+        const int o = k < nc0 ? 0 : 1;
+        const int c = o == 0 ? k : k - nc0;
+        const int n = o == 0 ? g.nx : g.ny, nl = o == 0 ? g.ny : g.nx;
+        const int last = (o == 0 ? nc0 : nc1) - 1;
+        if (c == 0) {
+#pragma unroll
+            for (int q = 0; q < NI; ++q) {
+                const int it = warp + 8 * q;
+                // dummy edge positions keep every width non-zero
+                A[q] = (float)lane - 0.5f;
+                B[q] = 0.f;
+                acc[q] = 0.f;
+                if (it < nitems) {
+                    const int vi = it / ipv, m = it - vi * ipv;
+                    const int view = v0 + vi;
+                    const float wx = tab.wx[view];
+                    const bool active = o == 0 ? wx > 0.f : wx < 1.f;
+                    const int j = 31 * m + lane;
+                    if (active && j <= d.nu) {
+                        const size_t ie = (size_t)view * (d.nu + 1) + j;
+                        A[q] = tab.eA[o][ie] - 0.5f;  // shifted for the midpoint tables
+                        B[q] = tab.eB[o][ie];
+                    }
+                }
+            }
+        }
+        if (!mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1)) failed = true;
+        const float4* buf = s_ring + (k & 1) * ring;
+        const int anchor = o == 0 ? tab.ym : tab.xm;
+        const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
+        const float lo_lim = -0.5f, hi_lim = (float)n - 0.5f;
+        for (int r = 0; r < nlc && !failed; ++r) {
+            const float t = (float)(l0 + r - anchor);
+            const float4* T = buf + (size_t)r * (n + 1);
+#pragma unroll
+            for (int q = 0; q < NI; ++q) {
+                const float xr = fmaf(B[q], t, A[q]);  // edge position - 1/2
+                const float xs = clampf(xr, lo_lim, hi_lim);
+                const float tt = xs + kRoundMagic;
+                const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
+                const float hi = e.x, lo = fmaf(e.z, xs - (tt - kRoundMagic), e.y);
+                const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
+                const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
+                const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
+                // signed integral over [x_j, x_j+1] over the signed width of
+                // the rounded footprint
+                acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
+            }
+        }
+        if (c == last && !failed) {
+#pragma unroll
+            for (int q = 0; q < NI; ++q) {
+                const int it = warp + 8 * q;
+                if (it >= nitems) continue;
+                const int vi = it / ipv, m = it - vi * ipv;
+                const int view = v0 + vi;
+                const int kk = 31 * m + lane;
+                const float wx = tab.wx[view];
+                const bool active = o == 0 ? wx > 0.f : wx < 1.f;
+                if (!active || lane >= 31 || kk >= d.nu) continue;
+                float v = acc[q] * tab.cL[o][(size_t)view * d.nu + kk] * (o == 0 ? wx : 1.f - wx);
+                Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
+                if (o == 1 && wx > 0.f) v += rdf(dst);  // the row pass of this view wrote first
+                stf(dst, v);
+            }
+        }
+        // every warp is done with buffer k & 1 before it is refilled
+        failed = __syncthreads_or(failed);
+        if (failed) break;
+        if (threadIdx.x == 0 && k + 2 < K) issue(k + 2);
+    }
+    if (failed) {
+        // chunks k and k + 1 may still be in flight: let them land (bounded) before exiting
+        if (threadIdx.x == 0)
+            for (int j = k; j < min(k + 2, K); ++j) mbar_wait_bounded(&s_bar[j & 1], (j >> 1) & 1);
+        return;
+    }
+    if (unweight_par) {
+        // FORCE_FBP on parallel FP: cancel the ray-length weight
+        // (ReverseWeightBPParallelKernel, distanceDriven2DUtils.cu:68-94)
+        for (int q = 0; q < NI; ++q) {
+            const int it = warp + 8 * q;
+            if (it >= nitems) continue;
+            const int vi = it / ipv, m = it - vi * ipv;
+            const int view = v0 + vi;
+            const int kk = 31 * m + lane;
+            if (lane >= 31 || kk >= d.nu) continue;
+            float sn, cs;
+            sincosf(deg[view], &sn, &cs);
+            Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
             stf(dst, rdf(dst) / (ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn)));
         }
     }
@@ -1240,8 +1456,24 @@ const T* cptr(const void* p) { return static_cast<const T*>(p); }
 template <typename T>
 T* mptr(void* p) { return static_cast<T*>(p); }
 
-size_t fp_workspace(const ctp_geometry& g) {
+// Scratch of the forward projector: the edge table and the transposed image
+// (every path), then the line tables of the streamed path.
+size_t fp_workspace_min(const ctp_geometry& g) {
     return align_up(table_floats(g.nview, g.nu) * sizeof(float)) + align_up(g.nbatch * g.nz * g.ny * g.nx * 4);
+}
+
+size_t fp_line_tables_bytes(const ctp_geometry& g) {
+    size_t slices = g.nbatch * g.nz;
+    return align_up(slices * (g.ny * (g.nx + 1) + g.nx * (g.ny + 1)) * sizeof(float4));
+}
+
+// Lines per chunk of the streamed path's two-buffer ring, or 0 if one line
+// per buffer does not fit.
+int fp_stream_chunk(const ctp_geometry& g) {
+    size_t line = (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+    if (2 * line > 200 * 1024) return 0;
+    int r = (int)((66 * 1024) / (2 * line));
+    return std::max(1, std::min(r, 8));
 }
 
 int build_table(float* base, const float* deg, const ctp_geometry& g, int geom, cudaStream_t s, DDTab& tab) {
@@ -1289,7 +1521,7 @@ bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
 
 template <typename Tin, typename Tout>
 int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
-              unsigned flags, char* ws, cudaStream_t s) {
+              unsigned flags, char* ws, size_t ws_bytes, cudaStream_t s) {
     DDTab tab;
     int rc = build_table(reinterpret_cast<float*>(ws), deg, g, geom, s, tab);
     if (rc) return rc;
@@ -1299,6 +1531,40 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     if ((rc = check_launch("transpose_kernel"))) return rc;
     int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
     int vgroup = 0, nrows = 0;
+    const int rchunk = fp_stream_chunk(g);
+    if (fp_fast_ok(g, vgroup, nrows) && rchunk > 0 &&
+        ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
+        // streamed path: line tables of rows (from the image) and columns (from its transpose)
+        float4* lt0 = reinterpret_cast<float4*>(ws + fp_workspace_min(g));
+        float4* lt1 = lt0 + g.nbatch * g.nz * g.ny * (g.nx + 1);
+        long long rows = (long long)(g.nbatch * g.nz * g.ny), cols = (long long)(g.nbatch * g.nz * g.nx);
+        line_tables_kernel<Tin><<<(unsigned)std::min<long long>((rows + 7) / 8, 148 * 16), 256, 0, s>>>(
+            lt0, cptr<Tin>(img), rows, (int)g.nx);
+        line_tables_kernel<Tin><<<(unsigned)std::min<long long>((cols + 7) / 8, 148 * 16), 256, 0, s>>>(
+            lt1, imgT, cols, (int)g.ny);
+        if ((rc = check_launch("line_tables_kernel"))) return rc;
+        size_t shm = 2 * (size_t)rchunk * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+        dim3 fg((unsigned)((g.nview + vgroup - 1) / vgroup), (unsigned)(g.nbatch * g.nz));
+        int ipv = (int)((g.nu + 30) / 31);
+        int per_warp = (vgroup * ipv + 7) / 8;
+        auto launch = [&](auto kern) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), lt0, lt1, tab, make_grid(g), make_det(g), (int)g.nview,
+                                      vgroup, rchunk, deg, unweight);
+        };
+        bool fan = geom == 0;
+        if (per_warp <= 4) {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 4, Tout>); else launch(dd2d_fp_stream_kernel<false, 4, Tout>);
+        } else if (per_warp <= 8) {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 8, Tout>); else launch(dd2d_fp_stream_kernel<false, 8, Tout>);
+        } else if (per_warp <= 12) {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 12, Tout>); else launch(dd2d_fp_stream_kernel<false, 12, Tout>);
+        } else {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 16, Tout>); else launch(dd2d_fp_stream_kernel<false, 16, Tout>);
+        }
+        return check_launch("dd2d_fp_stream_kernel");
+    }
     if (fp_fast_ok(g, vgroup, nrows)) {
         size_t shm = (size_t)nrows * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
         dim3 fg((unsigned)((g.nview + vgroup - 1) / vgroup), (unsigned)(g.nbatch * g.nz));
@@ -1332,25 +1598,33 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
-size_t dd2d_fp_workspace(const ctp_geometry& g, int, int, unsigned) { return fp_workspace(g); }
+size_t dd2d_fp_workspace(const ctp_geometry& g, int, int, unsigned) {
+    int vgroup = 0, nrows = 0;
+    bool stream = fp_fast_ok(g, vgroup, nrows) && fp_stream_chunk(g) > 0;
+    return fp_workspace_min(g) + (stream ? fp_line_tables_bytes(g) : 0);
+}
 
 int dd2d_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
             unsigned flags, void* workspace, size_t workspace_bytes, cudaStream_t s) {
     if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
     Scratch scr;
-    int rc = scr.acquire(workspace, workspace_bytes, fp_workspace(g), s);
+    // a caller's workspace of at least the minimum runs the staged path, one of
+    // the full query size (and scratch taken here) the streamed path
+    const size_t full = dd2d_fp_workspace(g, geom, type, flags);
+    const size_t have = workspace ? workspace_bytes : full;
+    int rc = scr.acquire(workspace, workspace_bytes, workspace ? fp_workspace_min(g) : full, s);
     if (rc) return rc;
     bool in16 = flags & (CTP_FLAG_IN_BF16 | CTP_FLAG_IN_FP16);
     bool out16 = flags & (CTP_FLAG_OUT_BF16 | CTP_FLAG_OUT_FP16);
-    if (!in16 && !out16) return launch_fp<float, float>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+    if (!in16 && !out16) return launch_fp<float, float>(prj, img, deg, g, geom, type, flags, scr.base(), have, s);
     if ((flags & CTP_FLAG_IN_BF16) && (flags & CTP_FLAG_OUT_BF16))
-        return launch_fp<__nv_bfloat16, __nv_bfloat16>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+        return launch_fp<__nv_bfloat16, __nv_bfloat16>(prj, img, deg, g, geom, type, flags, scr.base(), have, s);
     if ((flags & CTP_FLAG_IN_FP16) && (flags & CTP_FLAG_OUT_FP16))
-        return launch_fp<__half, __half>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+        return launch_fp<__half, __half>(prj, img, deg, g, geom, type, flags, scr.base(), have, s);
     if ((flags & CTP_FLAG_IN_BF16) && !out16)
-        return launch_fp<__nv_bfloat16, float>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+        return launch_fp<__nv_bfloat16, float>(prj, img, deg, g, geom, type, flags, scr.base(), have, s);
     if ((flags & CTP_FLAG_IN_FP16) && !out16)
-        return launch_fp<__half, float>(prj, img, deg, g, geom, type, flags, scr.base(), s);
+        return launch_fp<__half, float>(prj, img, deg, g, geom, type, flags, scr.base(), have, s);
     return set_error(CTP_ERR_UNSUPPORTED, "dd2d_fp: unsupported storage type combination (flags 0x%x)", flags);
 }
 
@@ -1544,7 +1818,7 @@ static int fp_scratch_address(void** out) {
 
 int dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
                     unsigned flags, cudaStream_t s) {
-    size_t need = fp_workspace(g);
+    size_t need = fp_workspace_min(g);
     if (need > kNoAllocScratchBytes)
         return set_error(CTP_ERR_TOO_LARGE,
                          "ctp_dd2d_fp_noalloc needs %zu bytes of scratch; its fixed buffer holds %zu "
@@ -1557,5 +1831,12 @@ int dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geom
 }
 
 size_t dd2d_fp_noalloc_capacity() { return kNoAllocScratchBytes; }
+
+int wait_timeouts(unsigned* count) {
+    if (!count) return set_error(CTP_ERR_INVALID_ARGUMENT, "count pointer is null");
+    cudaError_t e = cudaMemcpyFromSymbol(count, g_wait_timeouts, sizeof(unsigned));
+    if (e != cudaSuccess) return set_error((int)e, "reading the wait-timeout counter: %s", cudaGetErrorString(e));
+    return CTP_OK;
+}
 
 }  // namespace ctp

@@ -48,7 +48,7 @@ import torch
 from .. import _lib
 from ..projector import _device as D
 from ..recon import sqs_tv_update
-from .scheduler import ArrivalQueue, LatencyStats, MemoryBudget, Pending, SlotPool, bucket
+from .scheduler import ArrivalQueue, LatencyStats, MemoryBudget, Pending, SlotPool, bucket, bucket_sizes
 
 DTYPES = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float16": torch.float16}
 
@@ -118,6 +118,7 @@ class Job:
     t_admit: float = float("nan")
     t_done: float = float("nan")
     done_event: Optional[torch.cuda.Event] = field(default=None, repr=False)
+    tag: object = None  # free for the caller (the synthetic streams record the data source)
 
     @property
     def units(self) -> int:
@@ -162,6 +163,8 @@ class Lane:
         self.jobs: Dict[int, List] = {}  # job id -> [job, steps left]
         self.events: deque = deque()
         self.last_used = time.perf_counter()
+        # launch sizes step by 4 slices (fan/parallel) or 1 volume (cone)
+        self.granule = 1 if protocol.kind == "cone" else 4
         s = protocol.scan
         self.ny, self.nx = int(s.ny), int(s.nx)
         if protocol.kind == "cone":
@@ -274,6 +277,17 @@ class SQSLane(Lane):
                 self.graphs[key] = g
         self.cur = dst
 
+    def prepare(self) -> None:
+        """Capture the iteration graphs of every launch size ahead of the
+        stream.  The lane is empty, so every slot holds zeros and stays zero
+        (a constant image has no TV terms)."""
+        if self.jobs:
+            raise RuntimeError("prepare() runs on an empty lane")
+        with torch.cuda.stream(self.stream):
+            for b in bucket_sizes(self.capacity, self.granule):
+                for _ in range(2):
+                    self._run_step(b)
+
     def admit(self, job: Job) -> None:
         p = self.p
         start = self.pool.alloc(job.job_id, job.units)
@@ -303,7 +317,7 @@ class SQSLane(Lane):
 
     def step(self) -> List[Job]:
         hw = self.pool.high_water
-        b = bucket(hw, self.capacity)
+        b = bucket(hw, self.capacity, self.granule)
         with torch.cuda.stream(self.stream):
             self._run_step(b)
         done = []
@@ -336,7 +350,9 @@ class SQSLane(Lane):
 
 class FBPLane(Lane):
     """FBP lane (fan or parallel): each step filters and back projects every
-    job admitted since the previous step as one batch of slices."""
+    job admitted since the previous step as one batch of slices.  The ramp
+    filter is built in FP64 (``exact``), so the result tracks the FP64
+    reconstruction rather than the reference's FP32 filter construction."""
 
     def __init__(self, engine, protocol, capacity):
         super().__init__(engine, protocol, capacity)
@@ -361,14 +377,23 @@ class FBPLane(Lane):
                                                   non_blocking=True)
         self.jobs[job.job_id] = [job, 1]
 
-    def step(self) -> List[Job]:
+    def prepare(self) -> None:
+        """Run every launch size once on zeros (filter plans, workspaces)."""
+        with torch.cuda.stream(self.stream):
+            for b in bucket_sizes(self.capacity, self.granule):
+                self._filter_bp(b)
+
+    def _filter_bp(self, b: int) -> None:
         p = self.p
-        b = self.pool.high_water
+        y = self.y[:b] if self.y.dtype == torch.float32 else self.y[:b].float()
+        f = D.ramp_filter(p.scan, y, p.filter, self.geom, exact=True)
+        D.dd_bp(p.scan, f, self.ang, self.geom, is_fbp=True, out=self.img[:b])
+
+    def step(self) -> List[Job]:
+        b = bucket(self.pool.high_water, self.capacity, self.granule)
         done = []
         with torch.cuda.stream(self.stream):
-            y = self.y[:b] if self.y.dtype == torch.float32 else self.y[:b].float()
-            f = D.ramp_filter(p.scan, y, p.filter, self.geom)
-            D.dd_bp(p.scan, f, self.ang, self.geom, is_fbp=True, out=self.img[:b])
+            self._filter_bp(b)
             for jid in list(self.jobs):
                 job = self.jobs.pop(jid)[0]
                 start, n = self.pool.free(jid)
@@ -376,6 +401,7 @@ class FBPLane(Lane):
                 job.result.copy_(self.img[start:start + n].reshape(job.result.shape), non_blocking=True)
                 job.done_event = torch.cuda.Event()
                 job.done_event.record(self.stream)
+                self.y[start:start + n].zero_()
                 done.append(job)
         self._record()
         self.last_used = time.perf_counter()
@@ -447,11 +473,13 @@ class Engine:
         return lane
 
     def warmup(self, protocols: Sequence[Protocol]) -> None:
-        """Create the lanes of ``protocols`` ahead of the stream (projector
-        tables, normalisation images, cuFFT plans) so the first jobs do not
-        pay for them."""
+        """Create the lanes of ``protocols`` ahead of the stream (normalisation
+        images, filter plans, captured graphs of every launch size) so the
+        first jobs do not pay for them."""
         for p in protocols:
-            self.lane_for(p, 1)
+            lane = self.lane_for(p, 1)
+            if lane is not None and not lane.active:
+                lane.prepare()
         torch.cuda.synchronize(self.device)
 
     # loop ----------------------------------------------------------------
@@ -498,6 +526,16 @@ class Engine:
     def busy(self) -> bool:
         return bool(self.jobs)
 
+    def pass_once(self, now: float, now_fn=None) -> bool:
+        """One pass of the server loop at time ``now`` (seconds on the caller's
+        clock): admit queued jobs, step the lanes, collect finished results.
+        Returns whether anything happened, so a caller driving the loop from
+        its own event loop knows when to yield."""
+        progressed = self._admit(now)
+        progressed |= self._step()
+        progressed |= self._poll(now_fn or (lambda: now))
+        return progressed
+
     def run(self, jobs: Sequence[Job], realtime: bool = True, idle_sleep: float = 1e-4) -> dict:
         """Serve ``jobs`` (sorted by arrival).  With ``realtime`` a job is
         offered only once its arrival time has passed on the wall clock;
@@ -509,9 +547,7 @@ class Engine:
             now = now_fn()
             while pending and (not realtime or pending[0].arrival <= now):
                 self.submit(pending.popleft())
-            progressed = self._admit(now)
-            progressed |= self._step()
-            progressed |= self._poll(now_fn)
+            progressed = self.pass_once(now, now_fn)
             if not progressed:
                 time.sleep(idle_sleep)
         torch.cuda.synchronize(self.device)

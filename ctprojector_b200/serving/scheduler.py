@@ -88,15 +88,20 @@ class SlotPool:
         return moves
 
 
-def bucket(n: int, capacity: int) -> int:
-    """Launch size for ``n`` live slots: the next power of two, at most
-    ``capacity`` (one captured graph per size)."""
+def bucket(n: int, capacity: int, granule: int = 1) -> int:
+    """Launch size for ``n`` live slots: ``n`` rounded up to a multiple of
+    ``granule``, at most ``capacity`` (one captured graph per size, so the
+    granule bounds the number of graphs; empty slots in the launch are work
+    done on zeros)."""
     if n <= 0:
         return 0
-    b = 1
-    while b < n:
-        b <<= 1
-    return min(b, capacity)
+    g = max(1, int(granule))
+    return min(-(-n // g) * g, capacity)
+
+
+def bucket_sizes(capacity: int, granule: int = 1):
+    """Every launch size ``bucket`` can return for this capacity."""
+    return sorted({bucket(n, capacity, granule) for n in range(1, capacity + 1)})
 
 
 # --------------------------------------------------------------------------- memory
@@ -208,3 +213,11 @@ class LatencyStats:
         return {"jobs": len(self), "recons_per_s": self.throughput(t_start),
                 "p50_ms": 1e3 * self.percentile(50), "p99_ms": 1e3 * self.percentile(99),
                 "max_ms": 1e3 * max(self.latency) if self.latency else float("nan")}
+
+
+def shard(items, rank: int, world: int):
+    """Round-robin share of ``items`` for one of ``world`` replicas (one server
+    per GPU; jobs are independent, so no data crosses ranks)."""
+    if world <= 0 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of {world}")
+    return [x for i, x in enumerate(items) if i % world == rank]

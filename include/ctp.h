@@ -289,6 +289,13 @@ size_t ctp_tomo_bp_workspace(const ctp_geometry* g);
 int ctp_tv_sqs(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nbatch,
                size_t nx, size_t ny, size_t nz, float eps, void* stream);
 
+/* Bounded device-side waits that gave up on the current device since the
+   library was loaded (the streamed forward projector polls an mbarrier for
+   each chunk of line tables with an iteration limit, and counts a limit that
+   ran out instead of spinning for ever).  0 in a healthy process.  No
+   counterpart in the reference.  Synchronises with the device. */
+int ctp_wait_timeouts(unsigned int* count);
+
 /* One SQS iteration with the TV prior, fused into one pass (no counterpart
    entry in the reference: there it is sqs_one_step, recon/cupy/sqs_algorithms.py
    :22-57, calling the TV-SQS terms of TotalVariation.cu:21-149, in several

@@ -212,3 +212,22 @@ def test_per_call_path_matches_server():
     run_per_call(b, realtime=False)
     for x, y in zip(a, b):
         assert rel_l2(x.result.numpy(), y.result.numpy()) <= 1e-5
+
+
+def test_full_size_protocols_match_fp64_oracle():
+    """The served stream's own protocols at full size (bf16 sinograms): the
+    results of the jobs the FP64 oracle reconstructs in seconds are within
+    1e-4 of it (relative L2)."""
+    from ctprojector_b200.serving import Engine
+    from ctprojector_b200.serving import workload as W
+
+    protos = W.catalog(storage="bfloat16")
+    stream = [(0.0, "fan256_sqs", 1), (0.0, "fan256_fbp", 2), (0.0, "par512_fbp", 1), (0.0, "fan512_fbp", 1)]
+    pools = {n: W.sinogram_pool(protos[n], 1, 2, seed=i) for i, (_, n, _) in enumerate(stream)}
+    jobs = W.make_jobs(protos, stream, pools)
+    eng = Engine()
+    eng.run(jobs, realtime=False)
+    for job in jobs:
+        err = rel_l2(job.result.numpy(), _oracle_result(job))
+        assert err <= SERVE_TOL, (job.protocol.name, err)
+    eng.close()

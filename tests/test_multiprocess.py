@@ -1,0 +1,75 @@
+"""The multi-rank path on CPU with gloo, world size 2: every rank takes its
+own batch or jobs (no data crosses ranks) and the reported time is the
+slowest rank's.  Ranks are spawned processes; the rendezvous is on
+127.0.0.1."""
+import os
+import socket
+
+import pytest
+
+torch = pytest.importorskip("torch")
+mp = torch.multiprocessing
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    import sys
+
+    import numpy as np
+    import torch.distributed as dist
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    from ctprojector_b200 import synthetic as S
+    from ctprojector_b200.serving.scheduler import shard
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, init_method=f"tcp://127.0.0.1:{port}",
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        slowest = bench.max_over_ranks(10.0 + 5.0 * rank, torch.device("cpu"))
+        # each rank's batch seed, and a checksum of a small phantom made from it
+        rng = np.random.default_rng(S.seed_for(2, rank))
+        img = S.ellipse_phantom(rng, 32, 32, 1.0, 1.0)
+        mine = shard(list(range(11)), rank, world)
+        q.put((rank, slowest, float(img.sum()), mine))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_max_time_and_disjoint_shards():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    try:
+        for _ in range(world):
+            rank, slowest, checksum, mine = q.get(timeout=120)
+            out[rank] = (slowest, checksum, mine)
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    assert out[0][0] == out[1][0] == 15.0  # both ranks report the slowest rank's time
+    assert out[0][1] != out[1][1]  # independent batches
+    a, b = out[0][2], out[1][2]
+    assert sorted(a + b) == list(range(11)) and not set(a) & set(b)
+
+
+def test_max_over_ranks_without_process_group():
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    assert bench.max_over_ranks(3.5, torch.device("cpu")) == 3.5

@@ -5,7 +5,8 @@ import random
 
 import pytest
 
-from ctprojector_b200.serving.scheduler import ArrivalQueue, LatencyStats, MemoryBudget, Pending, SlotPool, bucket
+from ctprojector_b200.serving.scheduler import (ArrivalQueue, LatencyStats, MemoryBudget, Pending, SlotPool, bucket,
+                                                bucket_sizes)
 
 
 def test_slot_pool_first_fit_and_free():
@@ -76,8 +77,11 @@ def test_slot_pool_rejects_bad_requests():
 
 
 def test_bucket_sizes():
-    assert [bucket(n, 64) for n in (0, 1, 2, 3, 5, 16, 17, 63, 64)] == [0, 1, 2, 4, 8, 16, 32, 64, 64]
-    assert bucket(40, 48) == 48
+    assert [bucket(n, 64) for n in (0, 1, 2, 3, 5, 16, 17, 63, 64)] == [0, 1, 2, 3, 5, 16, 17, 63, 64]
+    assert [bucket(n, 64, 4) for n in (1, 4, 5, 17, 61, 64)] == [4, 4, 8, 20, 64, 64]
+    assert bucket(47, 46, 4) == 46
+    assert bucket_sizes(10, 4) == [4, 8, 10]
+    assert bucket_sizes(3) == [1, 2, 3]
 
 
 def test_memory_budget():
