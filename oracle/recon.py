@@ -60,17 +60,20 @@ def _layout(p, kind, y):
     return y, img_shape, zl
 
 
-def sqs_tv(p, kind, y, geo, n_iter, beta, weights, eps=1e-8):
-    """FP64 SQS-TV reconstruction of one job; returns [nz, ny, nx]."""
+def sqs_tv(p, kind, y, geo, n_iter, beta, weights, eps=1e-8, callback=None):
+    """FP64 SQS-TV reconstruction of one job; returns [nz, ny, nx].
+    ``callback(k, x)`` (optional) sees every iterate k = 1..n_iter."""
     y, shape, zl = _layout(p, kind, y)
     one = np.ones((1,) + shape[1:])
     norm = _bp(p, kind, _fp(p, kind, one, geo), geo).reshape(-1, shape[-2], shape[-1])
     x = np.zeros(shape)
-    for _ in range(n_iter):
+    for k in range(n_iter):
         r = _fp(p, kind, x, geo) - y
         bp = _bp(p, kind, r, geo)
         x = O.sqs_tv_update(x.reshape(-1, shape[-2], shape[-1]), bp.reshape(-1, shape[-2], shape[-1]), norm, zl,
                             weights, beta, eps).reshape(shape)
+        if callback is not None:
+            callback(k + 1, x.reshape(-1, shape[-2], shape[-1]))
     return x.reshape(-1, shape[-2], shape[-1])
 
 
