@@ -450,7 +450,153 @@ def run_reference(args, rank, world, local):
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "copies_inside_reference_calls_bytes": 4 * (img.size + 3 * n_prj) + 4 * (2 * n_prj + 2 * img.size)},
         "clocks": clk.summary(),
+        "served": None if args.no_served else run_reference_served(),
     }
+
+
+class _RefDD:
+    """The reference library's device-pointer DD entries and filters for one
+    2D protocol, called with the argument conventions of its cupy wrappers
+    (fan_equiangular.py:19-256, parallel.py:19-254): outputs allocated
+    zero-filled per call, back projections accumulate into them."""
+
+    def __init__(self, L, scan, kind, angles):
+        import torch
+
+        self.L, self.s, self.fan = L, scan, kind == "fan"
+        self.ang = torch.tensor(angles, device="cuda")
+
+    def _geo(self, nb, nu, nview):
+        from ctypes import c_float, c_ulong
+
+        s = self.s
+        g = [c_ulong(nb), c_ulong(s.nx), c_ulong(s.ny), c_ulong(1), c_float(s.dx), c_float(s.dy), c_float(s.dz),
+             c_float(s.cx), c_float(s.cy), c_float(s.cz), c_ulong(nu), c_ulong(1), c_ulong(nview)]
+        if self.fan:
+            return g + [c_float(s.du / s.dsd), c_float(s.dv), c_float(s.off_u), c_float(s.off_v), c_float(s.dsd),
+                        c_float(s.dso)]
+        return g + [c_float(s.du), c_float(s.dv), c_float(s.off_u), c_float(s.off_v)]
+
+    def fp(self, x):
+        import torch
+        from ctypes import c_int, c_void_p
+
+        nb, nview = x.shape[0], self.ang.numel()
+        out = torch.zeros(nb, nview, 1, self.s.nu, device="cuda")
+        f = self.L.cupyDistanceDrivenFanProjection if self.fan else self.L.cupyDistanceDrivenParallelProjection
+        rc = f(c_void_p(out.data_ptr()), c_void_p(x.data_ptr()), c_void_p(self.ang.data_ptr()),
+               *self._geo(nb, self.s.nu, nview), c_int(0))
+        assert rc == 0, rc
+        return out
+
+    def bp(self, y, fbp=False):
+        import torch
+        from ctypes import c_int, c_void_p
+
+        nb, nview = y.shape[0], y.shape[1]
+        out = torch.zeros(nb, 1, self.s.ny, self.s.nx, device="cuda")
+        f = self.L.cupyDistanceDrivenFanBackprojection if self.fan else self.L.cupyDistanceDrivenParallelBackprojection
+        rc = f(c_void_p(out.data_ptr()), c_void_p(y.data_ptr()), c_void_p(self.ang.data_ptr()),
+               *self._geo(nb, y.shape[3], nview), c_int(1 if fbp else 0))
+        assert rc == 0, rc
+        return out
+
+    def filt(self, y):
+        import torch
+        from ctypes import c_float, c_int, c_ulong, c_void_p
+
+        s = self.s
+        out = torch.zeros_like(y)
+        head = [c_void_p(out.data_ptr()), c_void_p(y.data_ptr()), c_int(y.shape[0]), c_ulong(y.shape[3]),
+                c_ulong(y.shape[2]), c_ulong(y.shape[1])]
+        if self.fan:  # fan_equiangular.py:19-71, 'hann' = 2
+            rc = self.L.cupyfbpFanFilter(*head, c_float(s.du / s.dsd), c_float(s.dv), c_float(s.off_u),
+                                         c_float(s.off_v), c_float(s.dsd), c_float(s.dso), c_int(2))
+        else:  # parallel.py:19-71
+            rc = self.L.cupyfbpParallelFilter(*head, c_float(s.du), c_float(s.dv), c_float(s.off_u), c_float(s.off_v),
+                                              c_int(2))
+        assert rc == 0, rc
+        return out
+
+
+def run_reference_served():
+    """The served 2D job stream of the ours arm (same seeded arrivals, mix and
+    slice counts; sinograms made here with the reference's own projector and
+    the same noise model) through the reference's per-call path: its cupy
+    entries for FP, BP and the filters and its TV prior (cupyTVSQS3D), FP32,
+    array arithmetic in between, one job at a time."""
+    import ctypes
+
+    import torch
+    from ctypes import c_float, c_ulong, c_void_p
+
+    from ctprojector_b200 import synthetic as S
+    from ctprojector_b200.serving import workload as W
+    from ctprojector_b200.serving.scheduler import LatencyStats
+
+    lp = os.path.join(ROOT, "oracle", "_ref", "libprojector.so")
+    tp = os.path.join(ROOT, "oracle", "_ref", "libprior.so")
+    if not (os.path.exists(lp) and os.path.exists(tp)):
+        return {"unavailable": "oracle/_ref/libprojector.so or libprior.so not built"}
+    L, T = ctypes.CDLL(lp), ctypes.CDLL(tp)
+    protos = W.catalog(storage="float32")
+    stream = W.arrivals(SERVED_JOBS, SERVED_RATE_HZ, SERVED_SEED, W.MIX_2D)
+    names = sorted({n for _, n, _ in stream})
+    ops = {n: _RefDD(L, protos[n].scan, protos[n].kind, protos[n].angles) for n in names}
+    pools = {}
+    for i, n in enumerate(names):
+        rng = np.random.default_rng(i)
+        sc = protos[n].scan
+        pools[n] = []
+        for _ in range(2):
+            img = np.stack([S.ellipse_phantom(rng, sc.nx, sc.ny, sc.dx, sc.dy)[None] for _ in range(16)])
+            y = ops[n].fp(torch.tensor(img, device="cuda")).cpu().numpy()
+            pools[n].append(torch.tensor(S.poisson_log(y, 1e5, rng)).pin_memory())
+    rng = np.random.default_rng(0)
+    jobs = [(t, n, nz, pools[n][int(rng.integers(2))][:nz]) for t, n, nz in stream]
+
+    def tv(x, w, eps):  # prior/cupy/recon_prior.py:85-135
+        s1, s2, var = torch.zeros_like(x), torch.zeros_like(x), torch.zeros_like(x)
+        rc = T.cupyTVSQS3D(c_void_p(s1.data_ptr()), c_void_p(s2.data_ptr()), c_void_p(var.data_ptr()),
+                           c_void_p(x.data_ptr()), c_float(w[2]), c_float(w[1]), c_float(w[0]), c_ulong(x.shape[0]),
+                           c_ulong(x.shape[3]), c_ulong(x.shape[2]), c_ulong(x.shape[1]), c_float(eps))
+        assert rc == 0, rc
+        return s1, s2
+
+    def reconstruct(n, ysino):
+        pr, op = protos[n], ops[n]
+        y = ysino.cuda()
+        if pr.algo == "fbp":
+            return op.bp(op.filt(y), True).cpu()
+        sc = pr.scan
+        nz = y.shape[0]
+        norm = op.bp(op.fp(torch.ones(1, 1, sc.ny, sc.nx, device="cuda")))
+        x = torch.zeros(nz, 1, sc.ny, sc.nx, device="cuda")
+        for _ in range(pr.n_iter):
+            g = op.bp(op.fp(x) - y)
+            s1, s2 = tv(x.reshape(1, nz, sc.ny, sc.nx).contiguous(), pr.tv_weights, pr.eps)
+            x = x - (g + pr.beta * s1.reshape(x.shape)) / (norm + pr.beta * s2.reshape(x.shape))
+        return x.cpu()
+
+    for n in names:  # first-call costs outside the stream
+        reconstruct(n, pools[n][0][:1])
+    torch.cuda.synchronize()
+    stats = LatencyStats()
+    t0 = time.perf_counter()
+    for t, n, nz, ysino in jobs:
+        wait = t - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        reconstruct(n, ysino)
+        torch.cuda.synchronize()
+        done = time.perf_counter() - t0
+        stats.add(done - t, done)
+    sm = stats.summary(0.0)
+    r = lambda x: round(x, 3)  # noqa: E731
+    return {"recons_per_s": r(sm["recons_per_s"]), "p50_ms": r(sm["p50_ms"]), "p99_ms": r(sm["p99_ms"]),
+            "jobs": sm["jobs"], "arrival_rate_hz": SERVED_RATE_HZ,
+            "path": "reference libprojector.so + libprior.so (built from its sources for sm_100a), cupy entries, "
+                    "FP32, one call per operation, one job at a time"}
 
 
 def main(argv=None):

@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <type_traits>
 #include <mutex>
 
 #include "ctp_common.cuh"
@@ -870,21 +871,25 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     return false;
 }
 
-template <bool FAN, int NI, typename Tout>
+// S slices of the same geometry per CTA (S > 1 for stacks): the edge
+// positions, their rounding to table indices and the footprint widths are
+// the same for every slice, so they are computed once and only the table
+// lookups, shuffles and sums repeat per slice.
+template <bool FAN, int NI, int S, typename Tout>
 __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
                                                              const float4* __restrict__ ltab1, DDTab tab, Grid g,
-                                                             Det d, int nview, int vgroup, int rchunk,
+                                                             Det d, int nview, int vgroup, int rchunk, int nslices,
                                                              const float* __restrict__ deg, int unweight_par) {
-    extern __shared__ float4 s_ring[];  // [2][rchunk * (max(nx, ny) + 1)]
+    extern __shared__ float4 s_ring[];  // [2][S][rchunk][max(nx, ny) + 1]
     __shared__ __align__(8) unsigned long long s_bar[2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int v0 = blockIdx.x * vgroup;
     const int nvg = min(vgroup, nview - v0);
-    const int slice = blockIdx.y;  // b * nz + iz, detector row iv = iz
-    const int iz = slice % g.nz, b = slice / g.nz;
+    const int s0 = blockIdx.y * S;  // first slice (b * nz + iz) of this CTA
+    const int ns = min(S, nslices - s0);
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
     const int nitems = nvg * ipv;
-    const size_t ring = (size_t)rchunk * (max(g.nx, g.ny) + 1);
+    const size_t ring = (size_t)S * rchunk * (max(g.nx, g.ny) + 1);
 
     // orientations with work in this CTA: rows (o = 0) for views traced along
     // y, columns (o = 1) for views traced along x, both in the blend band
@@ -899,8 +904,6 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
     const int nc0 = act0 ? (g.ny + rchunk - 1) / rchunk : 0;
     const int nc1 = act1 ? (g.nx + rchunk - 1) / rchunk : 0;
     const int K = nc0 + nc1;
-    const float4* src0 = ltab0 + (size_t)slice * g.ny * (g.nx + 1);
-    const float4* src1 = ltab1 + (size_t)slice * g.nx * (g.ny + 1);
 
     auto issue = [&](int k) {
         const int o = k < nc0 ? 0 : 1;
@@ -909,8 +912,13 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
         const unsigned bytes = (unsigned)((size_t)nlc * (n + 1) * sizeof(float4));
         unsigned long long* bar = &s_bar[k & 1];
-        mbar_expect_tx(bar, bytes);
-        bulk_copy_g2s(s_ring + (k & 1) * ring, (o == 0 ? src0 : src1) + (size_t)l0 * (n + 1), bytes, bar);
+        mbar_expect_tx(bar, bytes * (unsigned)ns);
+        for (int s = 0; s < ns; ++s) {
+            const float4* src = o == 0 ? ltab0 + (size_t)(s0 + s) * g.ny * (g.nx + 1)
+                                       : ltab1 + (size_t)(s0 + s) * g.nx * (g.ny + 1);
+            bulk_copy_g2s(s_ring + (k & 1) * ring + (size_t)s * rchunk * (n + 1), src + (size_t)l0 * (n + 1), bytes,
+                          bar);
+        }
     };
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);
@@ -923,7 +931,7 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         if (K > 1) issue(1);
     }
 
-    float A[NI], B[NI], acc[NI];
+    float A[NI], B[NI], acc[S][NI];
     bool failed = false;
     int k = 0;
     for (; k < K; ++k) {
@@ -938,7 +946,8 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
                 // dummy edge positions keep every width non-zero
                 A[q] = (float)lane - 0.5f;
                 B[q] = 0.f;
-                acc[q] = 0.f;
+#pragma unroll
+                for (int s = 0; s < S; ++s) acc[s][q] = 0.f;
                 if (it < nitems) {
                     const int vi = it / ipv, m = it - vi * ipv;
                     const int view = v0 + vi;
@@ -958,6 +967,7 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
         const float lo_lim = -0.5f, hi_lim = (float)n - 0.5f;
+        const size_t sstride = (size_t)rchunk * (n + 1);
         for (int r = 0; r < nlc && !failed; ++r) {
             const float t = (float)(l0 + r - anchor);
             const float4* T = buf + (size_t)r * (n + 1);
@@ -966,14 +976,22 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
                 const float xr = fmaf(B[q], t, A[q]);  // edge position - 1/2
                 const float xs = clampf(xr, lo_lim, hi_lim);
                 const float tt = xs + kRoundMagic;
-                const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
-                const float hi = e.x, lo = fmaf(e.z, xs - (tt - kRoundMagic), e.y);
-                const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
-                const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
+                const int idx = __float_as_int(tt) - kRoundMagicBits;
+                const float fr = xs - (tt - kRoundMagic);
                 const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
-                // signed integral over [x_j, x_j+1] over the signed width of
-                // the rounded footprint
-                acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
+                const float w = xn - xr;
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    if (s < ns) {
+                        const float4 e = T[s * sstride + idx];
+                        const float hi = e.x, lo = fmaf(e.z, fr, e.y);
+                        const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
+                        const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
+                        // signed integral over [x_j, x_j+1] over the signed width of
+                        // the rounded footprint
+                        acc[s][q] += __fdividef((hin - hi) + (lon - lo), w);
+                    }
+                }
             }
         }
         if (c == last && !failed) {
@@ -987,10 +1005,16 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
                 const float wx = tab.wx[view];
                 const bool active = o == 0 ? wx > 0.f : wx < 1.f;
                 if (!active || lane >= 31 || kk >= d.nu) continue;
-                float v = acc[q] * tab.cL[o][(size_t)view * d.nu + kk] * (o == 0 ? wx : 1.f - wx);
-                Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
-                if (o == 1 && wx > 0.f) v += rdf(dst);  // the row pass of this view wrote first
-                stf(dst, v);
+                const float wl = tab.cL[o][(size_t)view * d.nu + kk] * (o == 0 ? wx : 1.f - wx);
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    if (s >= ns) continue;
+                    const int slice = s0 + s, iz = slice % g.nz, b = slice / g.nz;
+                    float v = acc[s][q] * wl;
+                    Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
+                    if (o == 1 && wx > 0.f) v += rdf(dst);  // the row pass of this view wrote first
+                    stf(dst, v);
+                }
             }
         }
         // every warp is done with buffer k & 1 before it is refilled
@@ -1016,8 +1040,12 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
             if (lane >= 31 || kk >= d.nu) continue;
             float sn, cs;
             sincosf(deg[view], &sn, &cs);
-            Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
-            stf(dst, rdf(dst) / (ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn)));
+            const float wr = ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn);
+            for (int s = 0; s < ns; ++s) {
+                const int slice = s0 + s, iz = slice % g.nz, b = slice / g.nz;
+                Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
+                stf(dst, rdf(dst) / wr);
+            }
         }
     }
 }
@@ -1054,25 +1082,30 @@ struct ParView {
     float sy, jc, hx, hy;  // sx, sy: signed normalisations (0 = term inactive); jc: absolute coordinate
 };
 
-inline size_t par_fast_smem(int win) {
-    return (size_t)kPViews * (win + 1) * sizeof(float2) + kPViews * sizeof(ParView) + kPViews * sizeof(int) +
-           kPT * (kPT + 1) * sizeof(float);
+inline size_t par_fast_smem(int win, int S) {
+    return (size_t)S * kPViews * (win + 1) * sizeof(float2) + kPViews * sizeof(ParView) + kPViews * sizeof(int) +
+           (size_t)S * kPT * (kPT + 1) * sizeof(float);
 }
 
-template <typename Tp, typename Tout>
+// S slices of the same geometry per CTA: the per-view constants, the edge
+// positions and each lookup's index and fraction are shared; only the table
+// reads and the sums repeat per slice.
+template <typename Tp, typename Tout, int S>
 __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ prj,
                                                                const float* __restrict__ deg, int nview, Grid g,
-                                                               Det d, int fbp, int accumulate, int win) {
+                                                               Det d, int fbp, int accumulate, int win,
+                                                               int nslices) {
     extern __shared__ float4 smem_f4[];
     const int stride = win + 1;
-    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                  // [kPViews][stride]
-    ParView* s_par = reinterpret_cast<ParView*>(s_tab + kPViews * stride);  // 16-byte aligned: 256 * stride bytes before
-    int* s_w0 = reinterpret_cast<int*>(s_par + kPViews);                 // window start, INT_MIN = not staged
-    float* s_acc = reinterpret_cast<float*>(s_w0 + kPViews);             // [kPT][kPT + 1] merge buffer
+    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                       // [S][kPViews][stride]
+    ParView* s_par = reinterpret_cast<ParView*>(s_tab + S * kPViews * stride);  // 16-byte aligned: 256 * S * stride bytes before
+    int* s_w0 = reinterpret_cast<int*>(s_par + kPViews);                      // window start, INT_MIN = not staged
+    float* s_acc = reinterpret_cast<float*>(s_w0 + kPViews);                  // [S][kPT][kPT + 1] merge buffer
 
     const int tiles_x = (g.nx + kPT - 1) / kPT;
     const int tx0 = (blockIdx.x % tiles_x) * kPT, ty0 = (blockIdx.x / tiles_x) * kPT;
-    const int iz = blockIdx.y % g.nz, b = blockIdx.y / g.nz;
+    const int s0 = blockIdx.y * S;  // first slice (b * nz + iz) of this CTA
+    const int ns = min(S, nslices - s0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // x-layout: 4 pixels along x; a half warp spans 16 columns x 4 rows, so its
     // table reads fall on distinct banks.  y-layout: 4 pixels along y, lane = column.
@@ -1080,14 +1113,28 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
     const int xl_col = ((lane >> 4) * 4 + (lane & 3)) * 4;
     const int yl_col = lane, yl_row = warp * 4;
 
-    float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
-    int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);  // truncation, :383
-    bool row_ok = iv >= 0 && iv < d.nv;
-    float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
-    const Tp* rows = prj + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
+    // detector row of each slice (truncation, :383); a slice off the detector stages zeros
+    const Tp* rows[S];
+    bool row_ok[S];
+    bool any_row = false;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int slice = s0 + min(s, ns - 1), iz = slice % g.nz, b = slice / g.nz;
+        const float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
+        const int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);
+        row_ok[s] = s < ns && iv >= 0 && iv < d.nv;
+        rows[s] = prj + ((size_t)b * nview * d.nv + (row_ok[s] ? iv : 0)) * d.nu;
+        any_row |= row_ok[s];
+    }
+    float ax[S][4], ay[S][4];
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ax[s][k] = ay[s][k] = 0.f;
     const size_t vstride = (size_t)d.nv * d.nu;
+    const size_t tstride = (size_t)kPViews * stride;  // per slice
 
-    for (int v0 = 0; v0 < nview && row_ok; v0 += kPViews) {
+    for (int v0 = 0; v0 < nview && any_row; v0 += kPViews) {
         const int nvc = min(kPViews, nview - v0);
         if (threadIdx.x < nvc) {
             const int vi = threadIdx.x, view = v0 + vi;
@@ -1128,9 +1175,19 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
         }
         __syncthreads();
         // stage (running sum + value/2, value) for window cells w0 .. w0+win-1; entry win = (total, 0)
-        for (int vi = warp; vi < nvc; vi += 8) {
+        for (int sv = warp; sv < S * nvc; sv += 8) {
+            const int s = sv / nvc, vi = sv - s * nvc;
             const int w0 = s_w0[vi];
-            const bool ok = w0 != INT_MIN;
+            bool ok = w0 != INT_MIN;
+            const Tp* srow = rows[0];
+            bool rok = row_ok[0];
+#pragma unroll
+            for (int q = 1; q < S; ++q)
+                if (s == q) {
+                    srow = rows[q];
+                    rok = row_ok[q];
+                }
+            ok = ok && rok;
             const int view = v0 + vi;
             const int per = (stride + 31) / 32;
             const int k0 = lane * per;
@@ -1142,7 +1199,7 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
                 float x = 0.f;
                 if (ok && q < per && k < win) {
                     int cell = w0 + k;
-                    if (cell >= 0 && cell < d.nu) x = ldf(rows + (size_t)view * vstride + cell);
+                    if (cell >= 0 && cell < d.nu) x = ldf(srow + (size_t)view * vstride + cell);
                 }
                 v[q] = x;
                 run += x;
@@ -1154,7 +1211,7 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
                 if (lane >= o) incl += t;
             }
             float base = incl - run;
-            float2* T = s_tab + vi * stride;
+            float2* T = s_tab + s * tstride + vi * stride;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 int k = k0 + q;
@@ -1169,35 +1226,63 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
             if (s_w0[vi] != INT_MIN) {
                 if (P.sx != 0.f) {
                     const float e0 = fmaf((float)xl_col - 0.5f, P.jx, fmaf((float)xl_row, P.jy, P.jb));
-                    float f[5];
+                    float f[S][5];
 #pragma unroll
-                    for (int k = 0; k < 5; ++k) f[k] = prefix_eval_mid(T, fmaf((float)k, P.jx, e0));
+                    for (int k = 0; k < 5; ++k) {
+                        const float xs = fmaf((float)k, P.jx, e0);
+                        const float tt = xs + kRoundMagic;
+                        const int i = __float_as_int(tt) - kRoundMagicBits;
+                        const float fr = xs - (tt - kRoundMagic);
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) ax[k] = fmaf(f[k + 1] - f[k], P.sx, ax[k]);
+                        for (int s = 0; s < S; ++s) {
+                            const float2 e = T[s * tstride + i];
+                            f[s][k] = fmaf(e.y, fr, e.x);
+                        }
+                    }
+#pragma unroll
+                    for (int s = 0; s < S; ++s)
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) ax[s][k] = fmaf(f[s][k + 1] - f[s][k], P.sx, ax[s][k]);
                 }
                 if (P.sy != 0.f) {
                     const float e0 = fmaf((float)yl_row - 0.5f, P.jy, fmaf((float)yl_col, P.jx, P.jb));
-                    float f[5];
+                    float f[S][5];
 #pragma unroll
-                    for (int k = 0; k < 5; ++k) f[k] = prefix_eval_mid(T, fmaf((float)k, P.jy, e0));
+                    for (int k = 0; k < 5; ++k) {
+                        const float xs = fmaf((float)k, P.jy, e0);
+                        const float tt = xs + kRoundMagic;
+                        const int i = __float_as_int(tt) - kRoundMagicBits;
+                        const float fr = xs - (tt - kRoundMagic);
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) ay[k] = fmaf(f[k + 1] - f[k], P.sy, ay[k]);
+                        for (int s = 0; s < S; ++s) {
+                            const float2 e = T[s * tstride + i];
+                            f[s][k] = fmaf(e.y, fr, e.x);
+                        }
+                    }
+#pragma unroll
+                    for (int s = 0; s < S; ++s)
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) ay[s][k] = fmaf(f[s][k + 1] - f[s][k], P.sy, ay[s][k]);
                 }
             } else {
-                // window larger than the staging buffer: integrate the row in global memory
-                const Tp* grow = rows + (size_t)(v0 + vi) * vstride;
-                if (P.sx != 0.f) {
+                // window larger than the staging buffer: integrate the rows in global memory
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        float jc = P.jc + (float)(xl_col + k) * P.jx + (float)xl_row * P.jy;
-                        ax[k] += box_line(grow, 1, jc - P.hx, jc + P.hx, d.nu) * fabsf(P.sx);
+                for (int s = 0; s < S; ++s) {
+                    if (!row_ok[s]) continue;
+                    const Tp* grow = rows[s] + (size_t)(v0 + vi) * vstride;
+                    if (P.sx != 0.f) {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            float jc = P.jc + (float)(xl_col + k) * P.jx + (float)xl_row * P.jy;
+                            ax[s][k] += box_line(grow, 1, jc - P.hx, jc + P.hx, d.nu) * fabsf(P.sx);
+                        }
                     }
-                }
-                if (P.sy != 0.f) {
+                    if (P.sy != 0.f) {
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        float jc = P.jc + (float)yl_col * P.jx + (float)(yl_row + k) * P.jy;
-                        ay[k] += box_line(grow, 1, jc - P.hy, jc + P.hy, d.nu) * fabsf(P.sy);
+                        for (int k = 0; k < 4; ++k) {
+                            float jc = P.jc + (float)yl_col * P.jx + (float)(yl_row + k) * P.jy;
+                            ay[s][k] += box_line(grow, 1, jc - P.hy, jc + P.hy, d.nu) * fabsf(P.sy);
+                        }
                     }
                 }
             }
@@ -1206,17 +1291,24 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
     }
     // add the x-layout sums to the y-layout ones and store rows coalesced
 #pragma unroll
-    for (int k = 0; k < 4; ++k) s_acc[xl_row * (kPT + 1) + xl_col + k] = ax[k];
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s_acc[(s * kPT + xl_row) * (kPT + 1) + xl_col + k] = ax[s][k];
     __syncthreads();
     const int ix = tx0 + yl_col;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int iy = ty0 + yl_row + k;
-        if (ix < g.nx && iy < g.ny) {
-            Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
-            float a = ay[k] + s_acc[(yl_row + k) * (kPT + 1) + yl_col];
-            if (accumulate) a += rdf(o);
-            stf(o, a);
+    for (int s = 0; s < S; ++s) {
+        if (s >= ns) continue;
+        const int slice = s0 + s, iz = slice % g.nz, b = slice / g.nz;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int iy = ty0 + yl_row + k;
+            if (ix < g.nx && iy < g.ny) {
+                Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+                float a = ay[s][k] + s_acc[(s * kPT + yl_row + k) * (kPT + 1) + yl_col];
+                if (accumulate) a += rdf(o);
+                stf(o, a);
+            }
         }
     }
 }
@@ -1239,33 +1331,48 @@ struct FanView {
     int ym;  // x-edges at the centre row (1) or y-edges at the centre column (0)
 };
 
-inline size_t fan_fast_smem(int win) {
-    return (size_t)kPViews * (win + 1) * sizeof(float2) + kPViews * sizeof(FanView) + kPT * (kPT + 1) * sizeof(float);
+inline size_t fan_fast_smem(int win, int S) {
+    return (size_t)S * kPViews * (win + 1) * sizeof(float2) + kPViews * sizeof(FanView) +
+           (size_t)S * kPT * (kPT + 1) * sizeof(float);
 }
 
-template <typename Tp, typename Tout>
+// S slices of the same geometry per CTA: the atan mappings of the edge points,
+// the footprint widths, the FBP weights and each lookup's index and fraction
+// are shared; only the table reads and sums repeat per slice.
+template <typename Tp, typename Tout, int S>
 __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ src,
                                                                const float* __restrict__ deg, int nview, Grid g,
-                                                               Det d, float dso, int fbp, int accumulate, int win) {
+                                                               Det d, float dso, int fbp, int accumulate, int win,
+                                                               int nslices) {
     extern __shared__ float4 smem_f4[];
     const int stride = win + 1;
-    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                    // [kPViews][stride]
-    FanView* s_view = reinterpret_cast<FanView*>(s_tab + kPViews * stride);
-    float* s_acc = reinterpret_cast<float*>(s_view + kPViews);             // [kPT][kPT + 1] merge buffer
+    float2* s_tab = reinterpret_cast<float2*>(smem_f4);                        // [S][kPViews][stride]
+    FanView* s_view = reinterpret_cast<FanView*>(s_tab + S * kPViews * stride);
+    float* s_acc = reinterpret_cast<float*>(s_view + kPViews);                 // [S][kPT][kPT + 1] merge buffer
 
     const int tiles_x = (g.nx + kPT - 1) / kPT;
     const int tx0 = (blockIdx.x % tiles_x) * kPT, ty0 = (blockIdx.x / tiles_x) * kPT;
-    const int iz = blockIdx.y % g.nz, b = blockIdx.y / g.nz;
+    const int s0 = blockIdx.y * S;
+    const int ns = min(S, nslices - s0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int xl_row = warp * 4 + ((lane >> 2) & 3);
     const int xl_col = ((lane >> 4) * 4 + (lane & 3)) * 4;
     const int yl_col = lane, yl_row = warp * 4;
 
-    float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
-    int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);
-    bool row_ok = iv >= 0 && iv < d.nv;
-    const Tp* rows = src + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
+    const Tp* rows[S];
+    bool row_ok[S];
+    bool any_row = false;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int slice = s0 + min(s, ns - 1), iz = slice % g.nz, b = slice / g.nz;
+        const float zc = ((float)iz - g.nz / 2.f) * g.dz + g.cz + g.dz / 2;
+        const int iv = (int)(zc / d.dv + d.off_v + d.nv / 2.f - 0.5f);
+        row_ok[s] = s < ns && iv >= 0 && iv < d.nv;
+        rows[s] = src + ((size_t)b * nview * d.nv + (row_ok[s] ? iv : 0)) * d.nu;
+        any_row |= row_ok[s];
+    }
     const size_t vstride = (size_t)d.nv * d.nu;
+    const size_t tstride = (size_t)kPViews * stride;
     const float hdx = g.dx / 2.0f, hdy = g.dy / 2.0f;
     // x-layout: pixel centres (xs0 + k dx, ysx); y-layout: (xsy, ys0 + k dy)
     const float xs0 = ((float)(tx0 + xl_col) - g.nx / 2.f) * g.dx + g.cx + hdx;
@@ -1274,9 +1381,13 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
     const float ys0 = ((float)(ty0 + yl_row) - g.ny / 2.f) * g.dy + g.cy + hdy;
     const float jscale = -1.f / d.du, joff = -d.off_u + d.nu / 2.0f;
     const float dso2 = dso * dso;
-    float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
+    float ax[S][4], ay[S][4];
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ax[s][k] = ay[s][k] = 0.f;
 
-    for (int v0 = 0; v0 < nview && row_ok; v0 += kPViews) {
+    for (int v0 = 0; v0 < nview && any_row; v0 += kPViews) {
         const int nvc = min(kPViews, nview - v0);
         if (threadIdx.x < nvc) {
             const int vi = threadIdx.x, view = v0 + vi;
@@ -1310,9 +1421,18 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
             s_view[vi] = V;
         }
         __syncthreads();
-        for (int vi = warp; vi < nvc; vi += 8) {
+        for (int sv = warp; sv < S * nvc; sv += 8) {
+            const int s = sv / nvc, vi = sv - s * nvc;
             const int w0 = s_view[vi].w0;
-            const bool ok = w0 != INT_MIN;
+            const Tp* srow = rows[0];
+            bool rok = row_ok[0];
+#pragma unroll
+            for (int q = 1; q < S; ++q)
+                if (s == q) {
+                    srow = rows[q];
+                    rok = row_ok[q];
+                }
+            const bool ok = w0 != INT_MIN && rok;
             const int view = v0 + vi;
             const int per = (stride + 31) / 32;
             const int k0 = lane * per;
@@ -1324,7 +1444,7 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
                 float x = 0.f;
                 if (ok && q < per && k < win) {
                     int cell = w0 + k;
-                    if (cell >= 0 && cell < d.nu) x = ldf(rows + (size_t)view * vstride + cell);
+                    if (cell >= 0 && cell < d.nu) x = ldf(srow + (size_t)view * vstride + cell);
                 }
                 v[q] = x;
                 run += x;
@@ -1336,7 +1456,7 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
                 if (lane >= o) incl += t;
             }
             float base = incl - run;
-            float2* T = s_tab + vi * stride;
+            float2* T = s_tab + s * tstride + vi * stride;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 int k = k0 + q;
@@ -1348,8 +1468,7 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
         for (int vi = 0; vi < nvc; ++vi) {
             const FanView V = s_view[vi];
             const float2* T = s_tab + vi * stride;
-            const Tp* grow = rows + (size_t)(v0 + vi) * vstride;
-            const float fw0 = (float)V.w0 + 0.5f;  // window origin, shifted for prefix_eval_mid
+            const float fw0 = (float)V.w0 + 0.5f;  // window origin, shifted for the midpoint tables
             // edge points p_k = p_0 + k * step, k = 0..4, rotated: (rx, ry)
             float px, py, sx, sy;
             if (V.ym) {
@@ -1365,49 +1484,78 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
                 const float rx = fmaf((float)k, drx, rx0), ry = fmaf((float)k, dry, ry0);
                 j[k] = fmaf(atanf(rx / (ry + dso)), jscale, joff);
             }
-            float val[4];
-            if (V.w0 != INT_MIN) {
-                float f[5];
+            float wgt[4];
 #pragma unroll
-                for (int k = 0; k < 5; ++k) f[k] = prefix_eval_mid(T, j[k] - fw0);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) val[k] = __fdividef(f[k + 1] - f[k], j[k + 1] - j[k]);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float lo = fminf(j[k], j[k + 1]), hi = fmaxf(j[k], j[k + 1]);
-                    val[k] = __fdividef(box_line(grow, 1, lo, hi, d.nu), hi - lo);
+            for (int k = 0; k < 4; ++k) {
+                wgt[k] = 1.f;
+                if (fbp) {
+                    const float rxc = fmaf((float)k + 0.5f, drx, rx0), ryc = fmaf((float)k + 0.5f, dry, ry0);
+                    wgt[k] = dso2 / (rxc * rxc + (dso + ryc) * (dso + ryc));
                 }
             }
-            if (fbp) {
+            float val[S][4];
+            if (V.w0 != INT_MIN) {
+                float f[S][5];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float rxc = fmaf((float)k + 0.5f, drx, rx0), ryc = fmaf((float)k + 0.5f, dry, ry0);
-                    val[k] *= dso2 / (rxc * rxc + (dso + ryc) * (dso + ryc));
+                for (int k = 0; k < 5; ++k) {
+                    const float xs = j[k] - fw0;
+                    const float tt = xs + kRoundMagic;
+                    const int i = __float_as_int(tt) - kRoundMagicBits;
+                    const float fr = xs - (tt - kRoundMagic);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        const float2 e = T[s * tstride + i];
+                        f[s][k] = fmaf(e.y, fr, e.x);
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < S; ++s)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) val[s][k] = __fdividef(f[s][k + 1] - f[s][k], j[k + 1] - j[k]);
+            } else {
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    const Tp* grow = rows[s] + (size_t)(v0 + vi) * vstride;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float lo = fminf(j[k], j[k + 1]), hi = fmaxf(j[k], j[k + 1]);
+                        val[s][k] = row_ok[s] ? __fdividef(box_line(grow, 1, lo, hi, d.nu), hi - lo) : 0.f;
+                    }
                 }
             }
             if (V.ym) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) ax[k] += val[k];
+                for (int s = 0; s < S; ++s)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) ax[s][k] = fmaf(val[s][k], wgt[k], ax[s][k]);
             } else {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) ay[k] += val[k];
+                for (int s = 0; s < S; ++s)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) ay[s][k] = fmaf(val[s][k], wgt[k], ay[s][k]);
             }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) s_acc[xl_row * (kPT + 1) + xl_col + k] = ax[k];
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s_acc[(s * kPT + xl_row) * (kPT + 1) + xl_col + k] = ax[s][k];
     __syncthreads();
     const int ix = tx0 + yl_col;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int iy = ty0 + yl_row + k;
-        if (ix < g.nx && iy < g.ny) {
-            Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
-            float a = ay[k] + s_acc[(yl_row + k) * (kPT + 1) + yl_col];
-            if (accumulate) a += rdf(o);
-            stf(o, a);
+    for (int s = 0; s < S; ++s) {
+        if (s >= ns) continue;
+        const int slice = s0 + s, iz = slice % g.nz, b = slice / g.nz;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int iy = ty0 + yl_row + k;
+            if (ix < g.nx && iy < g.ny) {
+                Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+                float a = ay[s][k] + s_acc[(s * kPT + yl_row + k) * (kPT + 1) + yl_col];
+                if (accumulate) a += rdf(o);
+                stf(o, a);
+            }
         }
     }
 }
@@ -1492,6 +1640,8 @@ int build_table(float* base, const float* deg, const ctp_geometry& g, int geom, 
 // on its own slice, as for single-slice and matched stacks) and at most
 // kFMaxItems edge groups per warp.
 bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
+    // also reached from the workspace query, before the geometry is validated
+    if (g.nu == 0 || g.nview == 0 || g.nx == 0 || g.ny == 0 || g.nz == 0) return false;
     if (g.nz != g.nv) return false;
     for (size_t iv = 0; iv < g.nv; ++iv) {
         double z = ((double)iv - (g.nv - 1) / 2.0 + g.off_v) * g.dv;
@@ -1503,7 +1653,7 @@ bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
     // of the compiled group counts (4, 8, 12, 16 per warp) with the least waste
     vgroup = 0;
     double best = 1e30;
-    for (int v = 1; v * ipv <= kFMaxItems * 8; ++v) {
+    for (int v = 1; v * ipv <= kFMaxItems * 8 && v <= (int)g.nview; ++v) {
         int per_warp = (v * ipv + 7) / 8;
         int ni = per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : per_warp <= 12 ? 12 : 16;
         double waste = (double)(ni * 8) / (v * ipv) + 0.05 / v;  // prefer more views per staged image
@@ -1517,6 +1667,54 @@ bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
     nrows = 8;
     while (nrows > 1 && nrows * line > 110 * 1024) nrows /= 2;
     return nrows * line <= 200 * 1024;
+}
+
+// View group and edge groups per warp (one of the compiled counts) of the
+// streamed forward projector with S slices per CTA: the most views per CTA
+// whose edge groups fill the 8 warps with the least waste.
+bool fp_stream_shape(const ctp_geometry& g, int S, int& vgroup, int& ni) {
+    static const int kNi1[4] = {4, 8, 12, 16};
+    static const int kNi2[4] = {4, 6, 8, 10};
+    const int* set = S == 1 ? kNi1 : kNi2;
+    const int ipv = (int)((g.nu + 30) / 31);
+    vgroup = 0;
+    ni = 0;
+    if (ipv == 0 || g.nview == 0) return false;
+    double best = 1e30;
+    for (int v = 1; v * ipv <= set[3] * 8 && v <= (int)g.nview; ++v) {
+        const int per_warp = (v * ipv + 7) / 8;
+        int n = 0;
+        for (int i = 0; i < 4 && !n; ++i)
+            if (set[i] >= per_warp) n = set[i];
+        if (!n) continue;
+        const double waste = (double)(n * 8) / (v * ipv) + 0.05 / v;  // prefer more views per table chunk
+        if (waste < best) {
+            best = waste;
+            vgroup = v;
+            ni = n;
+        }
+    }
+    return vgroup > 0;
+}
+
+// Two-slice instances exist for float output only (16-bit outputs use one slice per CTA).
+template <typename Tout, typename L>
+void fp_stream_launch_s2(L& launch, bool fan, int ni) {
+    if constexpr (std::is_same<Tout, float>::value) {
+        if (ni == 4) {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 4, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 4, 2, Tout>);
+        } else if (ni == 6) {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 6, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 6, 2, Tout>);
+        } else if (ni == 8) {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 8, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 8, 2, Tout>);
+        } else {
+            if (fan) launch(dd2d_fp_stream_kernel<true, 10, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 10, 2, Tout>);
+        }
+    } else {
+        (void)launch;
+        (void)fan;
+        (void)ni;
+    }
 }
 
 template <typename Tin, typename Tout>
@@ -1543,26 +1741,36 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         line_tables_kernel<Tin><<<(unsigned)std::min<long long>((cols + 7) / 8, 148 * 16), 256, 0, s>>>(
             lt1, imgT, cols, (int)g.ny);
         if ((rc = check_launch("line_tables_kernel"))) return rc;
-        size_t shm = 2 * (size_t)rchunk * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
-        dim3 fg((unsigned)((g.nview + vgroup - 1) / vgroup), (unsigned)(g.nbatch * g.nz));
-        int ipv = (int)((g.nu + 30) / 31);
-        int per_warp = (vgroup * ipv + 7) / 8;
+        // slices per CTA: 2 for stacks with float output, else 1
+        const int nslices = (int)(g.nbatch * g.nz);
+        int S = (nslices >= 2 && !std::is_same<Tout, __half>::value && !std::is_same<Tout, __nv_bfloat16>::value) ? 2 : 1;
+        int sv = 0, ni = 0;
+        if (!fp_stream_shape(g, S, sv, ni)) {
+            S = 1;
+            fp_stream_shape(g, 1, sv, ni);
+        }
+        const int rc_s = std::max(1, rchunk / S);
+        size_t shm = 2 * (size_t)S * rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+        dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)((nslices + S - 1) / S));
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
             cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-            kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), lt0, lt1, tab, make_grid(g), make_det(g), (int)g.nview,
-                                      vgroup, rchunk, deg, unweight);
+            kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), lt0, lt1, tab, make_grid(g), make_det(g), (int)g.nview, sv,
+                                      rc_s, nslices, deg, unweight);
         };
-        bool fan = geom == 0;
-        if (per_warp <= 4) {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 4, Tout>); else launch(dd2d_fp_stream_kernel<false, 4, Tout>);
-        } else if (per_warp <= 8) {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 8, Tout>); else launch(dd2d_fp_stream_kernel<false, 8, Tout>);
-        } else if (per_warp <= 12) {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 12, Tout>); else launch(dd2d_fp_stream_kernel<false, 12, Tout>);
+        const bool fan = geom == 0;
+#define CTP_FP_STREAM(NI_, S_)                                                   \
+    if (fan) launch(dd2d_fp_stream_kernel<true, NI_, S_, Tout>);                 \
+    else launch(dd2d_fp_stream_kernel<false, NI_, S_, Tout>)
+        if (S == 1) {
+            if (ni == 4) { CTP_FP_STREAM(4, 1); }
+            else if (ni == 8) { CTP_FP_STREAM(8, 1); }
+            else if (ni == 12) { CTP_FP_STREAM(12, 1); }
+            else { CTP_FP_STREAM(16, 1); }
         } else {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 16, Tout>); else launch(dd2d_fp_stream_kernel<false, 16, Tout>);
+            fp_stream_launch_s2<Tout>(launch, fan, ni);
         }
+#undef CTP_FP_STREAM
         return check_launch("dd2d_fp_stream_kernel");
     }
     if (fp_fast_ok(g, vgroup, nrows)) {
@@ -1694,26 +1902,35 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
     if (geom == 0) {
         int fwin = fan_fast_window(g);
         int tiles_f = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
-        size_t fshm = fan_fast_smem(fwin);
-        dim3 fgrid((unsigned)tiles_f, (unsigned)(g.nbatch * g.nz));
+        // two slices per CTA for stacks (shared edge mappings), one otherwise
+        const int nslices = (int)(g.nbatch * g.nz);
+        const int FS = nslices >= 2 ? 2 : 1;
+        size_t fshm = fan_fast_smem(fwin, FS);
+        dim3 fgrid((unsigned)tiles_f, (unsigned)((nslices + FS - 1) / FS));
+        auto fan_fast = [&](auto k1, auto k2, const auto* srcp, int fbp_mode) {
+            if (FS == 2) {
+                cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
+                k2<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), srcp, deg, nview, gr, dt, dso, fbp_mode, accumulate, fwin,
+                                            nslices);
+            } else {
+                cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
+                k1<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), srcp, deg, nview, gr, dt, dso, fbp_mode, accumulate, fwin,
+                                            nslices);
+            }
+            return check_launch("dd2d_bp_fan_fast_kernel");
+        };
         if (fwin > 0 && !fbp) {
             float* wprj = reinterpret_cast<float*>(ws);
             size_t total = g.nbatch * g.nview * g.nv * g.nu;
             fan_preweight_kernel<Tin><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(wprj, cptr<Tin>(prj), deg,
                                                                                     nview, dt, gr, total);
             if ((rc = check_launch("fan_preweight_kernel"))) return rc;
-            auto kf = dd2d_bp_fan_fast_kernel<float, Tout>;
-            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
-            kf<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), wprj, deg, nview, gr, dt, dso, 0, accumulate, fwin);
-            return check_launch("dd2d_bp_fan_fast_kernel");
+            return fan_fast(dd2d_bp_fan_fast_kernel<float, Tout, 1>, dd2d_bp_fan_fast_kernel<float, Tout, 2>,
+                            (const float*)wprj, 0);
         }
-        if (fwin > 0) {
-            auto kf = dd2d_bp_fan_fast_kernel<Tin, Tout>;
-            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
-            kf<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, 1, accumulate,
-                                        fwin);
-            return check_launch("dd2d_bp_fan_fast_kernel");
-        }
+        if (fwin > 0)
+            return fan_fast(dd2d_bp_fan_fast_kernel<Tin, Tout, 1>, dd2d_bp_fan_fast_kernel<Tin, Tout, 2>,
+                            cptr<Tin>(prj), 1);
         if (!fbp) {
             float* wprj = reinterpret_cast<float*>(ws);
             size_t total = g.nbatch * g.nview * g.nv * g.nu;
@@ -1732,11 +1949,22 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
         int pwin = par_fast_window(g);
         if (pwin > 0) {
             int tiles_p = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
-            size_t pshm = par_fast_smem(pwin);
-            auto kf = dd2d_bp_par_fast_kernel<Tin, Tout>;
-            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
-            kf<<<dim3((unsigned)tiles_p, (unsigned)(g.nbatch * g.nz)), 256, pshm, s>>>(
-                mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin);
+            // two slices per CTA for stacks (shared per-view work), one otherwise
+            const int nslices = (int)(g.nbatch * g.nz);
+            const int S = nslices >= 2 ? 2 : 1;
+            size_t pshm = par_fast_smem(pwin, S);
+            dim3 pg((unsigned)tiles_p, (unsigned)((nslices + S - 1) / S));
+            if (S == 2) {
+                auto kf = dd2d_bp_par_fast_kernel<Tin, Tout, 2>;
+                cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
+                kf<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin,
+                                         nslices);
+            } else {
+                auto kf = dd2d_bp_par_fast_kernel<Tin, Tout, 1>;
+                cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
+                kf<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin,
+                                         nslices);
+            }
             return check_launch("dd2d_bp_par_fast_kernel");
         }
         auto k = dd2d_bp_parity_kernel<false, Tin, Tout>;

@@ -1,5 +1,6 @@
 # Builds the reference projector library (wudufan/CTProjector, kernel/projector/cuda)
-# from its own sources, for sm_100a, into oracle/_ref/libprojector.so.
+# from its own sources, for sm_100a, into oracle/_ref/libprojector.so, and its
+# TV prior (kernel/prior/cuda/TotalVariation.cu) into oracle/_ref/libprior.so.
 #
 # This is test infrastructure: the library is the GPU oracle that produces the
 # golden fixtures under tests/golden/ and the timed reference arm of bench.py.
@@ -11,6 +12,7 @@
 
 REF     ?= /root/reference
 SRC_DIR := $(REF)/src/ct_projector/kernel/projector/cuda
+PRIOR   := $(REF)/src/ct_projector/kernel/prior/cuda/TotalVariation.cu
 OUT     := oracle/_ref
 OBJ_DIR := $(OUT)/obj
 NVCC    ?= nvcc
@@ -21,7 +23,7 @@ OBJECTS := $(patsubst $(SRC_DIR)/%.cu,$(OBJ_DIR)/%.o,$(SOURCES))
 
 .PHONY: all clean
 
-all: $(OUT)/libprojector.so
+all: $(OUT)/libprojector.so $(OUT)/libprior.so
 
 $(OUT)/libprojector.so: $(OBJECTS)
 	$(NVCC) --shared $(ARCH) $(OBJECTS) -lcufft -o $@
@@ -30,6 +32,10 @@ $(OUT)/libprojector.so: $(OBJECTS)
 # from another, so it needs relocatable device code (-dc) and a device link.
 $(OBJ_DIR)/%.o: $(SRC_DIR)/%.cu | $(OBJ_DIR)
 	$(NVCC) -O3 $(ARCH) -I$(SRC_DIR)/.. -dc --compiler-options '-fPIC' -w $< -o $@
+
+# one self-contained translation unit
+$(OUT)/libprior.so: $(PRIOR) | $(OBJ_DIR)
+	$(NVCC) -O3 $(ARCH) --shared --compiler-options '-fPIC' -w $< -o $@
 
 $(OBJ_DIR):
 	mkdir -p $(OBJ_DIR)

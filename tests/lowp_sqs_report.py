@@ -9,9 +9,16 @@ the iterate itself are accumulated and kept in FP32.  Every iterate is
 compared with the same iterate of the FP64 oracle reconstruction of the
 float32 sinogram (so the storage rounding of the input counts as error).
 
-    python tests/lowp_sqs_report.py [--slices 1] [--iters 50] [--json out.json]
+The views start half a view step past 0, so none lies exactly on a 45 degree
+diagonal (there the reference's axis switch, which the GPU kernels replay with
+the same fast intrinsics, and the oracle's exact trigonometry may pick
+different axes; that case is tested separately).
 
-Test infrastructure (it runs the oracle); needs a CUDA device.
+    python tests/lowp_sqs_report.py [--slices 1] [--iters 50] [--json out.json]
+    python tests/lowp_sqs_report.py --oracle-out ref.npz    # CPU only: data + FP64 iterates
+    python tests/lowp_sqs_report.py --oracle-in ref.npz     # GPU part against saved iterates
+
+Test infrastructure (it runs the oracle); the GPU part needs a CUDA device.
 """
 from __future__ import annotations
 
@@ -60,48 +67,74 @@ def gpu_iterates(scan, ang, y32, storage, iters):
     return out
 
 
+def angles(nview):
+    import numpy as np
+
+    from ctprojector_b200 import synthetic as S
+
+    return (S.angles(nview, 2 * np.pi) + np.float32(np.pi / nview)).astype(np.float32)
+
+
+def oracle_part(slices, iters):
+    """Seeded phantom, FP64 projection with Poisson noise, and every iterate of
+    the FP64 oracle reconstruction (float32 copies)."""
+    from ctprojector_b200 import synthetic as S
+    from oracle import oracle as O
+    from oracle import recon as R
+
+    O.build()
+    scan, _, _ = S.config4()
+    ang = angles(scan.nview)
+    rng = np.random.default_rng(S.seed_for(4, 0))
+    img = np.stack([S.ellipse_phantom(rng, scan.nx, scan.ny, scan.dx, scan.dy)[None] for _ in range(slices)])
+    p = O.dd_fp(R._proj2d(scan), img.astype(np.float64), ang, "fan")
+    y32 = S.poisson_log(p, PHOTONS, rng)
+    its = []
+    t0 = time.perf_counter()
+    R.sqs_tv(scan, "fan", y32.astype(np.float64), ang, iters, BETA, WEIGHTS, EPS,
+             callback=lambda k, x: its.append(x.astype(np.float32)))
+    return y32, np.stack(its), ang, time.perf_counter() - t0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--slices", type=int, default=1)
     ap.add_argument("--iters", type=int, default=50)
     ap.add_argument("--json", default=None)
+    ap.add_argument("--oracle-out", default=None, help="compute the oracle part only and save it here")
+    ap.add_argument("--oracle-in", default=None, help="read the oracle part saved by --oracle-out")
     args = ap.parse_args(argv)
 
-    import torch
-
     from ctprojector_b200 import synthetic as S
-    from ctprojector_b200.projector import _device as D
-    from oracle import oracle as O
-    from oracle import recon as R
 
-    O.build()
-    scan, ang, _ = S.config4()
-    rng = np.random.default_rng(S.seed_for(4, 0))
-    img = np.stack([S.ellipse_phantom(rng, scan.nx, scan.ny, scan.dx, scan.dy)[None] for _ in range(args.slices)])
-    p = D.dd_fp(scan, torch.tensor(img, device="cuda"), torch.tensor(ang, device="cuda"), 0).cpu().numpy()
-    y32 = S.poisson_log(p, PHOTONS, rng)
-
-    t0 = time.perf_counter()
-    ref = {}
-    R.sqs_tv(scan, "fan", y32.astype(np.float64), ang, args.iters, BETA, WEIGHTS, EPS,
-             callback=lambda k, x: ref.__setitem__(k, x.copy()))
-    t_oracle = time.perf_counter() - t0
+    if args.oracle_in:
+        z = np.load(args.oracle_in)
+        y32, ref_its, ang, t_oracle = z["y32"], z["iterates"], z["angles"], float(z["seconds"])
+    else:
+        y32, ref_its, ang, t_oracle = oracle_part(args.slices, args.iters)
+        if args.oracle_out:
+            np.savez(args.oracle_out, y32=y32, iterates=ref_its, angles=ang, seconds=t_oracle)
+            print(f"saved {args.oracle_out}: {ref_its.shape[0]} iterates, oracle {t_oracle:.0f} s")
+            return 0
+    iters, slices = ref_its.shape[0], y32.shape[0]
+    scan, _, _ = S.config4()
+    ref = {k + 1: ref_its[k].astype(np.float64) for k in range(iters)}
     rows = {}
     for storage in STORAGES:
-        its = gpu_iterates(scan, ang, y32, storage, args.iters)
+        its = gpu_iterates(scan, ang, y32, storage, iters)
         rows[storage] = [(float(np.linalg.norm(x - ref[k + 1]) / np.linalg.norm(ref[k + 1])),
                           float(np.abs(x - ref[k + 1]).max())) for k, x in enumerate(its)]
-    peak = float(max(np.abs(ref[args.iters]).max(), 1e-30))
-    print(f"# reduced-precision SQS-TV, fan 512^2, 984 views, 888 cells, {args.slices} slice(s), "
-          f"{args.iters} iterations; FP64 oracle {t_oracle:.0f} s; max |x| of the last oracle iterate {peak:.4g}")
+    peak = float(max(np.abs(ref[iters]).max(), 1e-30))
+    print(f"# reduced-precision SQS-TV, fan 512^2, 984 views (half-step offset), 888 cells, {slices} slice(s), "
+          f"{iters} iterations; FP64 oracle {t_oracle:.0f} s; max |x| of the last oracle iterate {peak:.4g}")
     print("| iterate | fp32 rel L2 | fp32 max abs | bf16 rel L2 | bf16 max abs | fp16 rel L2 | fp16 max abs |")
     print("|---|---|---|---|---|---|---|")
-    for k in range(args.iters):
+    for k in range(iters):
         cells = " | ".join(f"{rows[s][k][0]:.3e} | {rows[s][k][1]:.3e}" for s in STORAGES)
         print(f"| {k + 1} | {cells} |")
     if args.json:
         with open(args.json, "w") as f:
-            json.dump({"iters": args.iters, "slices": args.slices, "peak": peak, "rows": rows}, f)
+            json.dump({"iters": iters, "slices": slices, "peak": peak, "rows": rows}, f)
     return 0
 
 

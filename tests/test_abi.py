@@ -89,3 +89,23 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(L, "LIB_PATH", str(tmp_path / "libctp.so"))
     with pytest.raises(CTProjectorError):
         L.lib()
+
+
+def test_workspace_queries_return_on_degenerate_geometry():
+    """The workspace queries run before any geometry validation, so zero
+    extents must not send their shape search into an endless loop (checked
+    in a child process with a time limit)."""
+    import subprocess
+    import sys
+
+    code = (
+        "from ctypes import byref\n"
+        "from ctprojector_b200._lib import Geometry, lib\n"
+        "for nu, nview, n in ((0, 90, 64), (96, 0, 64), (96, 90, 0), (0, 0, 0)):\n"
+        "    g = Geometry(1, n, n, 1, 1.0, 1.0, 1.0, 0, 0, 0, nu, 1, nview, 1.0, 1.0, 0, 0, 1000.0, 500.0)\n"
+        "    for geom in (0, 1):\n"
+        "        lib().ctp_dd2d_fp_workspace(byref(g), geom, 0, 0)\n"
+        "        lib().ctp_dd2d_bp_workspace(byref(g), geom, 0, 0)\n"
+        "print('ok')\n")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120, cwd=ROOT)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stderr
