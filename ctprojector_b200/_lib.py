@@ -106,12 +106,16 @@ _SIGNATURES = {
     "cTVSQS3D": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F],
     "ctp_tv_sqs": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F, _P],
     "ctp_wait_timeouts": [_P],
+    "cupyFbpTomoFilter": [_P, _P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, c_int, _F, _F],
+    "ctp_tomo_filter": [_P, _P, _P, _P, _GP, c_int, _F, _F, _P, _S, _P],
+    "ctp_tomo_filter_workspace": [_GP],
     "ctp_sqs_tv_update": [_P, _P, _P, _P, _P, _S, _P, _F, _F, _F, _F, _F, _S, _S, _S, c_uint, _P],
 }
 _RESTYPE = {
     "ctpGetLastErrorString": c_char_p,
     "ctpVersion": c_char_p,
     "ctp_dd2d_fp_workspace": c_size_t,
+    "ctp_tomo_filter_workspace": c_size_t,
     "ctp_dd2d_bp_workspace": c_size_t,
     "ctp_dd2d_fp_noalloc_capacity": c_size_t,
     "ctp_ramp_filter_workspace": c_size_t,

@@ -33,6 +33,9 @@ int tomo_bp(float*, const float*, const float*, const float*, const ctp_geometry
             cudaStream_t);
 size_t tomo_bp_workspace(const ctp_geometry&);
 int wait_timeouts(unsigned*);
+size_t tomo_filter_workspace(const ctp_geometry&);
+int tomo_filter(float*, const float*, const float*, const float*, const ctp_geometry&, int, float, float, void*, size_t,
+                cudaStream_t);
 int sqs_tv_update(float*, void*, const float*, const float*, const float*, size_t, const unsigned char*, float, float,
                   float, float, float, size_t, size_t, size_t, unsigned, cudaStream_t);
 int tv_sqs(float*, float*, float*, const float*, float, float, float, size_t, size_t, size_t, size_t, float,
@@ -637,5 +640,23 @@ int ctp_sqs_tv_update(float* x_out, void* x_lp, const float* x, const float* bp,
 }
 
 int ctp_wait_timeouts(unsigned int* count) { return wait_timeouts(count); }
+
+int cupyFbpTomoFilter(float* fprj, const float* prj, const float* detCenter, const float* src, int nBatches,
+                      size_t nu, size_t nv, size_t nview, float du, float dx, float dz, int typeFilter,
+                      float cutoffX, float cutoffZ) {
+    if (nBatches < 0) return set_error(CTP_ERR_INVALID_ARGUMENT, "negative batch count");
+    ctp_geometry g = make_geom((size_t)nBatches, 1, 1, 1, dx, 1.f, dz, 0.f, 0.f, 0.f, nu, nv, nview, du, 1.f, 0.f, 0.f,
+                               0.f, 0.f);
+    return finish_sync(tomo_filter(fprj, prj, detCenter, src, g, typeFilter, cutoffX, cutoffZ, nullptr, 0, 0), 0);
+}
+
+int ctp_tomo_filter(float* fprj, const float* prj, const float* detCenter, const float* src, const ctp_geometry* g,
+                    int filter, float cutoff_x, float cutoff_z, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!g) return set_error(CTP_ERR_INVALID_ARGUMENT, "geometry pointer is null");
+    return tomo_filter(fprj, prj, detCenter, src, *g, filter, cutoff_x, cutoff_z, workspace, workspace_bytes,
+                       as_stream(stream));
+}
+
+size_t ctp_tomo_filter_workspace(const ctp_geometry* g) { return g ? tomo_filter_workspace(*g) : 0; }
 
 }  // extern "C"

@@ -20,6 +20,7 @@
 //     multiply kernel scales the spectrum, and a crop kernel writes the first
 //     nu samples of each row.
 #include <cufft.h>
+#include <cmath>
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -518,6 +519,206 @@ int ramp_filter(float* fprj, const float* prj, const ctp_geometry& g, int geom, 
     if (flags & CTP_FLAG_FILTER_EXACT)
         return ramp_filter_exact(fprj, prj, g, geom, filter, workspace, workspace_bytes, s);
     return ramp_filter_reference(fprj, prj, g, geom, filter, workspace, workspace_bytes, s);
+}
+
+// ------------------------------------------------------------------ tomosynthesis FBP filter
+// fbpTomo::Filter and GetRampTomo (fbpTomo.cu:50-384): every view has its own
+// kernel.  The view's tilt (from the source-to-detector-centre direction in
+// the x-z plane) gives a virtual detector pitch vdu = du cos(tilt); the ramp
+// at that pitch is transformed, windowed by the product of an x window and a z
+// window whose frequencies scale with cos and sin of the tilt (both clamped
+// above at their cut-offs), transformed back, divided by L and transformed to
+// the R2C spectrum.  The rows of each view are zero padded to L = 2nu-1,
+// multiplied by the view's spectrum, transformed back, scaled by
+// pi / nview * vdu / L and cropped at nu-1.  The construction and the row
+// transforms replay the reference's FP32 steps and cuFFT plan shapes (one
+// length-L transform per view for the kernel, nv rows per transform for the
+// data), so the output stays within FP32 rounding of the reference.
+namespace {
+
+float tomo_frequency(int i, int L, float du, float dx, float angle_weight, float cutoff) {  // :50-68
+    float fu;
+    if (i > (L + 1) / 2)
+        fu = (i - L) / float(L) / du;
+    else
+        fu = i / float(L) / du;
+    float wx = fu * angle_weight * dx * 2;
+    if (wx > cutoff) wx = cutoff;
+    return wx;
+}
+
+struct TomoView {
+    float vdu, sin_t, cos_t;
+};
+
+TomoView tomo_view(float3 src, float3 det, float du) {  // :127-135
+    float r = sqrtf((det.x - src.x) * (det.x - src.x) + (det.z - src.z) * (det.z - src.z));
+    TomoView v;
+    v.sin_t = (det.x - src.x) / r;
+    v.cos_t = (src.z - det.z) / r;
+    v.vdu = du * v.cos_t;
+    return v;
+}
+
+// Spectra [nview][nu] of the per-view kernels, built on the device.
+int build_tomo_spectra(cufftComplex* spec, const std::vector<TomoView>& views, int nu, float dx, float dz,
+                       float cutoff_x, float cutoff_z, int filter) {
+    const int L = 2 * nu - 1;
+    const float PIf = 3.141592657f;  // projector.h:5
+    cufftHandle c2c = 0, r2c = 0;
+    cufftComplex* d = nullptr;
+    float* dk = nullptr;
+    int rc = CTP_OK;
+    if (cudaMalloc(&d, sizeof(cufftComplex) * L) != cudaSuccess || cudaMalloc(&dk, sizeof(float) * L) != cudaSuccess)
+        rc = set_error(cudaErrorMemoryAllocation, "tomo ramp allocation failed");
+    if (!rc && (cufftPlan1d(&c2c, L, CUFFT_C2C, 1) != CUFFT_SUCCESS || cufftPlan1d(&r2c, L, CUFFT_R2C, 1) != CUFFT_SUCCESS))
+        rc = set_error(CTP_ERR_CUFFT, "tomo ramp plan failed");
+    std::vector<cufftComplex> ramp(L), win(L);
+    std::vector<float> k(L);
+    for (size_t iv = 0; iv < views.size() && !rc; ++iv) {
+        const float vdu = views[iv].vdu;
+        for (int i = 0; i < L; i++) {
+            int kk = i - (nu - 1);
+            if (kk == 0)
+                ramp[i].x = 1 / (4 * vdu * vdu);
+            else if (kk % 2 != 0)
+                ramp[i].x = -1 / (PIf * PIf * kk * kk * vdu * vdu);
+            else
+                ramp[i].x = 0;
+            ramp[i].y = 0;
+        }
+        cudaMemcpy(d, ramp.data(), sizeof(cufftComplex) * L, cudaMemcpyHostToDevice);
+        cufftExecC2C(c2c, d, d, CUFFT_FORWARD);
+        cudaMemcpy(ramp.data(), d, sizeof(cufftComplex) * L, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < L; i++) {
+            if (filter == 1 || filter == 2) {
+                float wx = tomo_frequency(i, L, vdu, dx, views[iv].cos_t, cutoff_x);
+                float wz = tomo_frequency(i, L, vdu, dz, views[iv].sin_t, cutoff_z);
+                win[i].x = filter == 1
+                               ? (0.54f + 0.46f * cosf(PIf * wx / cutoff_x)) * (0.54f + 0.46f * cosf(PIf * wz / cutoff_z))
+                               : (0.5f + 0.5f * cosf(PIf * wx / cutoff_x)) * (0.5f + 0.5f * cosf(PIf * wz / cutoff_z));
+            } else {
+                win[i].x = 1;
+            }
+            win[i].y = 0;
+            float re = ramp[i].x * win[i].x - ramp[i].y * win[i].y;
+            float im = ramp[i].x * win[i].y + ramp[i].y * win[i].x;
+            ramp[i].x = re;
+            ramp[i].y = im;
+        }
+        cudaMemcpy(d, ramp.data(), sizeof(cufftComplex) * L, cudaMemcpyHostToDevice);
+        cufftExecC2C(c2c, d, d, CUFFT_INVERSE);
+        cudaMemcpy(ramp.data(), d, sizeof(cufftComplex) * L, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < L; i++) k[i] = ramp[i].x / L;
+        cudaMemcpy(dk, k.data(), sizeof(float) * L, cudaMemcpyHostToDevice);
+        if (cufftExecR2C(r2c, dk, spec + iv * nu) != CUFFT_SUCCESS) rc = set_error(CTP_ERR_CUFFT, "tomo ramp R2C failed");
+        cudaError_t e = cudaDeviceSynchronize();
+        if (!rc && e != cudaSuccess) rc = set_error((int)e, "tomo ramp: %s", cudaGetErrorString(e));
+    }
+    if (c2c) cufftDestroy(c2c);
+    if (r2c) cufftDestroy(r2c);
+    if (d) cudaFree(d);
+    if (dk) cudaFree(dk);
+    return rc;
+}
+
+// FilterByFreqMultiply1D against the kernel of each row's view.
+__global__ void tomo_cmul_kernel(cufftComplex* __restrict__ f, const cufftComplex* __restrict__ spec, int nu, int nv,
+                                 int nview, size_t rows) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= rows * nu) return;
+    size_t r = i / nu;
+    int n = (int)(i - r * nu);
+    int view = (int)((r / nv) % nview);
+    cufftComplex a = f[i], b = spec[(size_t)view * nu + n], v;
+    v.x = a.x * b.x - a.y * b.y;
+    v.y = a.x * b.y + a.y * b.x;
+    f[i] = v;
+}
+
+__global__ void tomo_crop_kernel(float* __restrict__ out, const float* __restrict__ pad, const float* __restrict__ scale,
+                                 int nu, int L, int nv, int nview, size_t rows) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= rows * nu) return;
+    size_t r = i / nu;
+    int n = (int)(i - r * nu);
+    out[i] = pad[r * L + nu - 1 + n] * scale[(r / nv) % nview];
+}
+
+}  // namespace
+
+size_t tomo_filter_workspace(const ctp_geometry& g) {
+    size_t nu = g.nu, L = 2 * nu - 1, rows = g.nbatch * g.nview * g.nv;
+    RefPlan* p = nullptr;
+    if (nu == 0 || g.nv == 0 || get_ref_plan((int)L, (int)nu, (int)g.nv, &p)) return 0;
+    return align_up(rows * L * sizeof(float)) + align_up(rows * nu * sizeof(cufftComplex)) + align_up(p->work) +
+           align_up(g.nview * nu * sizeof(cufftComplex)) + align_up(g.nview * sizeof(float));
+}
+
+int tomo_filter(float* fprj, const float* prj, const float* det_center, const float* src, const ctp_geometry& g,
+                int filter, float cutoff_x, float cutoff_z, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    if (g.nbatch == 0) return CTP_OK;
+    if (!fprj || !prj || !det_center || !src) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    if (g.nu == 0 || g.nv == 0 || g.nview == 0) return set_error(CTP_ERR_INVALID_ARGUMENT, "zero detector extent");
+    if (!(cutoff_x > 0) || !(cutoff_z > 0)) return set_error(CTP_ERR_INVALID_ARGUMENT, "cut-offs must be positive");
+    const int nu = (int)g.nu, L = 2 * nu - 1, nv = (int)g.nv, nview = (int)g.nview;
+    const size_t rows = g.nbatch * g.nview * g.nv;
+    // view geometry on the host (fbpTomo.cu:285-290 copies it back too)
+    std::vector<float3> hd(nview), hs(nview);
+    cudaError_t e = cudaMemcpyAsync(hd.data(), det_center, sizeof(float3) * nview, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), src, sizeof(float3) * nview, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_error((int)e, "tomo filter geometry: %s", cudaGetErrorString(e));
+    std::vector<TomoView> views(nview);
+    std::vector<float> scale(nview);
+    const float PIf = 3.141592657f;
+    for (int v = 0; v < nview; ++v) {
+        views[v] = tomo_view(hs[v], hd[v], g.du);
+        if (!(views[v].vdu != 0.f) || !std::isfinite(views[v].vdu))
+            return set_error(CTP_ERR_INVALID_ARGUMENT, "view %d: source and detector centre give no tilt", v);
+        scale[v] = PIf / g.nview * views[v].vdu / L;  // fbpTomo.cu:311
+    }
+    RefPlan* plan = nullptr;
+    int rc = get_ref_plan(L, nu, nv, &plan);
+    if (rc) return rc;
+    Scratch scr;
+    size_t pad_b = align_up(rows * L * sizeof(float)), frq_b = align_up(rows * nu * sizeof(cufftComplex));
+    size_t work_b = align_up(plan->work), spec_b = align_up(g.nview * nu * sizeof(cufftComplex));
+    if ((rc = scr.acquire(workspace, workspace_bytes, pad_b + frq_b + work_b + spec_b + align_up(g.nview * sizeof(float)),
+                          s)))
+        return rc;
+    float* pad = reinterpret_cast<float*>(scr.base());
+    cufftComplex* frq = reinterpret_cast<cufftComplex*>(scr.base() + pad_b);
+    void* work = scr.base() + pad_b + frq_b;
+    cufftComplex* spec = reinterpret_cast<cufftComplex*>(scr.base() + pad_b + frq_b + work_b);
+    float* dscale = reinterpret_cast<float*>(scr.base() + pad_b + frq_b + work_b + spec_b);
+    // the view kernels are built with synchronous copies and transforms (as in
+    // the reference; the filter is not on a hot path): the scratch must exist first
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_error((int)e, "tomo filter: %s", cudaGetErrorString(e));
+    if ((rc = build_tomo_spectra(spec, views, nu, g.dx, g.dz, cutoff_x, cutoff_z, filter))) return rc;
+    e = cudaMemcpyAsync(dscale, scale.data(), sizeof(float) * nview, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_error((int)e, "tomo filter scales: %s", cudaGetErrorString(e));
+    ref_pad_kernel<<<(unsigned)((rows * L + 255) / 256), 256, 0, s>>>(pad, prj, nullptr, nu, L, rows);
+    if ((rc = check_launch("ref_pad_kernel"))) return rc;
+    {
+        std::lock_guard<std::mutex> lk(plan->mu);
+        cufftSetStream(plan->fwd, s);
+        cufftSetStream(plan->inv, s);
+        cufftSetWorkArea(plan->fwd, work);
+        cufftSetWorkArea(plan->inv, work);
+        for (size_t r0 = 0; r0 < rows; r0 += nv)
+            if (cufftExecR2C(plan->fwd, pad + r0 * L, frq + r0 * nu) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecR2C failed");
+        tomo_cmul_kernel<<<(unsigned)((rows * nu + 255) / 256), 256, 0, s>>>(frq, spec, nu, nv, nview, rows);
+        if ((rc = check_launch("tomo_cmul_kernel"))) return rc;
+        for (size_t r0 = 0; r0 < rows; r0 += nv)
+            if (cufftExecC2R(plan->inv, frq + r0 * nu, pad + r0 * L) != CUFFT_SUCCESS)
+                return set_error(CTP_ERR_CUFFT, "cufftExecC2R failed");
+    }
+    tomo_crop_kernel<<<(unsigned)((rows * nu + 255) / 256), 256, 0, s>>>(fprj, pad, dscale, nu, L, nv, nview, rows);
+    return check_launch("tomo_crop_kernel");
 }
 
 // ------------------------------------------------------------------ fbp_bp

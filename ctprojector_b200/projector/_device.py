@@ -7,7 +7,7 @@ the allocator is warm.
 """
 from __future__ import annotations
 
-from ctypes import byref, c_ulonglong, c_void_p
+from ctypes import byref, c_float, c_ulonglong, c_void_p
 
 import numpy as np
 import torch
@@ -243,3 +243,20 @@ def tomo_bp(p, prj, det_center, src, out=None, stream=None):
     check(lib().ctp_tomo_bp(ptr(img), ptr(t), ptr(dc), ptr(sr), byref(g), 0, wp, wn,
                             stream_handle(stream, t.device)), "tomo distance_driven_bp")
     return img
+
+
+def tomo_filter(p, prj, det_center, src, filter_type: str = "hann", cutoff_x: float = 1.0, cutoff_z: float = 1.0,
+                out=None, stream=None):
+    """Tomosynthesis FBP filter; 'hamming' 1, 'hann' 2, anything else none
+    (tomo.py:188-193 of the reference cupy wrapper)."""
+    t = as_tensor(prj, lowp_ok=False)
+    dc, sr = _geom3(det_center), _geom3(src)
+    nb, nview, nv, nu = t.shape
+    g = make_geometry(p, nb, (1, 1, 1), nu, nv, nview, float(p.du))
+    fprj = _out(list(t.shape), torch.float32, t.device, out)
+    ft = filter_type.lower()
+    ifilter = 1 if ft == "hamming" else 2 if ft == "hann" else 0
+    ws, wp, wn = workspace(lib().ctp_tomo_filter_workspace(byref(g)), t.device)
+    check(lib().ctp_tomo_filter(ptr(fprj), ptr(t), ptr(dc), ptr(sr), byref(g), ifilter, c_float(cutoff_x),
+                                c_float(cutoff_z), wp, wn, stream_handle(stream, t.device)), "tomo filter_fbp")
+    return fprj

@@ -1,13 +1,11 @@
 """Tomosynthesis geometry (detector u = (1,0,0), v = (0,1,0)), device arrays.
 
 Same calls as ct_projector/projector/cupy/tomo.py of the reference:
-distance_driven_fp (:15), distance_driven_bp (:85).  ``branchless`` selects
+distance_driven_fp (:15), distance_driven_bp (:85), filter_fbp (:157).  ``branchless`` selects
 the same operator (both are the exact box integral).
 """
 from __future__ import annotations
 
-from ... import _lib
-from ...errors import CTProjectorError
 from .. import _device as D
 from .ct_projector import ct_projector
 
@@ -23,6 +21,11 @@ def distance_driven_bp(projector: ct_projector, prj, det_center, src, branchless
 
 
 def filter_fbp(projector: ct_projector, prj, det_center, src, filter_type: str = "hann", cutoff_x: float = 1,
-               cutoff_y: float = 1):
-    """The tomosynthesis FBP filter (reference tomo.py:157) is not part of this build."""
-    raise CTProjectorError(_lib.CTP_ERR_UNSUPPORTED, "tomo.filter_fbp is not implemented in ctprojector_b200")
+               cutoff_y: float = 1, *, out=None, stream=None):
+    """Tomosynthesis FBP filter (reference tomo.py:157, fbpTomo.cu:50-384):
+    each view's rows are filtered with a ramp at the view's virtual pitch
+    du * cos(tilt), windowed ('hamming', 'hann', else none) with cut-offs
+    ``cutoff_x`` along u and ``cutoff_y`` along the tilt direction (0, 1].
+    Returns [batch, nview, nv, nu]."""
+    return D.like_input(D.tomo_filter(projector, prj, det_center, src, filter_type, cutoff_x, cutoff_y, out=out,
+                                      stream=stream), prj)

@@ -289,6 +289,19 @@ size_t ctp_tomo_bp_workspace(const ctp_geometry* g);
 int ctp_tv_sqs(float* s1, float* s2, float* var, const float* img, float wx, float wy, float wz, size_t nbatch,
                size_t nx, size_t ny, size_t nz, float eps, void* stream);
 
+/* Tomosynthesis FBP filter, fbpTomo.cu:386 (cupyFbpTomoFilter, device
+   pointers; nBatches is an int in the reference's C signature).  Per view the
+   ramp at the virtual pitch du*cos(tilt), windowed (typeFilter 1 Hamming,
+   2 Hann, else none) with x/z cut-offs; fprj is overwritten. */
+int cupyFbpTomoFilter(float* fprj, const float* prj, const float* detCenter, const float* src, int nBatches,
+                      size_t nu, size_t nv, size_t nview, float du, float dx, float dz, int typeFilter,
+                      float cutoffX, float cutoffZ);
+/* The same with a ctp_geometry (nbatch, nu, nv, nview, du, dx, dz), a caller
+   workspace (size from ctp_tomo_filter_workspace) and a stream. */
+int ctp_tomo_filter(float* fprj, const float* prj, const float* detCenter, const float* src, const ctp_geometry* g,
+                    int filter, float cutoff_x, float cutoff_z, void* workspace, size_t workspace_bytes, void* stream);
+size_t ctp_tomo_filter_workspace(const ctp_geometry* g);
+
 /* Bounded device-side waits that gave up on the current device since the
    library was loaded (the streamed forward projector polls an mbarrier for
    each chunk of line tables with an iteration limit, and counts a limit that

@@ -342,3 +342,51 @@ def sqs_tv_update(x, bp, norm, zlink, weights, beta, eps=1e-8):
         s1[a:b], s2[a:b] = t1[0], t2[0]
     beta = float(np.float32(beta))
     return x - (_d(bp) + beta * s1) / (norm[idx] + beta * s2)
+
+
+def tomo_filter(p, prj, det_center, src, filter_type="hann", cutoff_x=1.0, cutoff_z=1.0):
+    """Tomosynthesis FBP filter in FP64 (fbpTomo::Filter and GetRampTomo,
+    kernel/projector/cuda/fbpTomo.cu:50-384 of the reference).  Per view: the
+    tilt from the source-to-detector-centre direction in the x-z plane
+    (:127-135), the ramp at the virtual pitch vdu = du cos(tilt), windowed in
+    frequency by (x window) * (z window) whose frequencies are
+    fu * cos * dx * 2 and fu * sin * dz * 2, each clamped above at its cut-off
+    (GetFrequency :50-68); every row of the view is convolved with it and
+    scaled by pi / nview * vdu (:311, with the transforms' 1/L)."""
+    prj = _d(prj)
+    dc, sr = _d(det_center), _d(src)
+    nb, nview, nv, nu = prj.shape
+    L = 2 * nu - 1
+    du, dx, dz = (float(np.float32(v)) for v in (p.du, p.dx, p.dz))
+    cx, cz = float(np.float32(cutoff_x)), float(np.float32(cutoff_z))
+    ft = filter_type.lower()
+    ifilter = 1 if ft == "hamming" else 2 if ft == "hann" else 0
+    k = np.arange(L) - (nu - 1)
+    i = np.arange(L)
+    n = 1
+    while n < 3 * nu - 2:
+        n *= 2
+    out = np.zeros_like(prj)
+    for v in range(nview):
+        ddx, ddz = dc[v, 0] - sr[v, 0], dc[v, 2] - sr[v, 2]
+        r = np.sqrt(ddx * ddx + ddz * ddz)
+        sin_t, cos_t = ddx / r, -ddz / r
+        vdu = du * cos_t
+        h = np.zeros(L)
+        h[k == 0] = 1.0 / (4 * vdu * vdu)
+        odd = (k % 2) != 0
+        h[odd] = -1.0 / (np.pi ** 2 * k[odd].astype(np.float64) ** 2 * vdu * vdu)
+        fu = np.where(i > (L + 1) // 2, (i - L) / L / vdu, i / L / vdu)
+        wx = np.minimum(fu * cos_t * dx * 2, cx)
+        wz = np.minimum(fu * sin_t * dz * 2, cz)
+        if ifilter == 1:
+            w = (0.54 + 0.46 * np.cos(np.pi * wx / cx)) * (0.54 + 0.46 * np.cos(np.pi * wz / cz))
+        elif ifilter == 2:
+            w = (0.5 + 0.5 * np.cos(np.pi * wx / cx)) * (0.5 + 0.5 * np.cos(np.pi * wz / cz))
+        else:
+            w = np.ones(L)
+        g = np.real(np.fft.ifft(np.fft.fft(h) * w))
+        X = np.fft.rfft(prj[:, v], n=n, axis=-1)
+        full = np.fft.irfft(X * np.fft.rfft(g, n=n), n=n, axis=-1)
+        out[:, v] = full[..., nu - 1: 2 * nu - 1] * (np.pi / nview * vdu)
+    return out

@@ -130,6 +130,24 @@ class Ref:
         return img
 
 
+    # tomo.py:157-221: the reference has only the device entry, called with device buffers
+    def tomo_filter(self, p, prj, dc, src, ifilter, cutoff_x, cutoff_z):
+        import torch
+
+        t = lambda a: torch.tensor(np.ascontiguousarray(a), device="cuda")  # noqa: E731
+        dp, ddc, dsr = t(prj), t(dc), t(src)
+        out = torch.zeros_like(dp)
+        self.call("cupyFbpTomoFilter", c_void_p(out.data_ptr()), c_void_p(dp.data_ptr()), c_void_p(ddc.data_ptr()),
+                  c_void_p(dsr.data_ptr()), c_ulong(prj.shape[0]), c_ulong(prj.shape[3]), c_ulong(prj.shape[2]),
+                  c_ulong(prj.shape[1]), c_float(p.du), c_float(p.dx), c_float(p.dz), c_int(ifilter),
+                  c_float(cutoff_x), c_float(cutoff_z))
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+
+
+TOMO_FILTERS = (("hann", 2, 1.0, 1.0), ("hamming_cut", 1, 0.8, 0.6), ("ramlak", 0, 1.0, 1.0))
+
+
 def run_case(ref: Ref, fn):
     name, p, inp = fn()
     out = {}
@@ -156,6 +174,8 @@ def run_case(ref: Ref, fn):
         prj = ref.tomo_fp(p, inp["img"], inp["det_center"], inp["src"])
         out["fp"] = prj
         out["bp"] = ref.tomo_bp(p, prj, inp["det_center"], inp["src"])
+        for fname, code, cx, cz in TOMO_FILTERS:
+            out[f"filter_{fname}"] = ref.tomo_filter(p, prj, inp["det_center"], inp["src"], code, cx, cz)
     geom_attrs = {f"geom_{k}": np.asarray(v) for k, v in p.as_dict().items()}
     return name, {**{f"in_{k}": v for k, v in inp.items()}, **{f"ref_{k}": v for k, v in out.items()}, **geom_attrs}
 
