@@ -106,6 +106,13 @@ _SIGNATURES = {
     "cTVSQS3D": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F],
     "ctp_tv_sqs": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F, _P],
     "ctp_wait_timeouts": [_P],
+    "cSiddonFanProjection": [_P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, _F, _F, _F, _S, _S, _S, _F, _F, _F, _F, _F, _F],
+    "cSiddonFanBackprojection": [_P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, _F, _F, _F, _S, _S, _S, _F, _F, _F, _F, _F,
+                                 _F],
+    "cfbpParallelBackprojection": [_P, _P, _P] + _REF_GEOM + [_F, _F, _F, _F, c_int],
+    "ctp_siddon_fan_fp": [_P, _P, _P, _GP, c_uint, _P],
+    "ctp_siddon_fan_bp": [_P, _P, _P, _GP, c_uint, _P],
+    "ctp_pixel_bp_parallel": [_P, _P, _P, _GP, c_uint, _P],
     "cupyFbpTomoFilter": [_P, _P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, c_int, _F, _F],
     "ctp_tomo_filter": [_P, _P, _P, _P, _GP, c_int, _F, _F, _P, _S, _P],
     "ctp_tomo_filter_workspace": [_GP],

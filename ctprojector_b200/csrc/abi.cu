@@ -33,6 +33,9 @@ int tomo_bp(float*, const float*, const float*, const float*, const ctp_geometry
             cudaStream_t);
 size_t tomo_bp_workspace(const ctp_geometry&);
 int wait_timeouts(unsigned*);
+int siddon_fan_fp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
+int siddon_fan_bp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
+int pixel_bp_parallel(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 size_t tomo_filter_workspace(const ctp_geometry&);
 int tomo_filter(float*, const float*, const float*, const float*, const ctp_geometry&, int, float, float, void*, size_t,
                 cudaStream_t);
@@ -487,8 +490,93 @@ int cfbpFanBackprojection(float* pImg, const float* pPrj, const float* pDeg, CTP
     return hc.finish();
 }
 
+// Fan-beam Siddon pair, host pointers (siddonFan.cu:127-274; nBatches is an
+// int there).  The reference zeroes the device output before tracing.
+static int siddon_fan_host(bool fp, float* out, const float* in, const float* deg, int nBatches, size_t nx, size_t ny,
+                           size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu, size_t nv,
+                           size_t nview, float da, float dv, float off_a, float off_v, float dsd, float dso) {
+    if (nBatches < 0) return set_error(CTP_ERR_INVALID_ARGUMENT, "negative batch count");
+    ctp_geometry g = make_geom((size_t)nBatches, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, nv, nview, da, dv, off_a,
+                               off_v, dsd, dso);
+    int rc = check_geometry(&g, true, true);
+    if (rc) return rc;
+    if (!out || !in || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    if (g.nbatch == 0) return CTP_OK;
+    HostCall hc;
+    size_t ni = g.nbatch * g.nz * g.ny * g.nx, np = g.nbatch * g.nview * g.nv * g.nu;
+    float* din = hc.upload(in, fp ? ni : np);
+    float* ddeg = hc.upload(deg, g.nview);
+    float* dout = hc.dev<float>(fp ? np : ni);
+    if (!hc.rc)
+        hc.rc = fp ? siddon_fan_fp(dout, din, ddeg, g, CTP_FLAG_ZERO_OUT, hc.s)
+                   : siddon_fan_bp(dout, din, ddeg, g, CTP_FLAG_ZERO_OUT, hc.s);
+    hc.download(out, dout, fp ? np : ni);
+    return hc.finish();
+}
+
+int cSiddonFanProjection(float* prj, const float* img, const float* deg, int nBatches, size_t nx, size_t ny,
+                         size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu, size_t nv,
+                         size_t nview, float da, float dv, float off_a, float off_v, float dsd, float dso) {
+    return siddon_fan_host(true, prj, img, deg, nBatches, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, nv, nview, da, dv,
+                           off_a, off_v, dsd, dso);
+}
+
+int cSiddonFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, size_t nx, size_t ny,
+                             size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu,
+                             size_t nv, size_t nview, float da, float dv, float off_a, float off_v, float dsd,
+                             float dso) {
+    return siddon_fan_host(false, img, prj, deg, nBatches, nx, ny, nz, dx, dy, dz, cx, cy, cz, nu, nv, nview, da, dv,
+                           off_a, off_v, dsd, dso);
+}
+
+// Pixel-driven parallel back projection, host pointers (fbpParallel.cu:271-345).
+int cfbpParallelBackprojection(float* pImg, const float* pPrj, const float* pDeg, CTP_GEOM_ARGS, float du, float dv,
+                               float off_u, float off_v, int typeProjector) {
+    (void)typeProjector;  // the reference reads no bit of it here
+    ctp_geometry g = CTP_GEOM(du, dv, off_u, off_v, 1000.f, 500.f);
+    int rc = check_geometry(&g, true, true);
+    if (rc) return rc;
+    if (!pImg || !pPrj || !pDeg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    if (g.nbatch == 0) return CTP_OK;
+    HostCall hc;
+    size_t ni = g.nbatch * g.nz * g.ny * g.nx, np = g.nbatch * g.nview * g.nv * g.nu;
+    float* dprj = hc.upload(pPrj, np);
+    float* ddeg = hc.upload(pDeg, g.nview);
+    float* dimg = hc.dev<float>(ni);
+    if (!hc.rc) hc.rc = pixel_bp_parallel(dimg, dprj, ddeg, g, CTP_FLAG_ZERO_OUT, hc.s);
+    hc.download(pImg, dimg, ni);
+    return hc.finish();
+}
+
 // ============================================================ extended entries
 static cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int ctp_siddon_fan_fp(float* prj, const float* img, const float* deg, const ctp_geometry* g, unsigned flags,
+                      void* stream) {
+    int rc = check_geometry(g, true, true);
+    if (rc) return rc;
+    if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    return siddon_fan_fp(prj, img, deg, *g, flags, as_stream(stream));
+}
+
+int ctp_siddon_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,
+                      void* stream) {
+    int rc = check_geometry(g, true, true);
+    if (rc) return rc;
+    if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    return siddon_fan_bp(img, prj, deg, *g, flags, as_stream(stream));
+}
+
+int ctp_pixel_bp_parallel(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,
+                          void* stream) {
+    int rc = check_geometry(g, true, true);
+    if (rc) return rc;
+    if (g->nbatch == 0) return CTP_OK;
+    if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    return pixel_bp_parallel(img, prj, deg, *g, flags, as_stream(stream));
+}
 
 int ctp_dd2d_fp(void* prj, const void* img, const float* deg, const ctp_geometry* g, int geom, int typeProjector,
                 unsigned flags, void* workspace, size_t workspace_bytes, void* stream) {

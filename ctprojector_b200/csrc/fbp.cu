@@ -795,6 +795,69 @@ __global__ void fbp_fan_bp_kernel(float* __restrict__ img, const float* __restri
     }
 }
 
+// Pixel-driven parallel back projection without weights (the numpy
+// module's pixel_driven_bp; bpParallelKernel3D, fbpParallel.cu:200-250):
+// pu = -((x cos + y sin)/du + off_u) + (nu-1)/2 and the same truncating
+// bilinear interpolation as fbp_fan_bp_kernel.
+__global__ void pixel_bp_par_kernel(float* __restrict__ img, const float* __restrict__ prj,
+                                    const float* __restrict__ deg, int nview, Grid g, Det d, int accumulate) {
+    __shared__ float s_c[kFbpViews], s_s[kFbpViews];
+    int ix = blockIdx.x * 32 + (threadIdx.x & 31);
+    int iy = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int zb = blockIdx.z % ((g.nz + kFbpZ - 1) / kFbpZ);
+    int b = blockIdx.z / ((g.nz + kFbpZ - 1) / kFbpZ);
+    int iz0 = zb * kFbpZ;
+    float x = ((float)ix + 0.5f - g.nx / 2.f) * g.dx + g.cx;
+    float y = ((float)iy + 0.5f - g.ny / 2.f) * g.dy + g.cy;
+    float z0 = ((float)iz0 + 0.5f - g.nz / 2.f) * g.dz + g.cz;
+    float acc[kFbpZ];
+#pragma unroll
+    for (int q = 0; q < kFbpZ; ++q) acc[q] = 0.f;
+    const float* pb = prj + (size_t)b * nview * d.nv * d.nu;
+    for (int v0 = 0; v0 < nview; v0 += kFbpViews) {
+        int nvc = min(kFbpViews, nview - v0);
+        if (threadIdx.x < nvc) {
+            double s, c;
+            sincos((double)deg[v0 + threadIdx.x], &s, &c);
+            s_c[threadIdx.x] = (float)c;
+            s_s[threadIdx.x] = (float)s;
+        }
+        __syncthreads();
+        if (ix < g.nx && iy < g.ny) {
+            for (int vi = 0; vi < nvc; ++vi) {
+                float pu = -((x * s_c[vi] + y * s_s[vi]) / d.du + d.off_u) + (d.nu - 1.0f) / 2.0f;
+                if (pu < 0 || pu >= d.nu) continue;
+                int i0 = (int)pu;
+                int i1 = min(i0 + 1, d.nu - 1);
+                float wu = pu - (float)i0;
+                const float* pv_base = pb + (size_t)(v0 + vi) * d.nv * d.nu;
+#pragma unroll
+                for (int q = 0; q < kFbpZ; ++q) {
+                    float pv = (z0 + q * g.dz) / d.dv + d.off_v + (d.nv - 1.0f) / 2.f;
+                    if (pv < 0 || pv >= d.nv) continue;
+                    int j0 = (int)pv;
+                    int j1 = min(j0 + 1, d.nv - 1);
+                    float wv = pv - (float)j0;
+                    const float* r0 = pv_base + (size_t)j0 * d.nu;
+                    const float* r1 = pv_base + (size_t)j1 * d.nu;
+                    acc[q] += __ldg(r0 + i0) * (1 - wu) * (1 - wv) + __ldg(r0 + i1) * wu * (1 - wv) +
+                              __ldg(r1 + i0) * (1 - wu) * wv + __ldg(r1 + i1) * wu * wv;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (ix < g.nx && iy < g.ny) {
+#pragma unroll
+        for (int q = 0; q < kFbpZ; ++q) {
+            int iz = iz0 + q;
+            if (iz >= g.nz) break;
+            float* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
+            *o = (accumulate ? *o : 0.f) + acc[q];
+        }
+    }
+}
+
 }  // namespace
 
 int fbp_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry& g, unsigned flags,
@@ -804,6 +867,15 @@ int fbp_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometr
     fbp_fan_bp_kernel<<<grid, 256, 0, s>>>(img, prj, deg, (int)g.nview, make_grid(g), make_det(g), g.dso,
                                            (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1);
     return check_launch("fbp_fan_bp_kernel");
+}
+
+int pixel_bp_parallel(float* img, const float* prj, const float* deg, const ctp_geometry& g, unsigned flags,
+                      cudaStream_t s) {
+    int zb = (int)((g.nz + kFbpZ - 1) / kFbpZ);
+    dim3 grid((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 7) / 8), (unsigned)(g.nbatch * zb));
+    pixel_bp_par_kernel<<<grid, 256, 0, s>>>(img, prj, deg, (int)g.nview, make_grid(g), make_det(g),
+                                             (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1);
+    return check_launch("pixel_bp_par_kernel");
 }
 
 }  // namespace ctp

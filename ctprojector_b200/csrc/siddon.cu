@@ -191,6 +191,63 @@ __global__ void __launch_bounds__(256) siddon_count_kernel(unsigned long long* _
     if (threadIdx.x == 0 && blk) atomicAdd(count, blk);
 }
 
+// Fan-beam rays (SiddonFanProjectionKernel, siddonFan.cu:12-44): source on
+// the circle of radius dso, detector cell on the arc of radius dsd at angle
+// a = (-(iu - (nu-1)/2) - off_u) da, both at height z = (iv - (nv-1)/2 + off_v)
+// dv, rotated by the view angle (trigonometry in FP64); the end points are not
+// moved towards the grid, as in the reference's fan kernels.
+__device__ void fan_ray_ends(double src[3], double dst[3], float deg, int iu, int iv, const Det& d, double dsd,
+                             double dso) {
+    double s, c, sa, ca;
+    sincos((double)deg, &s, &c);
+    const double a = (-((double)iu - (d.nu - 1) / 2.0) - d.off_u) * d.du;
+    sincos(a, &sa, &ca);
+    const double z = ((double)iv - (d.nv - 1) / 2.0 + d.off_v) * d.dv;
+    const double rx = dsd * sa, ry = -dso + dsd * ca;
+    src[0] = dso * s;
+    src[1] = -dso * c;
+    src[2] = z;
+    dst[0] = rx * c - ry * s;
+    dst[1] = rx * s + ry * c;
+    dst[2] = z;
+}
+
+__global__ void __launch_bounds__(256) siddon_fan_fp_kernel(float* __restrict__ prj, const float* __restrict__ img,
+                                                            const float* __restrict__ deg, int nview, Grid g, Det d,
+                                                            double dsd, double dso, int accumulate) {
+    int iu = blockIdx.x * 32 + (threadIdx.x & 31);
+    int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int view = blockIdx.z % nview, b = blockIdx.z / nview;
+    if (iu >= d.nu || iv >= d.nv) return;
+    double src[3], dst[3];
+    fan_ray_ends(src, dst, deg[view], iu, iv, d, dsd, dso);
+    Ray R = init_ray(src, dst, g);
+    float acc = 0.f;
+    if (R.hit) {
+        const float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
+        walk(R, g, [&](long long idx, float len) { acc += __ldg(vol + idx) * len; });
+    }
+    float* o = prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu;
+    *o = (accumulate ? *o : 0.f) + acc;
+}
+
+__global__ void __launch_bounds__(256) siddon_fan_bp_kernel(float* __restrict__ img, const float* __restrict__ prj,
+                                                            const float* __restrict__ deg, int nview, Grid g, Det d,
+                                                            double dsd, double dso) {
+    int iu = blockIdx.x * 32 + (threadIdx.x & 31);
+    int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int view = blockIdx.z % nview, b = blockIdx.z / nview;
+    if (iu >= d.nu || iv >= d.nv) return;
+    float p = __ldg(prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu);
+    if (p == 0.f) return;
+    double src[3], dst[3];
+    fan_ray_ends(src, dst, deg[view], iu, iv, d, dsd, dso);
+    Ray R = init_ray(src, dst, g);
+    if (!R.hit) return;
+    float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
+    walk(R, g, [&](long long idx, float len) { atomicAdd(vol + idx, p * len); });
+}
+
 dim3 ray_grid(const ctp_geometry& g, size_t nz_mult) {
     return dim3((unsigned)((g.nu + 31) / 32), (unsigned)((g.nv + 7) / 8), (unsigned)(g.nview * nz_mult));
 }
@@ -263,6 +320,26 @@ int siddon_nnz(unsigned long long* nnz_host, const float* dc, const float* du_, 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return set_error((int)e, "siddon_nnz: %s", cudaGetErrorString(e));
     return CTP_OK;
+}
+
+// Fan-beam Siddon pair (siddonFan.cu:12-274); g.du is the angular cell size.
+int siddon_fan_fp(float* prj, const float* img, const float* deg, const ctp_geometry& g, unsigned flags,
+                  cudaStream_t s) {
+    siddon_fan_fp_kernel<<<ray_grid(g, g.nbatch), 256, 0, s>>>(prj, img, deg, (int)g.nview, make_grid(g), make_det(g),
+                                                                (double)g.dsd, (double)g.dso,
+                                                                (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1);
+    return check_launch("siddon_fan_fp_kernel");
+}
+
+int siddon_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry& g, unsigned flags,
+                  cudaStream_t s) {
+    if (flags & CTP_FLAG_ZERO_OUT) {
+        cudaError_t e = cudaMemsetAsync(img, 0, g.nbatch * g.nz * g.ny * g.nx * sizeof(float), s);
+        if (e != cudaSuccess) return set_error((int)e, "siddon_fan_bp memset: %s", cudaGetErrorString(e));
+    }
+    siddon_fan_bp_kernel<<<ray_grid(g, g.nbatch), 256, 0, s>>>(img, prj, deg, (int)g.nview, make_grid(g), make_det(g),
+                                                                (double)g.dsd, (double)g.dso);
+    return check_launch("siddon_fan_bp_kernel");
 }
 
 }  // namespace ctp

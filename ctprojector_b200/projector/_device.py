@@ -260,3 +260,41 @@ def tomo_filter(p, prj, det_center, src, filter_type: str = "hann", cutoff_x: fl
     check(lib().ctp_tomo_filter(ptr(fprj), ptr(t), ptr(dc), ptr(sr), byref(g), ifilter, c_float(cutoff_x),
                                 c_float(cutoff_z), wp, wn, stream_handle(stream, t.device)), "tomo filter_fbp")
     return fprj
+
+
+# --------------------------------------------------------------------------- numpy-only reference projectors
+def siddon_fan_fp(p, img, angles, out=None, stream=None):
+    """Fan-beam Siddon forward projection (the reference's numpy siddon_fp)."""
+    t = as_tensor(img, lowp_ok=False)
+    ang = as_tensor(angles, lowp_ok=False)
+    nb = t.shape[0]
+    g = make_geometry(p, nb, t.shape[1:], p.nu, p.nv, ang.numel(), fan_da(p), float(p.dsd), float(p.dso))
+    prj = _out([nb, ang.numel(), int(p.nv), int(p.nu)], torch.float32, t.device, out)
+    check(lib().ctp_siddon_fan_fp(ptr(prj), ptr(t), ptr(ang), byref(g), _lib.FLAG_ZERO_OUT,
+                                  stream_handle(stream, t.device)), "siddon_fp")
+    return prj
+
+
+def siddon_fan_bp(p, prj, angles, out=None, accumulate=False, stream=None):
+    """Fan-beam Siddon back projection (transpose of siddon_fan_fp)."""
+    t = as_tensor(prj, lowp_ok=False)
+    ang = as_tensor(angles, lowp_ok=False)
+    nb, nview, nv, nu = t.shape
+    g = make_geometry(p, nb, (p.nz, p.ny, p.nx), nu, nv, nview, fan_da(p), float(p.dsd), float(p.dso))
+    img = _out([nb, int(p.nz), int(p.ny), int(p.nx)], torch.float32, t.device, out)
+    check(lib().ctp_siddon_fan_bp(ptr(img), ptr(t), ptr(ang), byref(g), 0 if accumulate else _lib.FLAG_ZERO_OUT,
+                                  stream_handle(stream, t.device)), "siddon_bp")
+    return img
+
+
+def pixel_bp_parallel(p, prj, angles, out=None, accumulate=False, stream=None):
+    """Pixel-driven parallel back projection (the reference's numpy pixel_driven_bp)."""
+    t = as_tensor(prj, lowp_ok=False)
+    ang = as_tensor(angles, lowp_ok=False)
+    nb, nview, nv, nu = t.shape
+    g = make_geometry(p, nb, (p.nz, p.ny, p.nx), nu, nv, nview, float(p.du))
+    img = _out([nb, int(p.nz), int(p.ny), int(p.nx)], torch.float32, t.device, out)
+    check(lib().ctp_pixel_bp_parallel(ptr(img), ptr(t), ptr(ang), byref(g), 0 if accumulate else _lib.FLAG_ZERO_OUT,
+                                      stream_handle(stream, t.device)), "pixel_driven_bp")
+    return img
+

@@ -46,3 +46,15 @@ def distance_driven_bp(projector: ct_projector, prj, angles, is_fbp: Union[bool,
     FBP weighting; adjoint=True gives the exact transpose of distance_driven_fp."""
     return D.like_input(D.dd_bp(projector, prj, angles, _lib.GEOM_FAN, is_fbp, branchless, adjoint, out=out,
                                 accumulate=accumulate, stream=stream, dtype=dtype), prj)
+
+
+def siddon_fp(projector: ct_projector, img, angles, *, out=None, stream=None):
+    """Fan-beam forward projection, Siddon ray driven, on device arrays (the
+    reference has it in its numpy module only, fan_equiangluar.py:131)."""
+    return D.like_input(D.siddon_fan_fp(projector, img, angles, out=out, stream=stream), img)
+
+
+def siddon_bp(projector: ct_projector, prj, angles, *, out=None, accumulate=False, stream=None):
+    """Transpose of siddon_fp (reference numpy fan_equiangluar.py:185)."""
+    return D.like_input(D.siddon_fan_bp(projector, prj, angles, out=out, accumulate=accumulate, stream=stream), prj)
+

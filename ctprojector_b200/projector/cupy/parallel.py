@@ -32,3 +32,11 @@ def distance_driven_bp(projector: ct_projector, prj, angles, is_fbp: Union[bool,
     """Parallel-beam back projection, distance driven.  Returns [batch, nz, ny, nx]."""
     return D.like_input(D.dd_bp(projector, prj, angles, _lib.GEOM_PARALLEL, is_fbp, branchless, adjoint, out=out,
                                 accumulate=accumulate, stream=stream, dtype=dtype), prj)
+
+
+def pixel_driven_bp(projector: ct_projector, prj, angles, *, out=None, accumulate=False, stream=None):
+    """Pixel-driven parallel back projection on device arrays (the reference
+    has it in its numpy module only, parallel.py:75)."""
+    return D.like_input(D.pixel_bp_parallel(projector, prj, angles, out=out, accumulate=accumulate, stream=stream),
+                        prj)
+

@@ -1,8 +1,8 @@
 """Equiangular fan-beam geometry, host arrays.
 
 Same calls and module name (sic) as ct_projector/projector/numpy/fan_equiangluar.py
-of the reference: ramp_filter (:19), fbp_bp (:75), distance_driven_fp (:241),
-distance_driven_bp (:302).  Inputs are cast to float32.
+of the reference: ramp_filter (:19), fbp_bp (:75), siddon_fp (:131),
+siddon_bp (:185), distance_driven_fp (:241), distance_driven_bp (:302).  Inputs are cast to float32.
 """
 from __future__ import annotations
 
@@ -61,15 +61,25 @@ def distance_driven_bp(projector: ct_projector, prj: np.ndarray, angles: np.ndar
     return img
 
 
-def siddon_fp(projector: ct_projector, img, angles):
-    """Siddon fan projector (reference :326) is not part of this build."""
-    from ...errors import CTProjectorError
+def siddon_fp(projector: ct_projector, img: np.ndarray, angles: np.ndarray) -> np.ndarray:
+    """Fan-beam forward projection, Siddon ray driven (reference :131)."""
+    img = f32(img)
+    angles = f32(angles)
+    prj = np.zeros([img.shape[0], len(angles), projector.nv, projector.nu], np.float32)
+    call("cSiddonFanProjection", p(prj), p(img), p(angles), c_int(img.shape[0]),
+         *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:])[1:],
+         c_float(projector.du / projector.dsd), c_float(projector.dv), c_float(projector.off_u),
+         c_float(projector.off_v), c_float(projector.dsd), c_float(projector.dso))
+    return prj
 
-    raise CTProjectorError(1002, "fan_equiangluar.siddon_fp is not implemented in ctprojector_b200")
 
-
-def siddon_bp(projector: ct_projector, prj, angles):
-    """Siddon fan back projector (reference :380) is not part of this build."""
-    from ...errors import CTProjectorError
-
-    raise CTProjectorError(1002, "fan_equiangluar.siddon_bp is not implemented in ctprojector_b200")
+def siddon_bp(projector: ct_projector, prj: np.ndarray, angles: np.ndarray) -> np.ndarray:
+    """Fan-beam back projection, Siddon ray driven: the transpose of siddon_fp (reference :185)."""
+    prj = f32(prj)
+    angles = f32(angles)
+    img = np.zeros([prj.shape[0], projector.nz, projector.ny, projector.nx], np.float32)
+    call("cSiddonFanBackprojection", p(img), p(prj), p(angles), c_int(prj.shape[0]),
+         *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:])[1:],
+         c_float(projector.du / projector.dsd), c_float(projector.dv), c_float(projector.off_u),
+         c_float(projector.off_v), c_float(projector.dsd), c_float(projector.dso))
+    return img

@@ -1,7 +1,8 @@
 """Parallel-beam geometry, host arrays.
 
 Same calls as ct_projector/projector/numpy/parallel.py of the reference:
-ramp_filter (:20), distance_driven_fp (:133), distance_driven_bp (:192).
+ramp_filter (:20), pixel_driven_bp (:75), distance_driven_fp (:133),
+distance_driven_bp (:192).
 """
 from __future__ import annotations
 
@@ -47,8 +48,13 @@ def distance_driven_bp(projector: ct_projector, prj: np.ndarray, angles: np.ndar
     return img
 
 
-def pixel_driven_bp(projector: ct_projector, prj, angles):
-    """The pixel-driven parallel back projector (reference :75) is not part of this build."""
-    from ...errors import CTProjectorError
-
-    raise CTProjectorError(1002, "parallel.pixel_driven_bp is not implemented in ctprojector_b200")
+def pixel_driven_bp(projector: ct_projector, prj: np.ndarray, angles: np.ndarray) -> np.ndarray:
+    """Parallel back projection, pixel driven: bilinear detector interpolation,
+    no weights (reference :75)."""
+    prj = f32(prj)
+    angles = f32(angles)
+    img = np.zeros([prj.shape[0], projector.nz, projector.ny, projector.nx], np.float32)
+    call("cfbpParallelBackprojection", p(img), p(prj), p(angles),
+         *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(projector.du),
+         c_float(projector.dv), c_float(projector.off_u), c_float(projector.off_v), c_int(0))
+    return img

@@ -302,6 +302,31 @@ int ctp_tomo_filter(float* fprj, const float* prj, const float* detCenter, const
                     int filter, float cutoff_x, float cutoff_z, void* workspace, size_t workspace_bytes, void* stream);
 size_t ctp_tomo_filter_workspace(const ctp_geometry* g);
 
+/* Fan-beam Siddon pair, host pointers: siddonFan.cu:127 (cSiddonFanProjection)
+   and :201 (cSiddonFanBackprojection); da = du / dsd; outputs overwritten. */
+int cSiddonFanProjection(float* prj, const float* img, const float* deg, int nBatches, size_t nx, size_t ny,
+                         size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu, size_t nv,
+                         size_t nview, float da, float dv, float off_a, float off_v, float dsd, float dso);
+int cSiddonFanBackprojection(float* img, const float* prj, const float* deg, int nBatches, size_t nx, size_t ny,
+                             size_t nz, float dx, float dy, float dz, float cx, float cy, float cz, size_t nu,
+                             size_t nv, size_t nview, float da, float dv, float off_a, float off_v, float dsd,
+                             float dso);
+/* Pixel-driven parallel back projection, host pointers: fbpParallel.cu:271
+   (cfbpParallelBackprojection); img overwritten. */
+int cfbpParallelBackprojection(float* pImg, const float* pPrj, const float* pDeg, size_t nBatches, size_t nx,
+                               size_t ny, size_t nz, float dx, float dy, float dz, float cx, float cy, float cz,
+                               size_t nu, size_t nv, size_t nview, float du, float dv, float off_u, float off_v,
+                               int typeProjector);
+/* The same three on device pointers and a stream (no counterpart entries in
+   the reference, which has only the host-pointer ones); g->du is the angular
+   cell size for the fan pair; CTP_FLAG_ZERO_OUT writes instead of adding. */
+int ctp_siddon_fan_fp(float* prj, const float* img, const float* deg, const ctp_geometry* g, unsigned flags,
+                      void* stream);
+int ctp_siddon_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,
+                      void* stream);
+int ctp_pixel_bp_parallel(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,
+                          void* stream);
+
 /* Bounded device-side waits that gave up on the current device since the
    library was loaded (the streamed forward projector polls an mbarrier for
    each chunk of line tables with an iteration limit, and counts a limit that

@@ -659,6 +659,80 @@ void oracle_siddon_bp(double* img, const double* prj, const float* det_center, c
     free(priv);
 }
 
+/* Fan-beam Siddon rays (SiddonFanProjectionKernel, siddonFan.cu:12-44): the
+ * source on the circle of radius dso, the detector cell on the arc of radius
+ * dsd at angle a = (-(iu - (nu-1)/2) - off_u) da, both at height
+ * z = (iv - (nv-1)/2 + off_v) dv, rotated by the view angle; the end points
+ * are not moved towards the grid. */
+static void siddon_fan_ray_ends(double* src, double* dst, double deg, long iu, long iv, const og_det* d, double dsd,
+                                double dso)
+{
+    double c = cos(deg), s = sin(deg);
+    double a = (-(iu - (d->nu - 1) / 2.0) - d->off_u) * d->du;
+    double z = (iv - (d->nv - 1) / 2.0 + d->off_v) * d->dv;
+    double rx = dsd * sin(a), ry = -dso + dsd * cos(a);
+    src[0] = dso * s;
+    src[1] = -dso * c;
+    src[2] = z;
+    dst[0] = rx * c - ry * s;
+    dst[1] = rx * s + ry * c;
+    dst[2] = z;
+}
+
+/* prj = FP(img) for fan-beam Siddon (the reference's host entry zeroes prj). */
+void oracle_siddon_fan_fp(double* prj, const double* img, const double* deg, long nb, og_grid g, og_det d,
+                          long nview, double dsd, double dso)
+{
+    long nxyz = g.nx * g.ny * g.nz;
+    long nrays = nview * d.nv * d.nu;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long t = 0; t < nb * nrays; t++) {
+        long ib = t / nrays, k = t % nrays;
+        long iview = k / (d.nu * d.nv), iv = (k / d.nu) % d.nv, iu = k % d.nu;
+        double s[3], e[3];
+        siddon_fan_ray_ends(s, e, deg[iview], iu, iv, &d, dsd, dso);
+        prj[t] = siddon_walk(img + ib * nxyz, NULL, 0, NULL, 0, s, e, &g);
+    }
+}
+
+/* img = BP(prj) for fan-beam Siddon: the transpose with the same segments. */
+void oracle_siddon_fan_bp(double* img, const double* prj, const double* deg, long nb, og_grid g, og_det d,
+                          long nview, double dsd, double dso)
+{
+    long nxyz = g.nx * g.ny * g.nz;
+    int nt = 1;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    double* priv = (double*)calloc((size_t)nt * nxyz, sizeof(double));
+    for (long ib = 0; ib < nb; ib++) {
+        memset(priv, 0, sizeof(double) * nt * nxyz);
+#pragma omp parallel
+        {
+            int tid = 0;
+#ifdef _OPENMP
+            tid = omp_get_thread_num();
+#endif
+            double* acc = priv + (size_t)tid * nxyz;
+#pragma omp for schedule(static)
+            for (long iview = 0; iview < nview; iview++)
+                for (long iv = 0; iv < d.nv; iv++)
+                    for (long iu = 0; iu < d.nu; iu++) {
+                        double p = prj[((ib * nview + iview) * d.nv + iv) * d.nu + iu];
+                        double s[3], e[3];
+                        siddon_fan_ray_ends(s, e, deg[iview], iu, iv, &d, dsd, dso);
+                        siddon_walk(NULL, acc, p, NULL, 1, s, e, &g);
+                    }
+        }
+        for (long i = 0; i < nxyz; i++) {
+            double v = 0;
+            for (int t = 0; t < nt; t++) v += priv[(size_t)t * nxyz + i];
+            img[ib * nxyz + i] = v;
+        }
+    }
+    free(priv);
+}
+
 long long oracle_siddon_nnz(const float* det_center, const float* det_u, const float* det_v, const float* src,
                             og_grid g, og_det d, long nview)
 {

@@ -66,6 +66,8 @@ def lib():
         L.oracle_siddon_fp.argtypes = [dp, dp, fp, fp, fp, fp, c_long, _Grid, _Det, c_long]
         L.oracle_siddon_bp.argtypes = [dp, dp, fp, fp, fp, fp, c_long, _Grid, _Det, c_long]
         L.oracle_siddon_nnz.argtypes = [fp, fp, fp, fp, _Grid, _Det, c_long]
+        L.oracle_siddon_fan_fp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double]
+        L.oracle_siddon_fan_bp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double]
         L.oracle_siddon_nnz.restype = c_longlong
         L.oracle_tomo_fp.argtypes = [dp, dp, fp, fp, c_long, _Grid, _Det, c_long]
         L.oracle_tomo_bp.argtypes = [dp, dp, fp, fp, c_long, _Grid, _Det, c_long]
@@ -390,3 +392,67 @@ def tomo_filter(p, prj, det_center, src, filter_type="hann", cutoff_x=1.0, cutof
         full = np.fft.irfft(X * np.fft.rfft(g, n=n), n=n, axis=-1)
         out[:, v] = full[..., nu - 1: 2 * nu - 1] * (np.pi / nview * vdu)
     return out
+
+
+def siddon_fan_fp(p, img, angles):
+    """fan_equiangluar.siddon_fp (numpy module): fan-beam Siddon rays,
+    siddonFan.cu:12-44 (angular cell size du / dsd)."""
+    img = _d(img)
+    ang = _d(angles)
+    nb = img.shape[0]
+    prj = np.zeros([nb, len(ang), int(p.nv), int(p.nu)], np.float64)
+    lib().oracle_siddon_fan_fp(_ptr(prj), _ptr(img), _ptr(ang), nb, _grid(p, img.shape[1:]),
+                               _det(p, p.nu, p.nv, _fan_da(p)), len(ang), float(np.float32(p.dsd)),
+                               float(np.float32(p.dso)))
+    return prj
+
+
+def siddon_fan_bp(p, prj, angles):
+    """fan_equiangluar.siddon_bp: the transpose of siddon_fan_fp."""
+    prj = _d(prj)
+    ang = _d(angles)
+    nb, nview, nv, nu = prj.shape
+    img = np.zeros([nb, int(p.nz), int(p.ny), int(p.nx)], np.float64)
+    lib().oracle_siddon_fan_bp(_ptr(img), _ptr(prj), _ptr(ang), nb, _grid(p), _det(p, nu, nv, _fan_da(p)), nview,
+                               float(np.float32(p.dsd)), float(np.float32(p.dso)))
+    return img
+
+
+def pixel_bp_parallel(p, prj, angles):
+    """parallel.pixel_driven_bp (numpy module; bpParallelKernel3D,
+    fbpParallel.cu:200-250): per pixel centre and view the detector position
+    pu = -((x cos + y sin)/du + off_u) + (nu-1)/2, pv per slice, bilinear
+    interpolation that returns 0 outside [0, n) (InterpolateXY with truncate,
+    cudaMath.cu:227-260), summed over views without weights."""
+    prj = _d(prj)
+    ang = _d(angles)
+    nb, nview, nv, nu = prj.shape
+    nx, ny, nz = int(p.nx), int(p.ny), int(p.nz)
+    f = lambda v: float(np.float32(v))  # noqa: E731
+    dx, dy, dz, cx, cy, cz = (f(getattr(p, k)) for k in ("dx", "dy", "dz", "cx", "cy", "cz"))
+    du, dv, off_u, off_v = f(p.du), f(p.dv), f(p.off_u), f(p.off_v)
+    x = (np.arange(nx) + 0.5 - nx / 2.0) * dx + cx
+    y = (np.arange(ny) + 0.5 - ny / 2.0) * dy + cy
+    z = (np.arange(nz) + 0.5 - nz / 2.0) * dz + cz
+    X, Y = np.meshgrid(x, y)
+    img = np.zeros([nb, nz, ny, nx])
+    pv = z / dv + off_v + (nv - 1) / 2.0
+    for v in range(nview):
+        c, s = np.cos(ang[v]), np.sin(ang[v])
+        pu = -((X * c + Y * s) / du + off_u) + (nu - 1) / 2.0
+        uin = (pu >= 0) & (pu < nu)
+        i0 = np.clip(np.floor(pu).astype(np.int64), 0, nu - 1)
+        i1 = np.clip(i0 + 1, 0, nu - 1)
+        wu = np.where(uin, pu - i0, 0.0)
+        for iz in range(nz):
+            if not (0 <= pv[iz] < nv):
+                continue
+            j0 = int(np.floor(pv[iz]))
+            j1 = min(j0 + 1, nv - 1)
+            wv = pv[iz] - j0
+            r0, r1 = prj[:, v, j0], prj[:, v, j1]
+            val = (r0[:, i0] * (1 - wu) * (1 - wv) + r0[:, i1] * wu * (1 - wv) + r1[:, i0] * (1 - wu) * wv +
+                   r1[:, i1] * wu * wv)
+            img[:, iz] += np.where(uin, val, 0.0)
+    return img
+

@@ -130,6 +130,27 @@ class Ref:
         return img
 
 
+    # fan_equiangluar.py:131-238 (numpy module): nBatches passed as an unsigned long
+    def siddon_fan(self, p, x, ang, fp):
+        if fp:
+            out = np.zeros([x.shape[0], len(ang), p.nv, p.nu], np.float32)
+            shapes = (x.shape[1:], out.shape[1:])
+        else:
+            out = np.zeros([x.shape[0], p.nz, p.ny, p.nx], np.float32)
+            shapes = (out.shape[1:], x.shape[1:])
+        self.call("cSiddonFanProjection" if fp else "cSiddonFanBackprojection", ptr(out), ptr(x), ptr(ang),
+                  *geom(p, x.shape[0], *shapes), c_float(p.du / p.dsd), c_float(p.dv), c_float(p.off_u),
+                  c_float(p.off_v), c_float(p.dsd), c_float(p.dso))
+        return out
+
+    # parallel.py:75-130 (numpy module)
+    def pixel_bp(self, p, prj, ang):
+        img = np.zeros([prj.shape[0], p.nz, p.ny, p.nx], np.float32)
+        self.call("cfbpParallelBackprojection", ptr(img), ptr(prj), ptr(ang),
+                  *geom(p, prj.shape[0], img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv),
+                  c_float(p.off_u), c_float(p.off_v), c_int(0))
+        return img
+
     # tomo.py:157-221: the reference has only the device entry, called with device buffers
     def tomo_filter(self, p, prj, dc, src, ifilter, cutoff_x, cutoff_z):
         import torch
@@ -162,6 +183,10 @@ def run_case(ref: Ref, fn):
         out["bp_fbp"] = ref.dd_bp(p, out["filter_hann"], ang, fan, 1)
         if fan:
             out["fbp_bp"] = ref.fbp_bp(p, out["filter_hann"], ang)
+            out["siddon_fp"] = ref.siddon_fan(p, img, ang, True)
+            out["siddon_bp"] = ref.siddon_fan(p, out["siddon_fp"], ang, False)
+        else:
+            out["pixel_bp"] = ref.pixel_bp(p, out["filter_hann"], ang)
     elif name == "kat":
         out["fp"] = ref.dd_fp(p, inp["img"], inp["angles"], False)
         out["bp_fbp"] = ref.dd_bp(p, inp["prj"], inp["angles"], False, 1)

@@ -230,3 +230,45 @@ def test_tomo_filter_matches_oracle_and_reference(oracle, key, name, cx, cz):
     if f"filter_{key}" in ref:
         out = host(tomo.filter_fbp(p, dev(ref["fp"]), dev(ginp["det_center"]), dev(ginp["src"]), name, cx, cz))
         assert rel_l2(out, ref[f"filter_{key}"]) <= TOL
+
+
+@pytest.mark.parametrize("name", ["fan_basic", "fan_offsets", "fan_wide"])
+def test_siddon_fan_matches_oracle_and_reference(oracle, name):
+    """Fan-beam Siddon pair (numpy-module projector of the reference): CUDA
+    vs the FP64 oracle and vs the reference's own outputs, and the adjoint
+    identity."""
+    from ctprojector_b200.projector.cupy import fan_equiangular as F
+    from ctprojector_b200.projector.numpy import fan_equiangluar as NF
+
+    p, inp = _case(name)
+    ang = dev(inp["angles"])
+    prj = host(F.siddon_fp(p, dev(inp["img"]), ang))
+    assert rel_l2(prj, oracle.siddon_fan_fp(p, inp["img"], inp["angles"])) <= TOL
+    bp = host(F.siddon_bp(p, dev(prj), ang))
+    assert rel_l2(bp, oracle.siddon_fan_bp(p, prj, inp["angles"])) <= TOL
+    assert rel_l2(NF.siddon_fp(p, inp["img"], inp["angles"]), prj) <= 1e-6  # host entry, same kernels
+    rng = np.random.default_rng(2)
+    y = rng.uniform(0, 1, prj.shape).astype(np.float32)
+    aty = host(F.siddon_bp(p, dev(y), ang))
+    assert abs(np.vdot(prj.astype(np.float64), y) - np.vdot(inp["img"].astype(np.float64), aty)) / (
+        np.linalg.norm(prj) * np.linalg.norm(y)) <= ADJ_TOL
+    _, ginp, ref = load_golden(name)
+    if "siddon_fp" in ref:
+        assert rel_l2(host(F.siddon_fp(p, dev(ginp["img"]), dev(ginp["angles"]))), ref["siddon_fp"]) <= TOL
+        assert rel_l2(host(F.siddon_bp(p, dev(ref["siddon_fp"]), dev(ginp["angles"]))), ref["siddon_bp"]) <= TOL
+
+
+@pytest.mark.parametrize("name", ["par_basic", "par_offsets", "par_wide"])
+def test_pixel_driven_bp_matches_oracle_and_reference(oracle, name):
+    from ctprojector_b200.projector.cupy import parallel as P
+    from ctprojector_b200.projector.numpy import parallel as NP
+
+    p, inp = _case(name)
+    rng = np.random.default_rng(4)
+    prj = rng.uniform(0, 1, (inp["img"].shape[0], len(inp["angles"]), p.nv, p.nu)).astype(np.float32)
+    out = host(P.pixel_driven_bp(p, dev(prj), dev(inp["angles"])))
+    assert rel_l2(out, oracle.pixel_bp_parallel(p, prj, inp["angles"])) <= TOL
+    assert rel_l2(NP.pixel_driven_bp(p, prj, inp["angles"]), out) <= 1e-6
+    _, ginp, ref = load_golden(name)
+    if "pixel_bp" in ref:
+        assert rel_l2(host(P.pixel_driven_bp(p, dev(ref["filter_hann"]), dev(ginp["angles"]))), ref["pixel_bp"]) <= TOL
