@@ -108,22 +108,46 @@ __device__ Ray init_ray(const double src[3], const double dst[3], const Grid& g)
 
 // The walk of SiddonRayTracing (siddon.cu:187-252): pick the nearest
 // crossing (ties go to the later axis), emit the segment in the current voxel,
-// step, stop when the index leaves the grid.
+// step, stop when the index leaves the grid.  The per-axis state is held in
+// scalars and the axis is chosen with branches, so nothing is indexed at run
+// time and the walk stays in registers.
 template <typename F>
-__device__ __forceinline__ void walk(Ray& R, const Grid& g, F&& emit) {
-    int n[3] = {g.nx, g.ny, g.nz};
-    long long nxy = (long long)g.nx * g.ny;
-    long long idx = R.ng[2] * nxy + (long long)R.ng[1] * g.nx + R.ng[0];
-    long long mv[3] = {R.step[0], (long long)R.step[1] * g.nx, R.step[2] * nxy};
+__device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
+    double a0 = R.alpha[0], a1 = R.alpha[1], a2 = R.alpha[2];
+    const double d0 = R.dalpha[0], d1 = R.dalpha[1], d2 = R.dalpha[2];
+    int g0 = R.ng[0], g1 = R.ng[1], g2 = R.ng[2];
+    const int s0 = R.step[0], s1 = R.step[1], s2 = R.step[2];
+    const long long nxy = (long long)g.nx * g.ny;
+    const long long m1 = (long long)s1 * g.nx, m2 = (long long)s2 * nxy;
+    long long idx = g2 * nxy + (long long)g1 * g.nx + g0;
+    double aprev = R.aprev;
     while (true) {
-        int k = (R.alpha[0] < R.alpha[1] && R.alpha[0] < R.alpha[2]) ? 0 : (R.alpha[1] < R.alpha[2] ? 1 : 2);
-        double anow = R.alpha[k];
-        R.alpha[k] += R.dalpha[k];
-        R.ng[k] += R.step[k];
-        emit(idx, (float)(anow - R.aprev));
-        R.aprev = anow;
-        if (R.ng[k] < 0 || R.ng[k] >= n[k]) break;
-        idx += mv[k];
+        double anow;
+        bool out;
+        long long mv;
+        if (a0 < a1 && a0 < a2) {
+            anow = a0;
+            a0 += d0;
+            g0 += s0;
+            out = g0 < 0 || g0 >= g.nx;
+            mv = s0;
+        } else if (a1 < a2) {
+            anow = a1;
+            a1 += d1;
+            g1 += s1;
+            out = g1 < 0 || g1 >= g.ny;
+            mv = m1;
+        } else {
+            anow = a2;
+            a2 += d2;
+            g2 += s2;
+            out = g2 < 0 || g2 >= g.nz;
+            mv = m2;
+        }
+        emit(idx, (float)(anow - aprev));
+        aprev = anow;
+        if (out) break;
+        idx += mv;
     }
 }
 
@@ -142,7 +166,16 @@ __global__ void __launch_bounds__(256) siddon_fp_kernel(Tout* __restrict__ prj, 
     float acc = 0.f;
     if (R.hit) {
         const Tin* vol = img + (size_t)b * g.nx * g.ny * g.nz;
-        walk(R, g, [&](long long idx, float len) { acc += ldf(vol + idx) * len; });
+        // each sample is added one step later, so its load overlaps the next
+        // step's arithmetic; the summation order is unchanged
+        float pv = 0.f, pl = 0.f;
+        walk(R, g, [&](long long idx, float len) {
+            const float v = ldf(vol + idx);
+            acc = fmaf(pv, pl, acc);
+            pv = v;
+            pl = len;
+        });
+        acc = fmaf(pv, pl, acc);
     }
     Tout* o = prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu;
     stf(o, (accumulate ? rdf(o) : 0.f) + acc);
@@ -225,7 +258,14 @@ __global__ void __launch_bounds__(256) siddon_fan_fp_kernel(float* __restrict__ 
     float acc = 0.f;
     if (R.hit) {
         const float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
-        walk(R, g, [&](long long idx, float len) { acc += __ldg(vol + idx) * len; });
+        float pv = 0.f, pl = 0.f;
+        walk(R, g, [&](long long idx, float len) {
+            const float v = __ldg(vol + idx);
+            acc = fmaf(pv, pl, acc);
+            pv = v;
+            pl = len;
+        });
+        acc = fmaf(pv, pl, acc);
     }
     float* o = prj + (((size_t)b * nview + view) * d.nv + iv) * d.nu + iu;
     *o = (accumulate ? *o : 0.f) + acc;
