@@ -1615,6 +1615,8 @@ size_t fp_line_tables_bytes(const ctp_geometry& g) {
     return align_up(slices * (g.ny * (g.nx + 1) + g.nx * (g.ny + 1)) * sizeof(float4));
 }
 
+constexpr size_t kFpStreamMinSlices = 8;
+
 // Lines per chunk of the streamed path's two-buffer ring, or 0 if one line
 // per buffer does not fit.
 int fp_stream_chunk(const ctp_geometry& g) {
@@ -1697,26 +1699,6 @@ bool fp_stream_shape(const ctp_geometry& g, int S, int& vgroup, int& ni) {
     return vgroup > 0;
 }
 
-// Two-slice instances exist for float output only (16-bit outputs use one slice per CTA).
-template <typename Tout, typename L>
-void fp_stream_launch_s2(L& launch, bool fan, int ni) {
-    if constexpr (std::is_same<Tout, float>::value) {
-        if (ni == 4) {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 4, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 4, 2, Tout>);
-        } else if (ni == 6) {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 6, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 6, 2, Tout>);
-        } else if (ni == 8) {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 8, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 8, 2, Tout>);
-        } else {
-            if (fan) launch(dd2d_fp_stream_kernel<true, 10, 2, Tout>); else launch(dd2d_fp_stream_kernel<false, 10, 2, Tout>);
-        }
-    } else {
-        (void)launch;
-        (void)fan;
-        (void)ni;
-    }
-}
-
 template <typename Tin, typename Tout>
 int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
               unsigned flags, char* ws, size_t ws_bytes, cudaStream_t s) {
@@ -1730,7 +1712,9 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
     int vgroup = 0, nrows = 0;
     const int rchunk = fp_stream_chunk(g);
-    if (fp_fast_ok(g, vgroup, nrows) && rchunk > 0 &&
+    // the streamed path pays off on stacks (the table pass is shared by every
+    // view group of a slice); a few slices run the staged kernel
+    if (fp_fast_ok(g, vgroup, nrows) && rchunk > 0 && g.nbatch * g.nz >= kFpStreamMinSlices &&
         ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
         // streamed path: line tables of rows (from the image) and columns (from its transpose)
         float4* lt0 = reinterpret_cast<float4*>(ws + fp_workspace_min(g));
@@ -1741,14 +1725,12 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         line_tables_kernel<Tin><<<(unsigned)std::min<long long>((cols + 7) / 8, 148 * 16), 256, 0, s>>>(
             lt1, imgT, cols, (int)g.ny);
         if ((rc = check_launch("line_tables_kernel"))) return rc;
-        // slices per CTA: 2 for stacks with float output, else 1
+        // one slice per CTA: sharing the edge work across two slices halves the
+        // lines per table chunk, and the warps then wait on the copies instead
         const int nslices = (int)(g.nbatch * g.nz);
-        int S = (nslices >= 2 && !std::is_same<Tout, __half>::value && !std::is_same<Tout, __nv_bfloat16>::value) ? 2 : 1;
+        const int S = 1;
         int sv = 0, ni = 0;
-        if (!fp_stream_shape(g, S, sv, ni)) {
-            S = 1;
-            fp_stream_shape(g, 1, sv, ni);
-        }
+        fp_stream_shape(g, S, sv, ni);
         const int rc_s = std::max(1, rchunk / S);
         size_t shm = 2 * (size_t)S * rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)((nslices + S - 1) / S));
@@ -1762,14 +1744,10 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
 #define CTP_FP_STREAM(NI_, S_)                                                   \
     if (fan) launch(dd2d_fp_stream_kernel<true, NI_, S_, Tout>);                 \
     else launch(dd2d_fp_stream_kernel<false, NI_, S_, Tout>)
-        if (S == 1) {
-            if (ni == 4) { CTP_FP_STREAM(4, 1); }
-            else if (ni == 8) { CTP_FP_STREAM(8, 1); }
-            else if (ni == 12) { CTP_FP_STREAM(12, 1); }
-            else { CTP_FP_STREAM(16, 1); }
-        } else {
-            fp_stream_launch_s2<Tout>(launch, fan, ni);
-        }
+        if (ni == 4) { CTP_FP_STREAM(4, 1); }
+        else if (ni == 8) { CTP_FP_STREAM(8, 1); }
+        else if (ni == 12) { CTP_FP_STREAM(12, 1); }
+        else { CTP_FP_STREAM(16, 1); }
 #undef CTP_FP_STREAM
         return check_launch("dd2d_fp_stream_kernel");
     }
@@ -1808,7 +1786,7 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
 // ------------------------------------------------------------------ launchers
 size_t dd2d_fp_workspace(const ctp_geometry& g, int, int, unsigned) {
     int vgroup = 0, nrows = 0;
-    bool stream = fp_fast_ok(g, vgroup, nrows) && fp_stream_chunk(g) > 0;
+    bool stream = fp_fast_ok(g, vgroup, nrows) && fp_stream_chunk(g) > 0 && g.nbatch * g.nz >= kFpStreamMinSlices;
     return fp_workspace_min(g) + (stream ? fp_line_tables_bytes(g) : 0);
 }
 

@@ -29,10 +29,18 @@ MIX: Dict[str, float] = {
 MIX_2D: Dict[str, float] = {k: v for k, v in MIX.items() if not k.startswith("cone")}
 
 
+def _offset(angles: np.ndarray, step: float) -> np.ndarray:
+    """Views shifted by half a view step.  No view then lies exactly on a 45
+    degree diagonal, where the reference's axis choice (reproduced here with
+    the same fast intrinsics) and an exact-trigonometry reconstruction may
+    pick different axes for that view."""
+    return (angles + np.float32(step / 2)).astype(np.float32)
+
+
 def catalog(storage: str = "bfloat16", n_iter: int = 20, image_storage: str = "float32",
             beta: float = 2e-4, eps: float = 1e-6) -> Dict[str, Protocol]:
-    """The protocols of the served stream (geometry of each family as in the
-    projector workloads: fan 256^2 / 360 views / 736 cells and fan 512^2 / 984
+    """The protocols of the served stream (views start half a view step past
+    0; geometry of each family as in the projector workloads: fan 256^2 / 360 views / 736 cells and fan 512^2 / 984
     views / 888 cells at SID 595, SDD 1085.6; parallel 512^2 / 720 views / 768
     cells; helical cone 64 x 512^2 at 0.7 x 0.7 x 1.0 mm, 360 views over one
     turn, 736 x 64 panel)."""
@@ -41,15 +49,17 @@ def catalog(storage: str = "bfloat16", n_iter: int = 20, image_storage: str = "f
     par512 = S.Scan(512, 512, 1, 0.8, 0.8, 1.0, 768, 1, 0.8, 1.0, 720)
     cone64 = S.Scan(512, 512, 64, 0.7, 0.7, 1.0, 736, 64, 1.2858, 1.0, 360)
     cgeo = S.helical(360, 1.0, cone64.dso, cone64.dsd, 64 * 1.0 * cone64.dso / cone64.dsd)
+    full = lambda n: _offset(S.angles(n, 2 * np.pi), 2 * np.pi / n)  # noqa: E731
+    half = lambda n: _offset(S.angles(n, np.pi), np.pi / n)  # noqa: E731
     sq = dict(n_iter=n_iter, beta=beta, tv_weights=(1.0, 1.0, 1.0), eps=eps, storage=storage,
               image_storage=image_storage)
     return {
-        "fan256_fbp": Protocol("fan256_fbp", "fan", "fbp", fan256, angles=S.angles(360, 2 * np.pi), storage=storage),
-        "fan256_sqs": Protocol("fan256_sqs", "fan", "sqs", fan256, angles=S.angles(360, 2 * np.pi), **sq),
-        "fan512_fbp": Protocol("fan512_fbp", "fan", "fbp", fan512, angles=S.angles(984, 2 * np.pi), storage=storage),
-        "fan512_sqs": Protocol("fan512_sqs", "fan", "sqs", fan512, angles=S.angles(984, 2 * np.pi), **sq),
-        "par512_fbp": Protocol("par512_fbp", "parallel", "fbp", par512, angles=S.angles(720, np.pi), storage=storage),
-        "par512_sqs": Protocol("par512_sqs", "parallel", "sqs", par512, angles=S.angles(720, np.pi), **sq),
+        "fan256_fbp": Protocol("fan256_fbp", "fan", "fbp", fan256, angles=full(360), storage=storage),
+        "fan256_sqs": Protocol("fan256_sqs", "fan", "sqs", fan256, angles=full(360), **sq),
+        "fan512_fbp": Protocol("fan512_fbp", "fan", "fbp", fan512, angles=full(984), storage=storage),
+        "fan512_sqs": Protocol("fan512_sqs", "fan", "sqs", fan512, angles=full(984), **sq),
+        "par512_fbp": Protocol("par512_fbp", "parallel", "fbp", par512, angles=half(720), storage=storage),
+        "par512_sqs": Protocol("par512_sqs", "parallel", "sqs", par512, angles=half(720), **sq),
         "cone64_sqs": Protocol("cone64_sqs", "cone", "sqs", cone64, cone=cgeo, **sq),
     }
 

@@ -149,6 +149,7 @@ def test_job_joins_a_running_lane():
     eng._admit(0.0)
     lane = eng.lanes["fan_sqs"]
     for _ in range(4):
+        torch.cuda.synchronize()  # a lane with two steps in flight is not stepped
         eng._step()
     eng.submit(b)
     eng._admit(0.0)

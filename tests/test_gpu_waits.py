@@ -37,9 +37,10 @@ def _fp(g, geom_kind, img, ang, ws_bytes):
 def test_streamed_fp_equals_staged(geom_kind, n, nview, nu, du):
     from ctprojector_b200._lib import Geometry, lib
 
-    g = Geometry(3, n, n, 1, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, nu, 1, nview, du, 1.0, 0.0, 0.0, 1085.6, 595.0)
+    # 8 slices: the smallest stack that takes the streamed path
+    g = Geometry(8, n, n, 1, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, nu, 1, nview, du, 1.0, 0.0, 0.0, 1085.6, 595.0)
     rng = np.random.default_rng(n)
-    img = torch.tensor(rng.uniform(0, 1, (3, 1, n, n)).astype(np.float32), device="cuda")
+    img = torch.tensor(rng.uniform(0, 1, (8, 1, n, n)).astype(np.float32), device="cuda")
     span = 2 * np.pi if geom_kind == 0 else np.pi
     ang = torch.tensor((np.arange(nview) * span / nview).astype(np.float32), device="cuda")
     full = lib().ctp_dd2d_fp_workspace(ctypes.byref(g), geom_kind, 0, 0)
