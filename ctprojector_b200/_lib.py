@@ -30,6 +30,7 @@ FLAG_IN_FP16 = 0x20
 FLAG_OUT_BF16 = 0x40
 FLAG_OUT_FP16 = 0x80
 FLAG_FILTER_EXACT = 0x100
+FLAG_TOMO_FIRST_VIEW_KERNEL = 0x200
 
 TYPE_FBP = 0x1
 TYPE_BRANCHLESS = 0x2
@@ -114,7 +115,7 @@ _SIGNATURES = {
     "ctp_siddon_fan_bp": [_P, _P, _P, _GP, c_uint, _P],
     "ctp_pixel_bp_parallel": [_P, _P, _P, _GP, c_uint, _P],
     "cupyFbpTomoFilter": [_P, _P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, c_int, _F, _F],
-    "ctp_tomo_filter": [_P, _P, _P, _P, _GP, c_int, _F, _F, _P, _S, _P],
+    "ctp_tomo_filter": [_P, _P, _P, _P, _GP, c_int, _F, _F, c_uint, _P, _S, _P],
     "ctp_tomo_filter_workspace": [_GP],
     "ctp_sqs_tv_update": [_P, _P, _P, _P, _P, _S, _P, _F, _F, _F, _F, _F, _S, _S, _S, c_uint, _P],
 }

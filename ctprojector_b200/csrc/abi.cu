@@ -37,8 +37,8 @@ int siddon_fan_fp(float*, const float*, const float*, const ctp_geometry&, unsig
 int siddon_fan_bp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 int pixel_bp_parallel(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 size_t tomo_filter_workspace(const ctp_geometry&);
-int tomo_filter(float*, const float*, const float*, const float*, const ctp_geometry&, int, float, float, void*, size_t,
-                cudaStream_t);
+int tomo_filter(float*, const float*, const float*, const float*, const ctp_geometry&, int, float, float, unsigned,
+                void*, size_t, cudaStream_t);
 int sqs_tv_update(float*, void*, const float*, const float*, const float*, size_t, const unsigned char*, float, float,
                   float, float, float, size_t, size_t, size_t, unsigned, cudaStream_t);
 int tv_sqs(float*, float*, float*, const float*, float, float, float, size_t, size_t, size_t, size_t, float,
@@ -735,13 +735,14 @@ int cupyFbpTomoFilter(float* fprj, const float* prj, const float* detCenter, con
     if (nBatches < 0) return set_error(CTP_ERR_INVALID_ARGUMENT, "negative batch count");
     ctp_geometry g = make_geom((size_t)nBatches, 1, 1, 1, dx, 1.f, dz, 0.f, 0.f, 0.f, nu, nv, nview, du, 1.f, 0.f, 0.f,
                                0.f, 0.f);
-    return finish_sync(tomo_filter(fprj, prj, detCenter, src, g, typeFilter, cutoffX, cutoffZ, nullptr, 0, 0), 0);
+    return finish_sync(tomo_filter(fprj, prj, detCenter, src, g, typeFilter, cutoffX, cutoffZ, 0, nullptr, 0, 0), 0);
 }
 
 int ctp_tomo_filter(float* fprj, const float* prj, const float* detCenter, const float* src, const ctp_geometry* g,
-                    int filter, float cutoff_x, float cutoff_z, void* workspace, size_t workspace_bytes, void* stream) {
+                    int filter, float cutoff_x, float cutoff_z, unsigned flags, void* workspace,
+                    size_t workspace_bytes, void* stream) {
     if (!g) return set_error(CTP_ERR_INVALID_ARGUMENT, "geometry pointer is null");
-    return tomo_filter(fprj, prj, detCenter, src, *g, filter, cutoff_x, cutoff_z, workspace, workspace_bytes,
+    return tomo_filter(fprj, prj, detCenter, src, *g, filter, cutoff_x, cutoff_z, flags, workspace, workspace_bytes,
                        as_stream(stream));
 }
 

@@ -1927,12 +1927,17 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
         int pwin = par_fast_window(g);
         if (pwin > 0) {
             int tiles_p = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
-            // two slices per CTA for stacks (shared per-view work), one otherwise
+            // slices per CTA for stacks (shared per-view work): 4, 2 or 1
             const int nslices = (int)(g.nbatch * g.nz);
-            const int S = nslices >= 2 ? 2 : 1;
+            const int S = nslices >= 4 ? 4 : nslices >= 2 ? 2 : 1;
             size_t pshm = par_fast_smem(pwin, S);
             dim3 pg((unsigned)tiles_p, (unsigned)((nslices + S - 1) / S));
-            if (S == 2) {
+            if (S == 4) {
+                auto kf = dd2d_bp_par_fast_kernel<Tin, Tout, 4>;
+                cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
+                kf<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin,
+                                         nslices);
+            } else if (S == 2) {
                 auto kf = dd2d_bp_par_fast_kernel<Tin, Tout, 2>;
                 cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
                 kf<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin,

@@ -656,7 +656,8 @@ size_t tomo_filter_workspace(const ctp_geometry& g) {
 }
 
 int tomo_filter(float* fprj, const float* prj, const float* det_center, const float* src, const ctp_geometry& g,
-                int filter, float cutoff_x, float cutoff_z, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+                int filter, float cutoff_x, float cutoff_z, unsigned flags, void* workspace, size_t workspace_bytes,
+                cudaStream_t s) {
     if (g.nbatch == 0) return CTP_OK;
     if (!fprj || !prj || !det_center || !src) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g.nu == 0 || g.nv == 0 || g.nview == 0) return set_error(CTP_ERR_INVALID_ARGUMENT, "zero detector extent");
@@ -696,7 +697,10 @@ int tomo_filter(float* fprj, const float* prj, const float* det_center, const fl
     // the reference; the filter is not on a hot path): the scratch must exist first
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return set_error((int)e, "tomo filter: %s", cudaGetErrorString(e));
-    if ((rc = build_tomo_spectra(spec, views, nu, g.dx, g.dz, cutoff_x, cutoff_z, filter))) return rc;
+    // the reference multiplies every view by the first view's kernel (fbpTomo.cu:323)
+    const bool first_only = flags & CTP_FLAG_TOMO_FIRST_VIEW_KERNEL;
+    const std::vector<TomoView> kviews = first_only ? std::vector<TomoView>(1, views[0]) : views;
+    if ((rc = build_tomo_spectra(spec, kviews, nu, g.dx, g.dz, cutoff_x, cutoff_z, filter))) return rc;
     e = cudaMemcpyAsync(dscale, scale.data(), sizeof(float) * nview, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return set_error((int)e, "tomo filter scales: %s", cudaGetErrorString(e));
@@ -711,7 +715,8 @@ int tomo_filter(float* fprj, const float* prj, const float* det_center, const fl
         for (size_t r0 = 0; r0 < rows; r0 += nv)
             if (cufftExecR2C(plan->fwd, pad + r0 * L, frq + r0 * nu) != CUFFT_SUCCESS)
                 return set_error(CTP_ERR_CUFFT, "cufftExecR2C failed");
-        tomo_cmul_kernel<<<(unsigned)((rows * nu + 255) / 256), 256, 0, s>>>(frq, spec, nu, nv, nview, rows);
+        tomo_cmul_kernel<<<(unsigned)((rows * nu + 255) / 256), 256, 0, s>>>(frq, spec, nu, nv,
+                                                                           first_only ? 1 : nview, rows);
         if ((rc = check_launch("tomo_cmul_kernel"))) return rc;
         for (size_t r0 = 0; r0 < rows; r0 += nv)
             if (cufftExecC2R(plan->inv, frq + r0 * nu, pad + r0 * L) != CUFFT_SUCCESS)

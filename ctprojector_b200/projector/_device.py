@@ -246,9 +246,10 @@ def tomo_bp(p, prj, det_center, src, out=None, stream=None):
 
 
 def tomo_filter(p, prj, det_center, src, filter_type: str = "hann", cutoff_x: float = 1.0, cutoff_z: float = 1.0,
-                out=None, stream=None):
+                out=None, stream=None, first_view_kernel: bool = False):
     """Tomosynthesis FBP filter; 'hamming' 1, 'hann' 2, anything else none
-    (tomo.py:188-193 of the reference cupy wrapper)."""
+    (tomo.py:188-193 of the reference cupy wrapper).  ``first_view_kernel``
+    filters every view with the first view's kernel, as the reference does."""
     t = as_tensor(prj, lowp_ok=False)
     dc, sr = _geom3(det_center), _geom3(src)
     nb, nview, nv, nu = t.shape
@@ -257,8 +258,9 @@ def tomo_filter(p, prj, det_center, src, filter_type: str = "hann", cutoff_x: fl
     ft = filter_type.lower()
     ifilter = 1 if ft == "hamming" else 2 if ft == "hann" else 0
     ws, wp, wn = workspace(lib().ctp_tomo_filter_workspace(byref(g)), t.device)
+    flags = _lib.FLAG_TOMO_FIRST_VIEW_KERNEL if first_view_kernel else 0
     check(lib().ctp_tomo_filter(ptr(fprj), ptr(t), ptr(dc), ptr(sr), byref(g), ifilter, c_float(cutoff_x),
-                                c_float(cutoff_z), wp, wn, stream_handle(stream, t.device)), "tomo filter_fbp")
+                                c_float(cutoff_z), flags, wp, wn, stream_handle(stream, t.device)), "tomo filter_fbp")
     return fprj
 
 

@@ -53,6 +53,8 @@ extern "C" {
 /* ---- flags for the extended entries ------------------------------------ */
 #define CTP_FLAG_ZERO_OUT 0x1  /* treat the output as zero (write instead of accumulate) */
 #define CTP_FLAG_ADJOINT 0x2   /* DD back projection: exact transpose of the forward projector */
+#define CTP_FLAG_TOMO_FIRST_VIEW_KERNEL 0x200 /* tomo filter: every view uses the first view's kernel, as the
+                                                 reference computes (fbpTomo.cu:323); default: each view its own */
 #define CTP_FLAG_IN_BF16 0x10  /* the input array is bfloat16 (FP32 accumulation) */
 #define CTP_FLAG_IN_FP16 0x20  /* the input array is float16 */
 #define CTP_FLAG_OUT_BF16 0x40 /* the output array is bfloat16 */
@@ -292,14 +294,17 @@ int ctp_tv_sqs(float* s1, float* s2, float* var, const float* img, float wx, flo
 /* Tomosynthesis FBP filter, fbpTomo.cu:386 (cupyFbpTomoFilter, device
    pointers; nBatches is an int in the reference's C signature).  Per view the
    ramp at the virtual pitch du*cos(tilt), windowed (typeFilter 1 Hamming,
-   2 Hann, else none) with x/z cut-offs; fprj is overwritten. */
+   2 Hann, else none) with x/z cut-offs; fprj is overwritten.  Each view is
+   filtered with its own kernel; the reference applies the first view's
+   kernel to every view (CTP_FLAG_TOMO_FIRST_VIEW_KERNEL reproduces that). */
 int cupyFbpTomoFilter(float* fprj, const float* prj, const float* detCenter, const float* src, int nBatches,
                       size_t nu, size_t nv, size_t nview, float du, float dx, float dz, int typeFilter,
                       float cutoffX, float cutoffZ);
 /* The same with a ctp_geometry (nbatch, nu, nv, nview, du, dx, dz), a caller
    workspace (size from ctp_tomo_filter_workspace) and a stream. */
 int ctp_tomo_filter(float* fprj, const float* prj, const float* detCenter, const float* src, const ctp_geometry* g,
-                    int filter, float cutoff_x, float cutoff_z, void* workspace, size_t workspace_bytes, void* stream);
+                    int filter, float cutoff_x, float cutoff_z, unsigned flags, void* workspace,
+                    size_t workspace_bytes, void* stream);
 size_t ctp_tomo_filter_workspace(const ctp_geometry* g);
 
 /* Fan-beam Siddon pair, host pointers: siddonFan.cu:127 (cSiddonFanProjection)

@@ -346,7 +346,7 @@ def sqs_tv_update(x, bp, norm, zlink, weights, beta, eps=1e-8):
     return x - (_d(bp) + beta * s1) / (norm[idx] + beta * s2)
 
 
-def tomo_filter(p, prj, det_center, src, filter_type="hann", cutoff_x=1.0, cutoff_z=1.0):
+def tomo_filter(p, prj, det_center, src, filter_type="hann", cutoff_x=1.0, cutoff_z=1.0, first_view_kernel=False):
     """Tomosynthesis FBP filter in FP64 (fbpTomo::Filter and GetRampTomo,
     kernel/projector/cuda/fbpTomo.cu:50-384 of the reference).  Per view: the
     tilt from the source-to-detector-centre direction in the x-z plane
@@ -354,7 +354,12 @@ def tomo_filter(p, prj, det_center, src, filter_type="hann", cutoff_x=1.0, cutof
     frequency by (x window) * (z window) whose frequencies are
     fu * cos * dx * 2 and fu * sin * dz * 2, each clamped above at its cut-off
     (GetFrequency :50-68); every row of the view is convolved with it and
-    scaled by pi / nview * vdu (:311, with the transforms' 1/L)."""
+    scaled by pi / nview * vdu (:311, with the transforms' 1/L).
+
+    ``first_view_kernel`` reproduces what the reference computes: it builds
+    every view's kernel but multiplies each view's spectrum by the first one
+    (FilterByFreqMultiply1D is given pcuFilter without a view offset,
+    fbpTomo.cu:323), keeping each view's own scale."""
     prj = _d(prj)
     dc, sr = _d(det_center), _d(src)
     nb, nview, nv, nu = prj.shape
@@ -373,6 +378,11 @@ def tomo_filter(p, prj, det_center, src, filter_type="hann", cutoff_x=1.0, cutof
         ddx, ddz = dc[v, 0] - sr[v, 0], dc[v, 2] - sr[v, 2]
         r = np.sqrt(ddx * ddx + ddz * ddz)
         sin_t, cos_t = ddx / r, -ddz / r
+        scale_vdu = du * cos_t
+        if first_view_kernel:
+            ddx, ddz = dc[0, 0] - sr[0, 0], dc[0, 2] - sr[0, 2]
+            r = np.sqrt(ddx * ddx + ddz * ddz)
+            sin_t, cos_t = ddx / r, -ddz / r
         vdu = du * cos_t
         h = np.zeros(L)
         h[k == 0] = 1.0 / (4 * vdu * vdu)
@@ -390,7 +400,7 @@ def tomo_filter(p, prj, det_center, src, filter_type="hann", cutoff_x=1.0, cutof
         g = np.real(np.fft.ifft(np.fft.fft(h) * w))
         X = np.fft.rfft(prj[:, v], n=n, axis=-1)
         full = np.fft.irfft(X * np.fft.rfft(g, n=n), n=n, axis=-1)
-        out[:, v] = full[..., nu - 1: 2 * nu - 1] * (np.pi / nview * vdu)
+        out[:, v] = full[..., nu - 1: 2 * nu - 1] * (np.pi / nview * scale_vdu)
     return out
 
 
