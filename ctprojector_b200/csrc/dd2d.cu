@@ -871,25 +871,21 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     return false;
 }
 
-// S slices of the same geometry per CTA (S > 1 for stacks): the edge
-// positions, their rounding to table indices and the footprint widths are
-// the same for every slice, so they are computed once and only the table
-// lookups, shuffles and sums repeat per slice.
-template <bool FAN, int NI, int S, typename Tout>
+template <bool FAN, int NI, typename Tout>
 __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
                                                              const float4* __restrict__ ltab1, DDTab tab, Grid g,
-                                                             Det d, int nview, int vgroup, int rchunk, int nslices,
+                                                             Det d, int nview, int vgroup, int rchunk,
                                                              const float* __restrict__ deg, int unweight_par) {
-    extern __shared__ float4 s_ring[];  // [2][S][rchunk][max(nx, ny) + 1]
+    extern __shared__ float4 s_ring[];  // [2][rchunk * (max(nx, ny) + 1)]
     __shared__ __align__(8) unsigned long long s_bar[2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int v0 = blockIdx.x * vgroup;
     const int nvg = min(vgroup, nview - v0);
-    const int s0 = blockIdx.y * S;  // first slice (b * nz + iz) of this CTA
-    const int ns = min(S, nslices - s0);
+    const int slice = blockIdx.y;  // b * nz + iz, detector row iv = iz
+    const int iz = slice % g.nz, b = slice / g.nz;
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
     const int nitems = nvg * ipv;
-    const size_t ring = (size_t)S * rchunk * (max(g.nx, g.ny) + 1);
+    const size_t ring = (size_t)rchunk * (max(g.nx, g.ny) + 1);
 
     // orientations with work in this CTA: rows (o = 0) for views traced along
     // y, columns (o = 1) for views traced along x, both in the blend band
@@ -904,6 +900,8 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
     const int nc0 = act0 ? (g.ny + rchunk - 1) / rchunk : 0;
     const int nc1 = act1 ? (g.nx + rchunk - 1) / rchunk : 0;
     const int K = nc0 + nc1;
+    const float4* src0 = ltab0 + (size_t)slice * g.ny * (g.nx + 1);
+    const float4* src1 = ltab1 + (size_t)slice * g.nx * (g.ny + 1);
 
     auto issue = [&](int k) {
         const int o = k < nc0 ? 0 : 1;
@@ -912,13 +910,8 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
         const unsigned bytes = (unsigned)((size_t)nlc * (n + 1) * sizeof(float4));
         unsigned long long* bar = &s_bar[k & 1];
-        mbar_expect_tx(bar, bytes * (unsigned)ns);
-        for (int s = 0; s < ns; ++s) {
-            const float4* src = o == 0 ? ltab0 + (size_t)(s0 + s) * g.ny * (g.nx + 1)
-                                       : ltab1 + (size_t)(s0 + s) * g.nx * (g.ny + 1);
-            bulk_copy_g2s(s_ring + (k & 1) * ring + (size_t)s * rchunk * (n + 1), src + (size_t)l0 * (n + 1), bytes,
-                          bar);
-        }
+        mbar_expect_tx(bar, bytes);
+        bulk_copy_g2s(s_ring + (k & 1) * ring, (o == 0 ? src0 : src1) + (size_t)l0 * (n + 1), bytes, bar);
     };
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);
@@ -931,7 +924,7 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         if (K > 1) issue(1);
     }
 
-    float A[NI], B[NI], acc[S][NI];
+    float A[NI], B[NI], acc[NI];
     bool failed = false;
     int k = 0;
     for (; k < K; ++k) {
@@ -946,8 +939,7 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
                 // dummy edge positions keep every width non-zero
                 A[q] = (float)lane - 0.5f;
                 B[q] = 0.f;
-#pragma unroll
-                for (int s = 0; s < S; ++s) acc[s][q] = 0.f;
+                acc[q] = 0.f;
                 if (it < nitems) {
                     const int vi = it / ipv, m = it - vi * ipv;
                     const int view = v0 + vi;
@@ -967,7 +959,6 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
         const float lo_lim = -0.5f, hi_lim = (float)n - 0.5f;
-        const size_t sstride = (size_t)rchunk * (n + 1);
         for (int r = 0; r < nlc && !failed; ++r) {
             const float t = (float)(l0 + r - anchor);
             const float4* T = buf + (size_t)r * (n + 1);
@@ -976,22 +967,14 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
                 const float xr = fmaf(B[q], t, A[q]);  // edge position - 1/2
                 const float xs = clampf(xr, lo_lim, hi_lim);
                 const float tt = xs + kRoundMagic;
-                const int idx = __float_as_int(tt) - kRoundMagicBits;
-                const float fr = xs - (tt - kRoundMagic);
+                const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
+                const float hi = e.x, lo = fmaf(e.z, xs - (tt - kRoundMagic), e.y);
+                const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
+                const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
                 const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
-                const float w = xn - xr;
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    if (s < ns) {
-                        const float4 e = T[s * sstride + idx];
-                        const float hi = e.x, lo = fmaf(e.z, fr, e.y);
-                        const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
-                        const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
-                        // signed integral over [x_j, x_j+1] over the signed width of
-                        // the rounded footprint
-                        acc[s][q] += __fdividef((hin - hi) + (lon - lo), w);
-                    }
-                }
+                // signed integral over [x_j, x_j+1] over the signed width of
+                // the rounded footprint
+                acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
             }
         }
         if (c == last && !failed) {
@@ -1005,16 +988,10 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
                 const float wx = tab.wx[view];
                 const bool active = o == 0 ? wx > 0.f : wx < 1.f;
                 if (!active || lane >= 31 || kk >= d.nu) continue;
-                const float wl = tab.cL[o][(size_t)view * d.nu + kk] * (o == 0 ? wx : 1.f - wx);
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    if (s >= ns) continue;
-                    const int slice = s0 + s, iz = slice % g.nz, b = slice / g.nz;
-                    float v = acc[s][q] * wl;
-                    Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
-                    if (o == 1 && wx > 0.f) v += rdf(dst);  // the row pass of this view wrote first
-                    stf(dst, v);
-                }
+                float v = acc[q] * tab.cL[o][(size_t)view * d.nu + kk] * (o == 0 ? wx : 1.f - wx);
+                Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
+                if (o == 1 && wx > 0.f) v += rdf(dst);  // the row pass of this view wrote first
+                stf(dst, v);
             }
         }
         // every warp is done with buffer k & 1 before it is refilled
@@ -1040,12 +1017,8 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
             if (lane >= 31 || kk >= d.nu) continue;
             float sn, cs;
             sincosf(deg[view], &sn, &cs);
-            const float wr = ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn);
-            for (int s = 0; s < ns; ++s) {
-                const int slice = s0 + s, iz = slice % g.nz, b = slice / g.nz;
-                Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
-                stf(dst, rdf(dst) / wr);
-            }
+            Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
+            stf(dst, rdf(dst) / (ref_y_main(deg[view]) ? g.dy / fabsf(cs) : g.dx / fabsf(sn)));
         }
     }
 }
@@ -1672,12 +1645,10 @@ bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
 }
 
 // View group and edge groups per warp (one of the compiled counts) of the
-// streamed forward projector with S slices per CTA: the most views per CTA
-// whose edge groups fill the 8 warps with the least waste.
-bool fp_stream_shape(const ctp_geometry& g, int S, int& vgroup, int& ni) {
-    static const int kNi1[4] = {4, 8, 12, 16};
-    static const int kNi2[4] = {4, 6, 8, 10};
-    const int* set = S == 1 ? kNi1 : kNi2;
+// streamed forward projector: the most views per CTA whose edge groups fill
+// the 8 warps with the least waste.
+bool fp_stream_shape(const ctp_geometry& g, int& vgroup, int& ni) {
+    static const int set[4] = {4, 8, 12, 16};
     const int ipv = (int)((g.nu + 30) / 31);
     vgroup = 0;
     ni = 0;
@@ -1725,29 +1696,28 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         line_tables_kernel<Tin><<<(unsigned)std::min<long long>((cols + 7) / 8, 148 * 16), 256, 0, s>>>(
             lt1, imgT, cols, (int)g.ny);
         if ((rc = check_launch("line_tables_kernel"))) return rc;
-        // one slice per CTA: sharing the edge work across two slices halves the
-        // lines per table chunk, and the warps then wait on the copies instead
+        // one slice per CTA (sharing the edge work across two slices halves the
+        // lines per table chunk, and the warps then wait on the copies instead)
         const int nslices = (int)(g.nbatch * g.nz);
-        const int S = 1;
         int sv = 0, ni = 0;
-        fp_stream_shape(g, S, sv, ni);
-        const int rc_s = std::max(1, rchunk / S);
-        size_t shm = 2 * (size_t)S * rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
-        dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)((nslices + S - 1) / S));
+        fp_stream_shape(g, sv, ni);
+        const int rc_s = rchunk;
+        size_t shm = 2 * (size_t)rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+        dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)nslices);
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
             cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), lt0, lt1, tab, make_grid(g), make_det(g), (int)g.nview, sv,
-                                      rc_s, nslices, deg, unweight);
+                                      rc_s, deg, unweight);
         };
         const bool fan = geom == 0;
-#define CTP_FP_STREAM(NI_, S_)                                                   \
-    if (fan) launch(dd2d_fp_stream_kernel<true, NI_, S_, Tout>);                 \
-    else launch(dd2d_fp_stream_kernel<false, NI_, S_, Tout>)
-        if (ni == 4) { CTP_FP_STREAM(4, 1); }
-        else if (ni == 8) { CTP_FP_STREAM(8, 1); }
-        else if (ni == 12) { CTP_FP_STREAM(12, 1); }
-        else { CTP_FP_STREAM(16, 1); }
+#define CTP_FP_STREAM(NI_)                                                       \
+    if (fan) launch(dd2d_fp_stream_kernel<true, NI_, Tout>);                     \
+    else launch(dd2d_fp_stream_kernel<false, NI_, Tout>)
+        if (ni == 4) { CTP_FP_STREAM(4); }
+        else if (ni == 8) { CTP_FP_STREAM(8); }
+        else if (ni == 12) { CTP_FP_STREAM(12); }
+        else { CTP_FP_STREAM(16); }
 #undef CTP_FP_STREAM
         return check_launch("dd2d_fp_stream_kernel");
     }
