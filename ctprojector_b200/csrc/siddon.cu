@@ -123,15 +123,16 @@ __device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
     double aprev = R.aprev;
     while (true) {
         // the axis is chosen with selects (lanes of a warp cross different
-        // axes, so branches would run all three paths); the two axes not
-        // chosen add zero, which leaves them unchanged
+        // axes, so branches would run all three paths) and its crossing is
+        // advanced with one FP64 add, written back to that axis only
         const bool kx = a0 < a1 && a0 < a2;
         const bool ky = !kx && a1 < a2;
         const bool kz = !kx && !ky;
         const double anow = kx ? a0 : (ky ? a1 : a2);
-        a0 += kx ? d0 : 0.0;
-        a1 += ky ? d1 : 0.0;
-        a2 += kz ? d2 : 0.0;
+        const double anext = anow + (kx ? d0 : (ky ? d1 : d2));
+        a0 = kx ? anext : a0;
+        a1 = ky ? anext : a1;
+        a2 = kz ? anext : a2;
         g0 += kx ? s0 : 0;
         g1 += ky ? s1 : 0;
         g2 += kz ? s2 : 0;
