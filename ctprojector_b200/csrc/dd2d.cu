@@ -649,13 +649,7 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 // Midpoint table of one line of n cells, built by one warp: n+1 entries
 // {hi, lo, r, 0} with hi + lo = integral over cells [0, i) plus r_i / 2 in
 // double-float form and r_i the cell value (0 past the end).
-// Streamed line tables store entry i at slot i + i/8: the entries that one
-// quarter warp reads (8 consecutive cell edges, up to ~11 entries apart) then
-// fall on different banks.
-__host__ __device__ __forceinline__ int padded_slot(int i) { return i + (i >> 3); }
-__host__ __device__ __forceinline__ int padded_len(int n) { return padded_slot(n) + 1; }
-
-template <typename Tin, bool PAD = false>
+template <typename Tin>
 __device__ __forceinline__ void stage_line(float4* __restrict__ T, const Tin* __restrict__ row, int n, int lane) {
     const int E = (n + 1 + 31) / 32;
     const int k0 = lane * E;
@@ -695,7 +689,7 @@ __device__ __forceinline__ void stage_line(float4* __restrict__ T, const Tin* __
         int k = k0 + q;
         if (k <= n) {
             float r = k < n ? ldf(row + k) : 0.f;
-            T[PAD ? padded_slot(k) : k] = make_float4(bhi, fmaf(0.5f, r, blo), r, 0.f);  // midpoint table
+            T[k] = make_float4(bhi, fmaf(0.5f, r, blo), r, 0.f);  // midpoint table
             float e;
             two_sum(bhi, r, bhi, e);
             blo += e;
@@ -718,7 +712,7 @@ __global__ void __launch_bounds__(256) line_tables_kernel(float4* __restrict__ o
     const int lane = threadIdx.x & 31;
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long l = w0; l < nlines; l += nw) stage_line<Tin, true>(out + l * padded_len(n), src + l * n, n, lane);
+    for (long long l = w0; l < nlines; l += nw) stage_line(out + l * (n + 1), src + l * n, n, lane);
 }
 
 // NI = edge groups per warp (compile time, so the group loop is straight-line
@@ -891,7 +885,7 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
     const int iz = slice % g.nz, b = slice / g.nz;
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
     const int nitems = nvg * ipv;
-    const size_t ring = (size_t)rchunk * padded_len(max(g.nx, g.ny));
+    const size_t ring = (size_t)rchunk * (max(g.nx, g.ny) + 1);
 
     // orientations with work in this CTA: rows (o = 0) for views traced along
     // y, columns (o = 1) for views traced along x, both in the blend band
@@ -906,18 +900,18 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
     const int nc0 = act0 ? (g.ny + rchunk - 1) / rchunk : 0;
     const int nc1 = act1 ? (g.nx + rchunk - 1) / rchunk : 0;
     const int K = nc0 + nc1;
-    const float4* src0 = ltab0 + (size_t)slice * g.ny * padded_len(g.nx);
-    const float4* src1 = ltab1 + (size_t)slice * g.nx * padded_len(g.ny);
+    const float4* src0 = ltab0 + (size_t)slice * g.ny * (g.nx + 1);
+    const float4* src1 = ltab1 + (size_t)slice * g.nx * (g.ny + 1);
 
     auto issue = [&](int k) {
         const int o = k < nc0 ? 0 : 1;
         const int c = o == 0 ? k : k - nc0;
         const int n = o == 0 ? g.nx : g.ny, nl = o == 0 ? g.ny : g.nx;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
-        const unsigned bytes = (unsigned)((size_t)nlc * padded_len(n) * sizeof(float4));
+        const unsigned bytes = (unsigned)((size_t)nlc * (n + 1) * sizeof(float4));
         unsigned long long* bar = &s_bar[k & 1];
         mbar_expect_tx(bar, bytes);
-        bulk_copy_g2s(s_ring + (k & 1) * ring, (o == 0 ? src0 : src1) + (size_t)l0 * padded_len(n), bytes, bar);
+        bulk_copy_g2s(s_ring + (k & 1) * ring, (o == 0 ? src0 : src1) + (size_t)l0 * (n + 1), bytes, bar);
     };
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);
@@ -967,13 +961,13 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         const float lo_lim = -0.5f, hi_lim = (float)n - 0.5f;
         for (int r = 0; r < nlc && !failed; ++r) {
             const float t = (float)(l0 + r - anchor);
-            const float4* T = buf + (size_t)r * padded_len(n);
+            const float4* T = buf + (size_t)r * (n + 1);
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
                 const float xr = fmaf(B[q], t, A[q]);  // edge position - 1/2
                 const float xs = clampf(xr, lo_lim, hi_lim);
                 const float tt = xs + kRoundMagic;
-                const float4 e = T[padded_slot(__float_as_int(tt) - kRoundMagicBits)];
+                const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
                 const float hi = e.x, lo = fmaf(e.z, xs - (tt - kRoundMagic), e.y);
                 const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
                 const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
@@ -1591,8 +1585,7 @@ size_t fp_workspace_min(const ctp_geometry& g) {
 
 size_t fp_line_tables_bytes(const ctp_geometry& g) {
     size_t slices = g.nbatch * g.nz;
-    return align_up(slices * (g.ny * (size_t)padded_len((int)g.nx) + g.nx * (size_t)padded_len((int)g.ny)) *
-                    sizeof(float4));
+    return align_up(slices * (g.ny * (g.nx + 1) + g.nx * (g.ny + 1)) * sizeof(float4));
 }
 
 constexpr size_t kFpStreamMinSlices = 8;
@@ -1600,9 +1593,9 @@ constexpr size_t kFpStreamMinSlices = 8;
 // Lines per chunk of the streamed path's two-buffer ring, or 0 if one line
 // per buffer does not fit.
 int fp_stream_chunk(const ctp_geometry& g) {
-    size_t line = (size_t)padded_len((int)std::max(g.nx, g.ny)) * sizeof(float4);
+    size_t line = (std::max(g.nx, g.ny) + 1) * sizeof(float4);
     if (2 * line > 200 * 1024) return 0;
-    int r = (int)((75 * 1024) / (2 * line));  // three CTAs per SM at 512^2
+    int r = (int)((66 * 1024) / (2 * line));
     return std::max(1, std::min(r, 8));
 }
 
@@ -1696,7 +1689,7 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
         // streamed path: line tables of rows (from the image) and columns (from its transpose)
         float4* lt0 = reinterpret_cast<float4*>(ws + fp_workspace_min(g));
-        float4* lt1 = lt0 + g.nbatch * g.nz * g.ny * (size_t)padded_len((int)g.nx);
+        float4* lt1 = lt0 + g.nbatch * g.nz * g.ny * (g.nx + 1);
         long long rows = (long long)(g.nbatch * g.nz * g.ny), cols = (long long)(g.nbatch * g.nz * g.nx);
         line_tables_kernel<Tin><<<(unsigned)std::min<long long>((rows + 7) / 8, 148 * 16), 256, 0, s>>>(
             lt0, cptr<Tin>(img), rows, (int)g.nx);
@@ -1709,7 +1702,7 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         int sv = 0, ni = 0;
         fp_stream_shape(g, sv, ni);
         const int rc_s = rchunk;
-        size_t shm = 2 * (size_t)rc_s * padded_len((int)std::max(g.nx, g.ny)) * sizeof(float4);
+        size_t shm = 2 * (size_t)rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)nslices);
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);

@@ -122,22 +122,28 @@ __device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
     long long idx = g2 * nxy + (long long)g1 * g.nx + g0;
     double aprev = R.aprev;
     while (true) {
-        // the axis is chosen with selects (lanes of a warp cross different
-        // axes, so branches would run all three paths) and its crossing is
-        // advanced with one FP64 add, written back to that axis only
-        const bool kx = a0 < a1 && a0 < a2;
-        const bool ky = !kx && a1 < a2;
-        const bool kz = !kx && !ky;
-        const double anow = kx ? a0 : (ky ? a1 : a2);
-        const double anext = anow + (kx ? d0 : (ky ? d1 : d2));
-        a0 = kx ? anext : a0;
-        a1 = ky ? anext : a1;
-        a2 = kz ? anext : a2;
-        g0 += kx ? s0 : 0;
-        g1 += ky ? s1 : 0;
-        g2 += kz ? s2 : 0;
-        const bool out = kx ? (g0 < 0 || g0 >= g.nx) : (ky ? (g1 < 0 || g1 >= g.ny) : (g2 < 0 || g2 >= g.nz));
-        const long long mv = kx ? (long long)s0 : (ky ? m1 : m2);
+        double anow;
+        bool out;
+        long long mv;
+        if (a0 < a1 && a0 < a2) {
+            anow = a0;
+            a0 += d0;
+            g0 += s0;
+            out = g0 < 0 || g0 >= g.nx;
+            mv = s0;
+        } else if (a1 < a2) {
+            anow = a1;
+            a1 += d1;
+            g1 += s1;
+            out = g1 < 0 || g1 >= g.ny;
+            mv = m1;
+        } else {
+            anow = a2;
+            a2 += d2;
+            g2 += s2;
+            out = g2 < 0 || g2 >= g.nz;
+            mv = m2;
+        }
         emit(idx, (float)(anow - aprev));
         aprev = anow;
         if (out) break;
