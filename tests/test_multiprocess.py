@@ -73,3 +73,63 @@ def test_max_over_ranks_without_process_group():
     import bench
 
     assert bench.max_over_ranks(3.5, torch.device("cpu")) == 3.5
+
+
+def _view_split_worker(rank, world, port, q):
+    import sys
+
+    import numpy as np
+    import torch.distributed as dist
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    from ctprojector_b200.multigpu import gather_slabs, view_shares, view_split_bp
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, init_method=f"tcp://127.0.0.1:{port}",
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        nview, m, shape = 7, 6, (5, 3, 4)
+        rng = np.random.default_rng(0)  # the same operator and data on every rank
+        mats = rng.standard_normal((nview, int(np.prod(shape)), m))
+        prj = rng.standard_normal((nview, m))
+
+        def bp_views(views):
+            acc = np.zeros(int(np.prod(shape)))
+            for v in views:
+                acc += mats[v] @ prj[v]
+            return torch.tensor(acc.reshape(shape), dtype=torch.float64)
+
+        slab, (z0, z1) = view_split_bp(bp_views, nview)
+        full = gather_slabs(slab, shape[0])
+        ref = bp_views(range(nview))
+        q.put((rank, view_shares(nview, rank, world), (z0, z1), float((slab - ref[z0:z1]).abs().max()),
+               float((full - ref).abs().max())))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_view_split_back_projection_two_ranks():
+    """Each rank back projects its share of the views; the reduce-scatter
+    leaves it the sum over all views for its z slab, and the all-gather
+    rebuilds the whole volume (5 slices over 2 ranks: uneven slabs)."""
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_view_split_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    try:
+        for _ in range(world):
+            rank, views, zr, err_slab, err_full = q.get(timeout=120)
+            out[rank] = (views, zr, err_slab, err_full)
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    assert sorted(out[0][0] + out[1][0]) == list(range(7)) and not set(out[0][0]) & set(out[1][0])
+    assert out[0][1] == (0, 3) and out[1][1] == (3, 5)
+    for r in range(world):
+        assert out[r][2] <= 1e-12 and out[r][3] <= 1e-12
