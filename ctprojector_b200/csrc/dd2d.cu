@@ -126,8 +126,16 @@ __global__ void dd_table_kernel(DDTabW t, const float* __restrict__ deg, int nvi
     double th = (double)deg[view];
     double sx, sy, ex, ey;
     edge_ray(geom, th, j, g, d, dsd, dso, sx, sy, ex, ey);
-    double by = (ex - sx) / (ey - sy), ay = sx + by * (ym + 0.5 - sy);
-    double bx = (ey - sy) / (ex - sx), ax = sy + bx * (xm + 0.5 - sx);
+    double by = (ex - sx) / (ey - sy), bx = (ey - sy) / (ex - sx);
+    if (geom != 0) {
+        // parallel rays: one slope per view, the same float for every edge
+        // (the parallel forward projector relies on equal footprint widths)
+        double s, c;
+        sincos(th, &s, &c);
+        by = -(s * g.dy) / (c * g.dx);
+        bx = -(c * g.dx) / (s * g.dy);
+    }
+    double ay = sx + by * (ym + 0.5 - sy), ax = sy + bx * (xm + 0.5 - sx);
     size_t ie = (size_t)view * (d.nu + 1) + j;
     t.eA[0][ie] = (float)ay;
     t.eB[0][ie] = (float)by;
@@ -612,16 +620,18 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
 // one onto detector rows).
 //
 // A CTA owns a group of views of one slice and streams the image through
-// shared memory kFRows lines at a time (rows of the image for the views traced
+// shared memory a few lines at a time (rows of the image for the views traced
 // along y, rows of the transposed image for those traced along x).  Each staged
-// line is stored as its running integral F in double-float form (hi, lo) plus
-// the pixel value r, so the integral of the line over [a, b] is F(b) - F(a)
-// with no cancellation.  Detector cells share their edges, so each lane of a
-// warp evaluates F at one edge (x = A + B t from the FP64 edge table) and takes
-// its neighbour's value with a shuffle: 31 rays per warp, one table read per
-// ray and line.  The normalisation by the footprint width, the ray-length
-// factor and the blend weight are those of DDFPTracing
-// (distanceDriven2DBoxInt.cu:21-106).
+// line is stored as its running integral F (double-float (hi, lo) for fan
+// beams, FP64 for parallel beams) plus the pixel value r, so the integral of
+// the line over [a, b] is F(b) - F(a) with no cancellation.  Detector cells
+// share their edges, so each lane of a warp evaluates F at one edge (x = A + B t
+// from the FP64 edge table): 31 rays per warp, one table read per ray and
+// line.  Fan beams take the neighbour edge's value with a shuffle and divide
+// by the footprint width on every line; parallel beams, whose width is the
+// same on every line, sum F per edge and difference once (fp_line).  The
+// normalisation by the footprint width, the ray-length factor and the blend
+// weight are those of DDFPTracing (distanceDriven2DBoxInt.cu:21-106).
 constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
 
 // Running integral at x' + 1/2 from a midpoint table: entry i holds
@@ -645,6 +655,81 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     float bb = s - a;
     e = (a - (s - bb)) + (b - bb);
 }
+
+// One image line's contribution to a thread's NI edge groups (edge position
+// minus 1/2 on line t: x = A + B t, clamped to [lo_lim, hi_lim]; T the
+// line's midpoint table).
+//   FAN: acc += (F(x_j+1) - F(x_j)) / (x_j+1 - x_j), the neighbour edge taken
+//        from the next lane (the footprint width changes from line to line);
+//        double-float table entries {hi, lo, r, 0}.
+//   parallel: every edge of a view has the same slope, so the width is the
+//        same on every line; each lane sums F at its own edge over the lines
+//        and the cell difference is taken once, after the last line
+//        (fp_cell_sum): no shuffle or divide per line.  The table entries
+//        hold C + r/2 as an FP64 value {lo word, hi word, r, 0}, summed in
+//        FP64 (accd); the small r * frac parts go to an FP32 sum (alo) that
+//        is folded into accd every 16 lines.  Positions are measured from
+//        the middle of the line (T points at the middle entry) so that their
+//        FP32 rounding is half as large.
+template <bool FAN, int NI>
+__device__ __forceinline__ void fp_line(const float4* __restrict__ T, float t, float lo_lim, float hi_lim,
+                                        const float (&A)[NI], const float (&B)[NI], float (&acc)[NI],
+                                        double (&accd)[NI], float (&alo)[NI]) {
+#pragma unroll
+    for (int q = 0; q < NI; ++q) {
+        const float xr = fmaf(B[q], t, A[q]);
+        const float xs = clampf(xr, lo_lim, hi_lim);
+        const float tt = xs + kRoundMagic;
+        const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
+        const float frac = xs - (tt - kRoundMagic);
+        if constexpr (FAN) {
+            const float hi = e.x, lo = fmaf(e.z, frac, e.y);
+            const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
+            const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
+            const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
+            // signed integral over [x_j, x_j+1] over the signed width of the
+            // rounded footprint
+            acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
+        } else {
+            accd[q] += __hiloint2double(__float_as_int(e.y), __float_as_int(e.x));
+            alo[q] = fmaf(e.z, frac, alo[q]);
+        }
+    }
+}
+
+// Parallel sums: fold the FP32 part (at most 16 lines of r * frac) into the
+// FP64 sum.
+template <bool FAN, int NI>
+__device__ __forceinline__ void fp_renorm(double (&accd)[NI], float (&alo)[NI]) {
+    if constexpr (!FAN) {
+#pragma unroll
+        for (int q = 0; q < NI; ++q) {
+            accd[q] += (double)alo[q];
+            alo[q] = 0.f;
+        }
+    }
+}
+
+// Sum over lines of the cell integral over the footprint width, for the cell
+// between this lane's edge and the next lane's (all lanes call it; parallel
+// sums renormalised first).
+template <bool FAN>
+__device__ __forceinline__ float fp_cell_sum(float acc, double accd, float A) {
+    if constexpr (FAN) {
+        return acc;
+    } else {
+        const double dn = __shfl_down_sync(0xffffffffu, accd, 1);
+        const float An = __shfl_down_sync(0xffffffffu, A, 1);
+        return __fdividef((float)(dn - accd), An - A);
+    }
+}
+
+// Offset of the position origin from the start of a line of n cells: the
+// middle entry for the parallel sums, the start for fan beams.  Even, so that
+// the clamped ends -h - 1/2 and n - h - 1/2 round (half to even) onto table
+// entries 0 and n or n - 1.
+template <bool FAN>
+__device__ __forceinline__ int fp_origin(int n) { return FAN ? 0 : (n >> 1) & ~1; }
 
 // Midpoint table of one line of n cells, built by one warp: n+1 entries
 // {hi, lo, r, 0} with hi + lo = integral over cells [0, i) plus r_i / 2 in
@@ -697,29 +782,72 @@ __device__ __forceinline__ void stage_line(float4* __restrict__ T, const Tin* __
     }
 }
 
-// Stage lines (length n, stride n between lines) into consecutive tables.
+// FP64 midpoint table of one line (the parallel-beam sums): n+1 entries
+// {C_i + r_i/2 as the low and high words of a double, r_i, 0} with C_i the
+// integral over cells [0, i) and r_i the cell value (0 past the end).
 template <typename Tin>
+__device__ __forceinline__ void stage_line_fp64(float4* __restrict__ T, const Tin* __restrict__ row, int n,
+                                                int lane) {
+    const int E = (n + 1 + 31) / 32;
+    const int k0 = lane * E;
+    double tot = 0.0;
+    for (int q = 0; q < E; ++q) {
+        const int k = k0 + q;
+        if (k < n) tot += (double)ldf(row + k);
+    }
+    double inc = tot;  // inclusive scan of the lane totals
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    double c = inc - tot;
+    for (int q = 0; q < E; ++q) {
+        const int k = k0 + q;
+        if (k <= n) {
+            const float r = k < n ? ldf(row + k) : 0.f;
+            const double m = c + 0.5 * (double)r;
+            T[k] = make_float4(__int_as_float(__double2loint(m)), __int_as_float(__double2hiint(m)), r, 0.f);
+            c += (double)r;
+        }
+    }
+}
+
+// Stage lines (length n, stride n between lines) into consecutive tables.
+template <typename Tin, bool FP64>
 __device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ src, int nlines, int n, int warp,
                             int lane, int nwarps) {
-    for (int l = warp; l < nlines; l += nwarps) stage_line(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
+    for (int l = warp; l < nlines; l += nwarps) {
+        if constexpr (FP64) stage_line_fp64(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
+        else stage_line(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
+    }
 }
 
 // The tables of every line of a stack of slices (one warp per line), for the
-// forward projector that streams them into shared memory.
-template <typename Tin>
+// forward projector that streams them into shared memory; FP64 entries for
+// parallel beams.
+template <typename Tin, bool FP64>
 __global__ void __launch_bounds__(256) line_tables_kernel(float4* __restrict__ out, const Tin* __restrict__ src,
                                                           long long nlines, int n) {
     const int lane = threadIdx.x & 31;
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long l = w0; l < nlines; l += nw) stage_line(out + l * (n + 1), src + l * n, n, lane);
+    for (long long l = w0; l < nlines; l += nw) {
+        if constexpr (FP64) stage_line_fp64(out + l * (n + 1), src + l * n, n, lane);
+        else stage_line(out + l * (n + 1), src + l * n, n, lane);
+    }
 }
 
 // NI = edge groups per warp (compile time, so the group loop is straight-line
 // code with independent dependency chains); groups beyond the CTA's views are
 // harmless dummies whose results are dropped.
+// Parallel beams hold four registers per edge group (position, slope and the
+// double-float sum): above 4 groups per warp they run two CTAs per SM.
+template <bool FAN, int NI>
+constexpr int fp_fast_min_blocks() { return FAN || NI <= 4 ? 3 : 2; }
+
 template <bool FAN, int NI, typename Tin, typename Tout>
-__global__ void __launch_bounds__(256, 3) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
+__global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
                                                            const Tin* __restrict__ imgT, DDTab tab, Grid g, Det d,
                                                            int nview, int vgroup, int nrows_chunk,
                                                            const float* __restrict__ deg, int unweight_par) {
@@ -737,15 +865,20 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_fast_kernel(Tout* __restrict__
         const int nl = o == 0 ? g.ny : g.nx;  // lines
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const Tin* src = (o == 0 ? img : imgT) + (size_t)slice * g.nx * g.ny;
-        float A[NI], B[NI], acc[NI];
+        float A[NI], B[NI], acc[NI], alo[NI];
+        double accd[NI];
         bool any = false;
+        const int h = fp_origin<FAN>(n);
+        const float shift = 0.5f + (float)h;  // midpoint tables, origin at entry h
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
             const int it = warp + 8 * q;
             // dummy edge positions keep every width non-zero
-            A[q] = (float)lane - 0.5f;
+            A[q] = (float)lane - shift;
             B[q] = 0.f;
             acc[q] = 0.f;
+            accd[q] = 0.0;
+            alo[q] = 0.f;
             if (it < nitems) {
                 const int vi = it / ipv, m = it - vi * ipv;
                 const int view = v0 + vi;
@@ -754,7 +887,7 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_fast_kernel(Tout* __restrict__
                 const int j = 31 * m + lane;
                 if (active && j <= d.nu) {
                     const size_t ie = (size_t)view * (d.nu + 1) + j;
-                    A[q] = tab.eA[o][ie] - 0.5f;  // shifted for the midpoint tables
+                    A[q] = tab.eA[o][ie] - shift;
                     B[q] = tab.eB[o][ie];
                     any = true;
                 }
@@ -762,42 +895,31 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_fast_kernel(Tout* __restrict__
         }
         // every warp takes part in staging whether or not it has work
         if (!__syncthreads_or(any)) continue;
-        const float lo_lim = -0.5f, hi_lim = (float)n - 0.5f;
-        for (int l0 = 0; l0 < nl; l0 += nrows_chunk) {
+        const float lo_lim = -shift, hi_lim = (float)n - shift;
+        const int renorm = max(1, 16 / nrows_chunk);  // chunks between renormalisations
+        for (int l0 = 0, c = 0; l0 < nl; l0 += nrows_chunk, ++c) {
             const int nlc = min(nrows_chunk, nl - l0);
             __syncthreads();
-            stage_lines(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
+            stage_lines<Tin, !FAN>(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
             __syncthreads();
-            for (int r = 0; r < nlc; ++r) {
-                const float t = (float)(l0 + r - anchor);
-                const float4* T = s_lines + (size_t)r * (n + 1);
-#pragma unroll
-                for (int q = 0; q < NI; ++q) {
-                    const float xr = fmaf(B[q], t, A[q]);  // edge position - 1/2
-                    const float xs = clampf(xr, lo_lim, hi_lim);
-                    const float tt = xs + kRoundMagic;
-                    const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
-                    const float hi = e.x, lo = fmaf(e.z, xs - (tt - kRoundMagic), e.y);
-                    const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
-                    const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
-                    const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
-                    // signed integral over [x_j, x_j+1] over the signed width of
-                    // the rounded footprint
-                    acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
-                }
-            }
+            for (int r = 0; r < nlc; ++r)
+                fp_line<FAN, NI>(s_lines + (size_t)r * (n + 1) + h, (float)(l0 + r - anchor), lo_lim, hi_lim, A, B,
+                                 acc, accd, alo);
+            if ((c + 1) % renorm == 0) fp_renorm<FAN, NI>(accd, alo);
         }
+        fp_renorm<FAN, NI>(accd, alo);
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
             const int it = warp + 8 * q;
             if (it >= nitems) continue;
+            const float sum = fp_cell_sum<FAN>(acc[q], accd[q], A[q]);
             const int vi = it / ipv, m = it - vi * ipv;
             const int view = v0 + vi;
             const int k = 31 * m + lane;
             const float wx = tab.wx[view];
             const bool active = o == 0 ? wx > 0.f : wx < 1.f;
             if (!active || lane >= 31 || k >= d.nu) continue;
-            float v = acc[q] * tab.cL[o][(size_t)view * d.nu + k] * (o == 0 ? wx : 1.f - wx);
+            float v = sum * tab.cL[o][(size_t)view * d.nu + k] * (o == 0 ? wx : 1.f - wx);
             Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + k;
             if (o == 1 && wx > 0.f) v += rdf(dst);  // the row sweep of this view wrote first
             stf(dst, v);
@@ -871,8 +993,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     return false;
 }
 
+// Parallel beams above 8 edge groups per warp (four registers per group) run
+// two CTAs per SM.
+template <bool FAN, int NI>
+constexpr int fp_stream_min_blocks() { return FAN || NI <= 8 ? 3 : 2; }
+
 template <bool FAN, int NI, typename Tout>
-__global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
+__global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
                                                              const float4* __restrict__ ltab1, DDTab tab, Grid g,
                                                              Det d, int nview, int vgroup, int rchunk,
                                                              const float* __restrict__ deg, int unweight_par) {
@@ -924,7 +1051,10 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         if (K > 1) issue(1);
     }
 
-    float A[NI], B[NI], acc[NI];
+    // per edge group: edge position and slope, and the sums of fp_line
+    float A[NI], B[NI], acc[NI], alo[NI];
+    double accd[NI];
+    const int renorm = max(1, 16 / rchunk);  // chunks between renormalisations of (acc, alo)
     bool failed = false;
     int k = 0;
     for (; k < K; ++k) {
@@ -932,14 +1062,18 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
         const int c = o == 0 ? k : k - nc0;
         const int n = o == 0 ? g.nx : g.ny, nl = o == 0 ? g.ny : g.nx;
         const int last = (o == 0 ? nc0 : nc1) - 1;
+        const int h = fp_origin<FAN>(n);
+        const float shift = 0.5f + (float)h;  // midpoint tables, origin at entry h
         if (c == 0) {
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
                 const int it = warp + 8 * q;
                 // dummy edge positions keep every width non-zero
-                A[q] = (float)lane - 0.5f;
+                A[q] = (float)lane - shift;
                 B[q] = 0.f;
                 acc[q] = 0.f;
+                accd[q] = 0.0;
+                alo[q] = 0.f;
                 if (it < nitems) {
                     const int vi = it / ipv, m = it - vi * ipv;
                     const int view = v0 + vi;
@@ -948,47 +1082,35 @@ __global__ void __launch_bounds__(256, 3) dd2d_fp_stream_kernel(Tout* __restrict
                     const int j = 31 * m + lane;
                     if (active && j <= d.nu) {
                         const size_t ie = (size_t)view * (d.nu + 1) + j;
-                        A[q] = tab.eA[o][ie] - 0.5f;  // shifted for the midpoint tables
+                        A[q] = tab.eA[o][ie] - shift;
                         B[q] = tab.eB[o][ie];
                     }
                 }
             }
         }
         if (!mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1)) failed = true;
+        failed = __any_sync(0xffffffffu, failed);  // the line loop shuffles: whole warps stop together
         const float4* buf = s_ring + (k & 1) * ring;
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
-        const float lo_lim = -0.5f, hi_lim = (float)n - 0.5f;
-        for (int r = 0; r < nlc && !failed; ++r) {
-            const float t = (float)(l0 + r - anchor);
-            const float4* T = buf + (size_t)r * (n + 1);
-#pragma unroll
-            for (int q = 0; q < NI; ++q) {
-                const float xr = fmaf(B[q], t, A[q]);  // edge position - 1/2
-                const float xs = clampf(xr, lo_lim, hi_lim);
-                const float tt = xs + kRoundMagic;
-                const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
-                const float hi = e.x, lo = fmaf(e.z, xs - (tt - kRoundMagic), e.y);
-                const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
-                const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
-                const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
-                // signed integral over [x_j, x_j+1] over the signed width of
-                // the rounded footprint
-                acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
-            }
-        }
+        const float lo_lim = -shift, hi_lim = (float)n - shift;
+        for (int r = 0; r < nlc && !failed; ++r)
+            fp_line<FAN, NI>(buf + (size_t)r * (n + 1) + h, (float)(l0 + r - anchor), lo_lim, hi_lim, A, B, acc, accd,
+                             alo);
+        if ((c + 1) % renorm == 0 || c == last) fp_renorm<FAN, NI>(accd, alo);
         if (c == last && !failed) {
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
                 const int it = warp + 8 * q;
                 if (it >= nitems) continue;
+                const float sum = fp_cell_sum<FAN>(acc[q], accd[q], A[q]);
                 const int vi = it / ipv, m = it - vi * ipv;
                 const int view = v0 + vi;
                 const int kk = 31 * m + lane;
                 const float wx = tab.wx[view];
                 const bool active = o == 0 ? wx > 0.f : wx < 1.f;
                 if (!active || lane >= 31 || kk >= d.nu) continue;
-                float v = acc[q] * tab.cL[o][(size_t)view * d.nu + kk] * (o == 0 ? wx : 1.f - wx);
+                float v = sum * tab.cL[o][(size_t)view * d.nu + kk] * (o == 0 ? wx : 1.f - wx);
                 Tout* dst = prj + (((size_t)b * nview + view) * d.nv + iz) * d.nu + kk;
                 if (o == 1 && wx > 0.f) v += rdf(dst);  // the row pass of this view wrote first
                 stf(dst, v);
@@ -1588,8 +1710,6 @@ size_t fp_line_tables_bytes(const ctp_geometry& g) {
     return align_up(slices * (g.ny * (g.nx + 1) + g.nx * (g.ny + 1)) * sizeof(float4));
 }
 
-constexpr size_t kFpStreamMinSlices = 8;
-
 // Lines per chunk of the streamed path's two-buffer ring, or 0 if one line
 // per buffer does not fit.
 int fp_stream_chunk(const ctp_geometry& g) {
@@ -1683,18 +1803,23 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
     int vgroup = 0, nrows = 0;
     const int rchunk = fp_stream_chunk(g);
-    // the streamed path pays off on stacks (the table pass is shared by every
-    // view group of a slice); a few slices run the staged kernel
-    if (fp_fast_ok(g, vgroup, nrows) && rchunk > 0 && g.nbatch * g.nz >= kFpStreamMinSlices &&
-        ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
+    // the streamed path is the faster one from a single slice up (the tables
+    // are built once per slice instead of once per view group); a workspace
+    // without room for the line tables runs the staged kernel
+    if (fp_fast_ok(g, vgroup, nrows) && rchunk > 0 && ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
         // streamed path: line tables of rows (from the image) and columns (from its transpose)
         float4* lt0 = reinterpret_cast<float4*>(ws + fp_workspace_min(g));
         float4* lt1 = lt0 + g.nbatch * g.nz * g.ny * (g.nx + 1);
         long long rows = (long long)(g.nbatch * g.nz * g.ny), cols = (long long)(g.nbatch * g.nz * g.nx);
-        line_tables_kernel<Tin><<<(unsigned)std::min<long long>((rows + 7) / 8, 148 * 16), 256, 0, s>>>(
-            lt0, cptr<Tin>(img), rows, (int)g.nx);
-        line_tables_kernel<Tin><<<(unsigned)std::min<long long>((cols + 7) / 8, 148 * 16), 256, 0, s>>>(
-            lt1, imgT, cols, (int)g.ny);
+        const unsigned rgrid = (unsigned)std::min<long long>((rows + 7) / 8, 148 * 16);
+        const unsigned cgrid = (unsigned)std::min<long long>((cols + 7) / 8, 148 * 16);
+        if (geom == 0) {
+            line_tables_kernel<Tin, false><<<rgrid, 256, 0, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
+            line_tables_kernel<Tin, false><<<cgrid, 256, 0, s>>>(lt1, imgT, cols, (int)g.ny);
+        } else {
+            line_tables_kernel<Tin, true><<<rgrid, 256, 0, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
+            line_tables_kernel<Tin, true><<<cgrid, 256, 0, s>>>(lt1, imgT, cols, (int)g.ny);
+        }
         if ((rc = check_launch("line_tables_kernel"))) return rc;
         // one slice per CTA (sharing the edge work across two slices halves the
         // lines per table chunk, and the warps then wait on the copies instead)
@@ -1756,7 +1881,7 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
 // ------------------------------------------------------------------ launchers
 size_t dd2d_fp_workspace(const ctp_geometry& g, int, int, unsigned) {
     int vgroup = 0, nrows = 0;
-    bool stream = fp_fast_ok(g, vgroup, nrows) && fp_stream_chunk(g) > 0 && g.nbatch * g.nz >= kFpStreamMinSlices;
+    bool stream = fp_fast_ok(g, vgroup, nrows) && fp_stream_chunk(g) > 0;
     return fp_workspace_min(g) + (stream ? fp_line_tables_bytes(g) : 0);
 }
 

@@ -62,6 +62,24 @@ def test_dd_fp_matches_oracle(name, oracle):
     assert rel_l2(prj, ref) <= TOL
 
 
+@pytest.mark.parametrize("name", ["par_offsets", "par_wide", "fan_wide"])
+def test_streamed_fp_stack_matches_oracle(name, oracle):
+    """Stacks of 8 or more slices run the streamed forward projector (line
+    tables copied into shared memory); parallel beams there sum each edge's
+    running integrals over the lines and take the cell differences once."""
+    p, inp = _case(name)
+    fan = name.startswith("fan")
+    rng = np.random.default_rng(11)
+    base = inp["img"]
+    reps = -(-8 // (base.shape[0] * base.shape[1]))
+    img = np.concatenate([base * np.float32(1 + 0.25 * k) + rng.uniform(0, 0.2, base.shape).astype(np.float32)
+                          for k in range(reps)]).astype(np.float32)
+    assert img.shape[0] * img.shape[1] >= 8
+    prj = host(mods(fan).distance_driven_fp(p, dev(img), dev(inp["angles"])))
+    ref = oracle.dd_fp(p, img, inp["angles"], "fan" if fan else "parallel")
+    assert rel_l2(prj, ref) <= TOL
+
+
 @pytest.mark.parametrize("name", DD_CASES)
 @pytest.mark.parametrize("is_fbp", [False, True])
 def test_dd_bp_parity_matches_oracle(name, is_fbp, oracle):

@@ -37,7 +37,7 @@ def _fp(g, geom_kind, img, ang, ws_bytes):
 def test_streamed_fp_equals_staged(geom_kind, n, nview, nu, du):
     from ctprojector_b200._lib import Geometry, lib
 
-    # 8 slices: the smallest stack that takes the streamed path
+    # 8 slices: a stack that takes the streamed path
     g = Geometry(8, n, n, 1, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, nu, 1, nview, du, 1.0, 0.0, 0.0, 1085.6, 595.0)
     rng = np.random.default_rng(n)
     img = torch.tensor(rng.uniform(0, 1, (8, 1, n, n)).astype(np.float32), device="cuda")
