@@ -90,11 +90,8 @@ int Scratch::acquire(void* user, size_t user_bytes, size_t need, cudaStream_t s)
         ptr_ = user;
         return CTP_OK;
     }
-    cudaError_t e = cudaMallocAsync(&ptr_, need, s);
-    if (e != cudaSuccess) {
-        ptr_ = nullptr;
-        return set_error((int)e, "scratch allocation of %zu bytes failed: %s", need, cudaGetErrorString(e));
-    }
+    int rc = scratch_alloc(&ptr_, need, s);
+    if (rc) return rc;
     owned_ = true;
     return CTP_OK;
 }
@@ -128,7 +125,8 @@ int finish_sync(int rc, cudaStream_t s) {
     return CTP_OK;
 }
 
-// Host-pointer call: pooled device buffers, copies in, op, copy out.
+// Host-pointer call: pooled device buffers, copies in (through pinned
+// staging chunks), op, copy out.
 struct HostCall {
     cudaStream_t s = cudaStreamPerThread;
     void* bufs[8] = {nullptr};
@@ -138,11 +136,7 @@ struct HostCall {
     T* dev(size_t count) {
         if (rc) return nullptr;
         void* p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, count * sizeof(T) + 16, s);
-        if (e != cudaSuccess) {
-            rc = set_error((int)e, "device buffer of %zu bytes: %s", count * sizeof(T), cudaGetErrorString(e));
-            return nullptr;
-        }
+        if ((rc = scratch_alloc(&p, count * sizeof(T) + 16, s))) return nullptr;
         bufs[n++] = p;
         return static_cast<T*>(p);
     }
@@ -150,8 +144,7 @@ struct HostCall {
     T* upload(const T* host, size_t count) {
         T* d = dev<T>(count);
         if (rc) return nullptr;
-        cudaError_t e = cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) rc = set_error((int)e, "host to device copy: %s", cudaGetErrorString(e));
+        rc = staged_upload(d, host, count * sizeof(T), s);
         return d;
     }
     template <typename T>
@@ -165,8 +158,7 @@ struct HostCall {
     template <typename T>
     void download(T* host, const T* d, size_t count) {
         if (rc) return;
-        cudaError_t e = cudaMemcpyAsync(host, d, count * sizeof(T), cudaMemcpyDeviceToHost, s);
-        if (e != cudaSuccess) rc = set_error((int)e, "device to host copy: %s", cudaGetErrorString(e));
+        rc = staged_download(host, d, count * sizeof(T), s);
     }
     int finish() {
         for (int i = 0; i < n; ++i) cudaFreeAsync(bufs[i], s);

@@ -26,6 +26,13 @@ int check_geometry(const ctp_geometry* g, bool need_image, bool need_detector);
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+// staging.cu: the library's stream-ordered scratch pool (plain
+// cudaMallocAsync under graph capture), and copies between pageable host
+// arrays and the device through pinned chunks (synchronous for downloads).
+int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+int staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t s);
+int staged_download(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 // Scratch memory for one call: the caller's workspace when given, otherwise a
 // stream-ordered pool allocation released on the same stream.
 class Scratch {
