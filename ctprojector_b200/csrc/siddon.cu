@@ -108,50 +108,54 @@ __device__ Ray init_ray(const double src[3], const double dst[3], const Grid& g)
 
 // The walk of SiddonRayTracing (siddon.cu:187-252): pick the nearest
 // crossing (ties go to the later axis), emit the segment in the current voxel,
-// step, stop when the index leaves the grid.  The per-axis state is held in
-// scalars and the axis is chosen with branches, so nothing is indexed at run
-// time and the walk stays in registers.
-template <typename F>
+// step, stop when the index leaves the grid.  The crossing parameters are
+// exact in FP64 (an axis' k-th crossing is its first one plus k steps); the
+// walk itself runs in FP32 on their offsets from an anchor, the previous
+// crossing, re-anchored every kAnchorSteps crossings so that the offsets stay
+// within a few voxels (a segment's FP32 rounding is then ~1e-7 of that).  The
+// axis is chosen by selects, not branches, so the rays of a warp step
+// together, and the FP32 arithmetic keeps the walk off the FP64 pipe.
+// IdxT: int when the volume has fewer than 2^31 voxels, else long long.
+constexpr int kAnchorSteps = 16;
+
+template <typename IdxT, typename F>
 __device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
-    double a0 = R.alpha[0], a1 = R.alpha[1], a2 = R.alpha[2];
-    const double d0 = R.dalpha[0], d1 = R.dalpha[1], d2 = R.dalpha[2];
-    int g0 = R.ng[0], g1 = R.ng[1], g2 = R.ng[2];
-    const int s0 = R.step[0], s1 = R.step[1], s2 = R.step[2];
-    const long long nxy = (long long)g.nx * g.ny;
-    const long long m1 = (long long)s1 * g.nx, m2 = (long long)s2 * nxy;
-    long long idx = g2 * nxy + (long long)g1 * g.nx + g0;
-    double aprev = R.aprev;
-    while (true) {
-        double anow;
-        bool out;
-        long long mv;
-        if (a0 < a1 && a0 < a2) {
-            anow = a0;
-            a0 += d0;
-            g0 += s0;
-            out = g0 < 0 || g0 >= g.nx;
-            mv = s0;
-        } else if (a1 < a2) {
-            anow = a1;
-            a1 += d1;
-            g1 += s1;
-            out = g1 < 0 || g1 >= g.ny;
-            mv = m1;
-        } else {
-            anow = a2;
-            a2 += d2;
-            g2 += s2;
-            out = g2 < 0 || g2 >= g.nz;
-            mv = m2;
+    // crossings left on each axis before its index leaves the grid
+    int r0 = R.step[0] > 0 ? g.nx - 1 - R.ng[0] : R.ng[0];
+    int r1 = R.step[1] > 0 ? g.ny - 1 - R.ng[1] : R.ng[1];
+    int r2 = R.step[2] > 0 ? g.nz - 1 - R.ng[2] : R.ng[2];
+    const int q0 = r0, q1 = r1, q2 = r2;
+    const IdxT m0 = (IdxT)R.step[0], m1 = (IdxT)R.step[1] * g.nx, m2 = (IdxT)R.step[2] * g.nx * g.ny;
+    IdxT idx = ((IdxT)R.ng[2] * g.ny + R.ng[1]) * g.nx + R.ng[0];
+    const float d0 = (float)R.dalpha[0], d1 = (float)R.dalpha[1], d2 = (float)R.dalpha[2];
+    double ta = R.aprev;  // anchor: the crossing the local offsets start from
+    for (;;) {
+        float l0 = (float)(fma((double)(q0 - r0), R.dalpha[0], R.alpha[0]) - ta);
+        float l1 = (float)(fma((double)(q1 - r1), R.dalpha[1], R.alpha[1]) - ta);
+        float l2 = (float)(fma((double)(q2 - r2), R.dalpha[2], R.alpha[2]) - ta);
+        float lp = 0.f;
+#pragma unroll 4
+        for (int k = 0; k < kAnchorSteps; ++k) {
+            const bool bx = l0 < l1 && l0 < l2;
+            const bool by = !bx && l1 < l2;
+            const bool bz = !bx && !by;
+            const float m = bx ? l0 : (by ? l1 : l2);
+            emit(idx, m - lp);
+            lp = m;
+            l0 = bx ? l0 + d0 : l0;
+            l1 = by ? l1 + d1 : l1;
+            l2 = bz ? l2 + d2 : l2;
+            r0 -= bx;
+            r1 -= by;
+            r2 -= bz;
+            idx += bx ? m0 : (by ? m1 : m2);
+            if ((r0 | r1 | r2) < 0) return;
         }
-        emit(idx, (float)(anow - aprev));
-        aprev = anow;
-        if (out) break;
-        idx += mv;
+        ta += (double)lp;
     }
 }
 
-template <typename Tin, typename Tout>
+template <typename Tin, typename Tout, typename IdxT>
 __global__ void __launch_bounds__(256) siddon_fp_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
                                                         const float* __restrict__ dc, const float* __restrict__ du_,
                                                         const float* __restrict__ dv_, const float* __restrict__ sr,
@@ -169,7 +173,7 @@ __global__ void __launch_bounds__(256) siddon_fp_kernel(Tout* __restrict__ prj, 
         // each sample is added one step later, so its load overlaps the next
         // step's arithmetic; the summation order is unchanged
         float pv = 0.f, pl = 0.f;
-        walk(R, g, [&](long long idx, float len) {
+        walk<IdxT>(R, g, [&](IdxT idx, float len) {
             const float v = ldf(vol + idx);
             acc = fmaf(pv, pl, acc);
             pv = v;
@@ -183,7 +187,7 @@ __global__ void __launch_bounds__(256) siddon_fp_kernel(Tout* __restrict__ prj, 
 
 // Transpose: scatter prj * length into the volume (FP32 atomics, as the
 // reference's SiddonRayTracingTransposeAtomicAdd, siddon.cu:332).
-template <typename Tin>
+template <typename Tin, typename IdxT>
 __global__ void __launch_bounds__(256) siddon_bp_kernel(float* __restrict__ img, const Tin* __restrict__ prj,
                                                         const float* __restrict__ dc, const float* __restrict__ du_,
                                                         const float* __restrict__ dv_, const float* __restrict__ sr,
@@ -199,7 +203,7 @@ __global__ void __launch_bounds__(256) siddon_bp_kernel(float* __restrict__ img,
     Ray R = init_ray(src, dst, g);
     if (!R.hit) return;
     float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
-    walk(R, g, [&](long long idx, float len) { atomicAdd(vol + idx, p * len); });
+    walk<IdxT>(R, g, [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
 }
 
 __global__ void __launch_bounds__(256) siddon_count_kernel(unsigned long long* __restrict__ count,
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(256) siddon_count_kernel(unsigned long long* _
         double src[3], dst[3];
         ray_ends(src, dst, view, iu, iv, dc, du_, dv_, sr, g, d);
         Ray R = init_ray(src, dst, g);
-        if (R.hit) walk(R, g, [&](long long, float) { ++c; });
+        if (R.hit) walk<long long>(R, g, [&](long long, float) { ++c; });
     }
     __shared__ unsigned long long blk;
     if (threadIdx.x == 0) blk = 0;
@@ -245,6 +249,7 @@ __device__ void fan_ray_ends(double src[3], double dst[3], float deg, int iu, in
     dst[2] = z;
 }
 
+template <typename IdxT>
 __global__ void __launch_bounds__(256) siddon_fan_fp_kernel(float* __restrict__ prj, const float* __restrict__ img,
                                                             const float* __restrict__ deg, int nview, Grid g, Det d,
                                                             double dsd, double dso, int accumulate) {
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(256) siddon_fan_fp_kernel(float* __restrict__ 
     if (R.hit) {
         const float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
         float pv = 0.f, pl = 0.f;
-        walk(R, g, [&](long long idx, float len) {
+        walk<IdxT>(R, g, [&](IdxT idx, float len) {
             const float v = __ldg(vol + idx);
             acc = fmaf(pv, pl, acc);
             pv = v;
@@ -271,6 +276,7 @@ __global__ void __launch_bounds__(256) siddon_fan_fp_kernel(float* __restrict__ 
     *o = (accumulate ? *o : 0.f) + acc;
 }
 
+template <typename IdxT>
 __global__ void __launch_bounds__(256) siddon_fan_bp_kernel(float* __restrict__ img, const float* __restrict__ prj,
                                                             const float* __restrict__ deg, int nview, Grid g, Det d,
                                                             double dsd, double dso) {
@@ -285,17 +291,19 @@ __global__ void __launch_bounds__(256) siddon_fan_bp_kernel(float* __restrict__ 
     Ray R = init_ray(src, dst, g);
     if (!R.hit) return;
     float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
-    walk(R, g, [&](long long idx, float len) { atomicAdd(vol + idx, p * len); });
+    walk<IdxT>(R, g, [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
 }
 
 dim3 ray_grid(const ctp_geometry& g, size_t nz_mult) {
     return dim3((unsigned)((g.nu + 31) / 32), (unsigned)((g.nv + 7) / 8), (unsigned)(g.nview * nz_mult));
 }
 
-}  // namespace
+// 32-bit voxel indices when one volume has fewer than 2^31 voxels.
+bool small_volume(const ctp_geometry& g) { return (unsigned long long)g.nx * g.ny * g.nz < (1ull << 31); }
 
-int siddon_fp(void* prj, const void* img, const float* dc, const float* du_, const float* dv_, const float* sr,
-              const ctp_geometry& g, unsigned flags, cudaStream_t s) {
+template <typename IdxT>
+int launch_siddon_fp(void* prj, const void* img, const float* dc, const float* du_, const float* dv_, const float* sr,
+                     const ctp_geometry& g, unsigned flags, cudaStream_t s) {
     int acc = (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1;
     dim3 grid = ray_grid(g, g.nbatch);
     Grid gr = make_grid(g);
@@ -303,25 +311,49 @@ int siddon_fp(void* prj, const void* img, const float* dc, const float* du_, con
     int nv = (int)g.nview;
     if (flags & CTP_FLAG_IN_BF16) {
         if (flags & CTP_FLAG_OUT_BF16)
-            siddon_fp_kernel<__nv_bfloat16, __nv_bfloat16><<<grid, 256, 0, s>>>(
+            siddon_fp_kernel<__nv_bfloat16, __nv_bfloat16, IdxT><<<grid, 256, 0, s>>>(
                 (__nv_bfloat16*)prj, (const __nv_bfloat16*)img, dc, du_, dv_, sr, nv, gr, dt, acc);
         else
-            siddon_fp_kernel<__nv_bfloat16, float><<<grid, 256, 0, s>>>((float*)prj, (const __nv_bfloat16*)img, dc,
-                                                                       du_, dv_, sr, nv, gr, dt, acc);
+            siddon_fp_kernel<__nv_bfloat16, float, IdxT><<<grid, 256, 0, s>>>(
+                (float*)prj, (const __nv_bfloat16*)img, dc, du_, dv_, sr, nv, gr, dt, acc);
     } else if (flags & CTP_FLAG_IN_FP16) {
         if (flags & CTP_FLAG_OUT_FP16)
-            siddon_fp_kernel<__half, __half><<<grid, 256, 0, s>>>((__half*)prj, (const __half*)img, dc, du_, dv_, sr,
-                                                                  nv, gr, dt, acc);
+            siddon_fp_kernel<__half, __half, IdxT><<<grid, 256, 0, s>>>((__half*)prj, (const __half*)img, dc, du_, dv_,
+                                                                        sr, nv, gr, dt, acc);
         else
-            siddon_fp_kernel<__half, float><<<grid, 256, 0, s>>>((float*)prj, (const __half*)img, dc, du_, dv_, sr,
-                                                                 nv, gr, dt, acc);
+            siddon_fp_kernel<__half, float, IdxT><<<grid, 256, 0, s>>>((float*)prj, (const __half*)img, dc, du_, dv_,
+                                                                       sr, nv, gr, dt, acc);
     } else {
         if (flags & (CTP_FLAG_OUT_BF16 | CTP_FLAG_OUT_FP16))
             return set_error(CTP_ERR_UNSUPPORTED, "siddon_fp: FP32 input with 16-bit output is not supported");
-        siddon_fp_kernel<float, float><<<grid, 256, 0, s>>>((float*)prj, (const float*)img, dc, du_, dv_, sr, nv, gr,
-                                                            dt, acc);
+        siddon_fp_kernel<float, float, IdxT><<<grid, 256, 0, s>>>((float*)prj, (const float*)img, dc, du_, dv_, sr,
+                                                                  nv, gr, dt, acc);
     }
     return check_launch("siddon_fp_kernel");
+}
+
+template <typename IdxT>
+int launch_siddon_bp(void* img, const void* prj, const float* dc, const float* du_, const float* dv_,
+                     const float* sr, const ctp_geometry& g, unsigned flags, cudaStream_t s) {
+    dim3 grid = ray_grid(g, g.nbatch);
+    if (flags & CTP_FLAG_IN_BF16)
+        siddon_bp_kernel<__nv_bfloat16, IdxT><<<grid, 256, 0, s>>>((float*)img, (const __nv_bfloat16*)prj, dc, du_,
+                                                                   dv_, sr, (int)g.nview, make_grid(g), make_det(g));
+    else if (flags & CTP_FLAG_IN_FP16)
+        siddon_bp_kernel<__half, IdxT><<<grid, 256, 0, s>>>((float*)img, (const __half*)prj, dc, du_, dv_, sr,
+                                                            (int)g.nview, make_grid(g), make_det(g));
+    else
+        siddon_bp_kernel<float, IdxT><<<grid, 256, 0, s>>>((float*)img, (const float*)prj, dc, du_, dv_, sr,
+                                                           (int)g.nview, make_grid(g), make_det(g));
+    return check_launch("siddon_bp_kernel");
+}
+
+}  // namespace
+
+int siddon_fp(void* prj, const void* img, const float* dc, const float* du_, const float* dv_, const float* sr,
+              const ctp_geometry& g, unsigned flags, cudaStream_t s) {
+    return small_volume(g) ? launch_siddon_fp<int>(prj, img, dc, du_, dv_, sr, g, flags, s)
+                           : launch_siddon_fp<long long>(prj, img, dc, du_, dv_, sr, g, flags, s);
 }
 
 int siddon_bp(void* img, const void* prj, const float* dc, const float* du_, const float* dv_, const float* sr,
@@ -332,17 +364,8 @@ int siddon_bp(void* img, const void* prj, const float* dc, const float* du_, con
         cudaError_t e = cudaMemsetAsync(img, 0, g.nbatch * g.nz * g.ny * g.nx * sizeof(float), s);
         if (e != cudaSuccess) return set_error((int)e, "siddon_bp memset: %s", cudaGetErrorString(e));
     }
-    dim3 grid = ray_grid(g, g.nbatch);
-    if (flags & CTP_FLAG_IN_BF16)
-        siddon_bp_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>((float*)img, (const __nv_bfloat16*)prj, dc, du_, dv_,
-                                                             sr, (int)g.nview, make_grid(g), make_det(g));
-    else if (flags & CTP_FLAG_IN_FP16)
-        siddon_bp_kernel<__half><<<grid, 256, 0, s>>>((float*)img, (const __half*)prj, dc, du_, dv_, sr,
-                                                      (int)g.nview, make_grid(g), make_det(g));
-    else
-        siddon_bp_kernel<float><<<grid, 256, 0, s>>>((float*)img, (const float*)prj, dc, du_, dv_, sr,
-                                                     (int)g.nview, make_grid(g), make_det(g));
-    return check_launch("siddon_bp_kernel");
+    return small_volume(g) ? launch_siddon_bp<int>(img, prj, dc, du_, dv_, sr, g, flags, s)
+                           : launch_siddon_bp<long long>(img, prj, dc, du_, dv_, sr, g, flags, s);
 }
 
 int siddon_nnz(unsigned long long* nnz_host, const float* dc, const float* du_, const float* dv_, const float* sr,
@@ -365,9 +388,13 @@ int siddon_nnz(unsigned long long* nnz_host, const float* dc, const float* du_, 
 // Fan-beam Siddon pair (siddonFan.cu:12-274); g.du is the angular cell size.
 int siddon_fan_fp(float* prj, const float* img, const float* deg, const ctp_geometry& g, unsigned flags,
                   cudaStream_t s) {
-    siddon_fan_fp_kernel<<<ray_grid(g, g.nbatch), 256, 0, s>>>(prj, img, deg, (int)g.nview, make_grid(g), make_det(g),
-                                                                (double)g.dsd, (double)g.dso,
-                                                                (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1);
+    const int acc = (flags & CTP_FLAG_ZERO_OUT) ? 0 : 1;
+    if (small_volume(g))
+        siddon_fan_fp_kernel<int><<<ray_grid(g, g.nbatch), 256, 0, s>>>(prj, img, deg, (int)g.nview, make_grid(g),
+                                                                       make_det(g), (double)g.dsd, (double)g.dso, acc);
+    else
+        siddon_fan_fp_kernel<long long><<<ray_grid(g, g.nbatch), 256, 0, s>>>(
+            prj, img, deg, (int)g.nview, make_grid(g), make_det(g), (double)g.dsd, (double)g.dso, acc);
     return check_launch("siddon_fan_fp_kernel");
 }
 
@@ -377,8 +404,12 @@ int siddon_fan_bp(float* img, const float* prj, const float* deg, const ctp_geom
         cudaError_t e = cudaMemsetAsync(img, 0, g.nbatch * g.nz * g.ny * g.nx * sizeof(float), s);
         if (e != cudaSuccess) return set_error((int)e, "siddon_fan_bp memset: %s", cudaGetErrorString(e));
     }
-    siddon_fan_bp_kernel<<<ray_grid(g, g.nbatch), 256, 0, s>>>(img, prj, deg, (int)g.nview, make_grid(g), make_det(g),
-                                                                (double)g.dsd, (double)g.dso);
+    if (small_volume(g))
+        siddon_fan_bp_kernel<int><<<ray_grid(g, g.nbatch), 256, 0, s>>>(img, prj, deg, (int)g.nview, make_grid(g),
+                                                                       make_det(g), (double)g.dsd, (double)g.dso);
+    else
+        siddon_fan_bp_kernel<long long><<<ray_grid(g, g.nbatch), 256, 0, s>>>(
+            img, prj, deg, (int)g.nview, make_grid(g), make_det(g), (double)g.dsd, (double)g.dso);
     return check_launch("siddon_fan_bp_kernel");
 }
 
