@@ -2,15 +2,43 @@
 the reference argument lists of the c* entries."""
 from __future__ import annotations
 
+import ctypes
 from ctypes import c_float, c_int, c_size_t, c_void_p
 
 import numpy as np
 
 from ..._lib import check, lib
 
+_HUGE = 2 << 20  # transparent huge page
+_MADV_HUGEPAGE = 14
+try:
+    _madvise = ctypes.CDLL(None, use_errno=True).madvise
+    _madvise.argtypes = [c_void_p, c_size_t, c_int]
+    _madvise.restype = c_int
+except (OSError, AttributeError):
+    _madvise = None
+
+# Output arrays of at least 8 MB are backed by transparent huge pages where
+# the kernel offers them (module switch, on by default).
+huge_outputs = True
+
 
 def f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def out_array(shape) -> np.ndarray:
+    """A float32 output array for a host entry, which overwrites all of it.
+    The first write of a fresh array costs a page fault and a page clear per
+    4 KB page; large arrays are advised onto 2 MB pages (madvise
+    MADV_HUGEPAGE), which takes 512 times fewer faults."""
+    n = int(np.prod(shape)) * 4
+    if not huge_outputs or _madvise is None or n < 4 * _HUGE:
+        return np.empty(shape, np.float32)
+    buf = np.empty(n + _HUGE, np.uint8)
+    off = (-buf.ctypes.data) % _HUGE
+    _madvise(c_void_p(buf.ctypes.data + off), c_size_t(n // _HUGE * _HUGE), _MADV_HUGEPAGE)  # a hint: failure is harmless
+    return buf[off:off + n].view(np.float32).reshape(shape)
 
 
 def p(a: np.ndarray) -> c_void_p:
@@ -30,4 +58,4 @@ def call(name: str, *args):
     check(getattr(lib(), name)(*args), name)
 
 
-__all__ = ["f32", "p", "geom_args", "call", "c_float", "c_int", "c_size_t"]
+__all__ = ["f32", "out_array", "p", "geom_args", "call", "c_float", "c_int", "c_size_t"]

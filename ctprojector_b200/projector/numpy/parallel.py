@@ -12,13 +12,13 @@ from typing import Union
 import numpy as np
 
 from .._device import filter_code
-from ._host import c_float, c_int, call, f32, geom_args, p
+from ._host import c_float, c_int, call, f32, geom_args, out_array, p
 from .ct_projector import ct_projector
 
 
 def ramp_filter(projector: ct_projector, prj: np.ndarray, filter_type: str = "hann") -> np.ndarray:
     prj = f32(prj)
-    fprj = np.zeros(prj.shape, np.float32)
+    fprj = out_array(prj.shape)
     call("cfbpParallelFilter", p(fprj), p(prj), c_int(prj.shape[0]), c_size_t(prj.shape[3]), c_size_t(prj.shape[2]),
          c_size_t(prj.shape[1]), c_float(projector.du), c_float(projector.dv), c_float(projector.off_u),
          c_float(projector.off_v), c_int(filter_code(filter_type)))
@@ -29,7 +29,7 @@ def distance_driven_fp(projector: ct_projector, img: np.ndarray, angles: np.ndar
                        branchless: Union[bool, int] = False) -> np.ndarray:
     img = f32(img)
     angles = f32(angles)
-    prj = np.zeros([img.shape[0], len(angles), projector.nv, projector.nu], np.float32)
+    prj = out_array([img.shape[0], len(angles), projector.nv, projector.nu])
     call("cDistanceDrivenParallelProjection", p(prj), p(img), p(angles),
          *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(projector.du),
          c_float(projector.dv), c_float(projector.off_u), c_float(projector.off_v), c_int(2 if branchless else 0))
@@ -40,7 +40,7 @@ def distance_driven_bp(projector: ct_projector, prj: np.ndarray, angles: np.ndar
                        is_fbp: Union[bool, int] = False, branchless: Union[bool, int] = False) -> np.ndarray:
     prj = f32(prj)
     angles = f32(angles)
-    img = np.zeros([prj.shape[0], projector.nz, projector.ny, projector.nx], np.float32)
+    img = out_array([prj.shape[0], projector.nz, projector.ny, projector.nx])
     call("cDistanceDrivenParallelBackprojection", p(img), p(prj), p(angles),
          *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(projector.du),
          c_float(projector.dv), c_float(projector.off_u), c_float(projector.off_v),
@@ -53,7 +53,7 @@ def pixel_driven_bp(projector: ct_projector, prj: np.ndarray, angles: np.ndarray
     no weights (reference :75)."""
     prj = f32(prj)
     angles = f32(angles)
-    img = np.zeros([prj.shape[0], projector.nz, projector.ny, projector.nx], np.float32)
+    img = out_array([prj.shape[0], projector.nz, projector.ny, projector.nx])
     call("cfbpParallelBackprojection", p(img), p(prj), p(angles),
          *geom_args(projector, img.shape[0], img.shape[1:], prj.shape[1:]), c_float(projector.du),
          c_float(projector.dv), c_float(projector.off_u), c_float(projector.off_v), c_int(0))
