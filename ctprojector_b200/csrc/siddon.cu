@@ -118,21 +118,20 @@ __device__ Ray init_ray(const double src[3], const double dst[3], const Grid& g)
 // IdxT: int when the volume has fewer than 2^31 voxels, else long long.
 constexpr int kAnchorSteps = 16;
 
+// One span of the walk: per axis k, crossing m (0-based) lies at
+// a0[k] + m da[k]; taken[k] crossings are behind the start, rem[k] more stay
+// inside the span (the next one after those leaves it); idx is the start
+// voxel and mv[k] the index step of a crossing; ta is the start parameter.
 template <typename IdxT, typename F>
-__device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
-    // crossings left on each axis before its index leaves the grid
-    int r0 = R.step[0] > 0 ? g.nx - 1 - R.ng[0] : R.ng[0];
-    int r1 = R.step[1] > 0 ? g.ny - 1 - R.ng[1] : R.ng[1];
-    int r2 = R.step[2] > 0 ? g.nz - 1 - R.ng[2] : R.ng[2];
-    const int q0 = r0, q1 = r1, q2 = r2;
-    const IdxT m0 = (IdxT)R.step[0], m1 = (IdxT)R.step[1] * g.nx, m2 = (IdxT)R.step[2] * g.nx * g.ny;
-    IdxT idx = ((IdxT)R.ng[2] * g.ny + R.ng[1]) * g.nx + R.ng[0];
-    const float d0 = (float)R.dalpha[0], d1 = (float)R.dalpha[1], d2 = (float)R.dalpha[2];
-    double ta = R.aprev;  // anchor: the crossing the local offsets start from
+__device__ __forceinline__ void walk_span(const double a0[3], const double da[3], const int taken[3], int r0, int r1,
+                                          int r2, IdxT idx, const IdxT mv[3], double ta, F&& emit) {
+    const int q0 = r0 + taken[0], q1 = r1 + taken[1], q2 = r2 + taken[2];  // crossings taken = q - r
+    const float d0 = (float)da[0], d1 = (float)da[1], d2 = (float)da[2];
     for (;;) {
-        float l0 = (float)(fma((double)(q0 - r0), R.dalpha[0], R.alpha[0]) - ta);
-        float l1 = (float)(fma((double)(q1 - r1), R.dalpha[1], R.alpha[1]) - ta);
-        float l2 = (float)(fma((double)(q2 - r2), R.dalpha[2], R.alpha[2]) - ta);
+        // offsets of the next crossings from the anchor (never behind it)
+        float l0 = fmaxf((float)(fma((double)(q0 - r0), da[0], a0[0]) - ta), 0.f);
+        float l1 = fmaxf((float)(fma((double)(q1 - r1), da[1], a0[1]) - ta), 0.f);
+        float l2 = fmaxf((float)(fma((double)(q2 - r2), da[2], a0[2]) - ta), 0.f);
         float lp = 0.f;
 #pragma unroll 4
         for (int k = 0; k < kAnchorSteps; ++k) {
@@ -148,11 +147,23 @@ __device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
             r0 -= bx;
             r1 -= by;
             r2 -= bz;
-            idx += bx ? m0 : (by ? m1 : m2);
+            idx += bx ? mv[0] : (by ? mv[1] : mv[2]);
             if ((r0 | r1 | r2) < 0) return;
         }
         ta += (double)lp;
     }
+}
+
+template <typename IdxT, typename F>
+__device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
+    // crossings left on each axis before its index leaves the grid
+    const int r0 = R.step[0] > 0 ? g.nx - 1 - R.ng[0] : R.ng[0];
+    const int r1 = R.step[1] > 0 ? g.ny - 1 - R.ng[1] : R.ng[1];
+    const int r2 = R.step[2] > 0 ? g.nz - 1 - R.ng[2] : R.ng[2];
+    const IdxT mv[3] = {(IdxT)R.step[0], (IdxT)R.step[1] * g.nx, (IdxT)R.step[2] * g.nx * g.ny};
+    const IdxT idx = ((IdxT)R.ng[2] * g.ny + R.ng[1]) * g.nx + R.ng[0];
+    const int taken[3] = {0, 0, 0};
+    walk_span<IdxT>(R.alpha, R.dalpha, taken, r0, r1, r2, idx, mv, R.aprev, emit);
 }
 
 template <typename Tin, typename Tout, typename IdxT>
