@@ -154,16 +154,23 @@ __device__ __forceinline__ void walk_span(const double a0[3], const double da[3]
     }
 }
 
+// The whole walk of a ray over a volume with index strides (sx, sy, sz).
 template <typename IdxT, typename F>
-__device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
+__device__ __forceinline__ void walk_strided(const Ray& R, const Grid& g, IdxT sx, IdxT sy, IdxT sz, F&& emit) {
     // crossings left on each axis before its index leaves the grid
     const int r0 = R.step[0] > 0 ? g.nx - 1 - R.ng[0] : R.ng[0];
     const int r1 = R.step[1] > 0 ? g.ny - 1 - R.ng[1] : R.ng[1];
     const int r2 = R.step[2] > 0 ? g.nz - 1 - R.ng[2] : R.ng[2];
-    const IdxT mv[3] = {(IdxT)R.step[0], (IdxT)R.step[1] * g.nx, (IdxT)R.step[2] * g.nx * g.ny};
-    const IdxT idx = ((IdxT)R.ng[2] * g.ny + R.ng[1]) * g.nx + R.ng[0];
+    const IdxT mv[3] = {(IdxT)R.step[0] * sx, (IdxT)R.step[1] * sy, (IdxT)R.step[2] * sz};
+    const IdxT idx = (IdxT)R.ng[0] * sx + (IdxT)R.ng[1] * sy + (IdxT)R.ng[2] * sz;
     const int taken[3] = {0, 0, 0};
     walk_span<IdxT>(R.alpha, R.dalpha, taken, r0, r1, r2, idx, mv, R.aprev, emit);
+}
+
+// The walk over the volume's own [z][y][x] layout.
+template <typename IdxT, typename F>
+__device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
+    walk_strided<IdxT>(R, g, (IdxT)1, (IdxT)g.nx, (IdxT)g.nx * g.ny, emit);
 }
 
 template <typename Tin, typename Tout, typename IdxT>
@@ -197,12 +204,18 @@ __global__ void __launch_bounds__(256) siddon_fp_kernel(Tout* __restrict__ prj, 
 }
 
 // Transpose: scatter prj * length into the volume (FP32 atomics, as the
-// reference's SiddonRayTracingTransposeAtomicAdd, siddon.cu:332).
+// reference's SiddonRayTracingTransposeAtomicAdd, siddon.cu:332).  The lanes
+// of a warp are neighbouring detector cells, so at a given step they sit on
+// voxels next to each other across the rays, along the detector's u
+// direction.  When u runs mainly along y, those voxels are a row apart in the
+// [z][y][x] volume and every lane's reduction is a separate L2 sector; such
+// views scatter into imgT, laid out [z][x][y] (when given), where they are
+// adjacent and share sectors, and imgT is added back transposed at the end.
 template <typename Tin, typename IdxT>
-__global__ void __launch_bounds__(256) siddon_bp_kernel(float* __restrict__ img, const Tin* __restrict__ prj,
-                                                        const float* __restrict__ dc, const float* __restrict__ du_,
-                                                        const float* __restrict__ dv_, const float* __restrict__ sr,
-                                                        int nview, Grid g, Det d) {
+__global__ void __launch_bounds__(256) siddon_bp_kernel(float* __restrict__ img, float* __restrict__ imgT,
+                                                        const Tin* __restrict__ prj, const float* __restrict__ dc,
+                                                        const float* __restrict__ du_, const float* __restrict__ dv_,
+                                                        const float* __restrict__ sr, int nview, Grid g, Det d) {
     int iu = blockIdx.x * 32 + (threadIdx.x & 31);
     int iv = blockIdx.y * 8 + (threadIdx.x >> 5);
     int view = blockIdx.z % nview, b = blockIdx.z / nview;
@@ -213,8 +226,30 @@ __global__ void __launch_bounds__(256) siddon_bp_kernel(float* __restrict__ img,
     ray_ends(src, dst, view, iu, iv, dc, du_, dv_, sr, g, d);
     Ray R = init_ray(src, dst, g);
     if (!R.hit) return;
-    float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
-    walk<IdxT>(R, g, [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
+    const bool across_y = imgT && fabsf(du_[view * 3 + 1]) > fabsf(du_[view * 3]);
+    float* vol = (across_y ? imgT : img) + (size_t)b * g.nx * g.ny * g.nz;
+    if (across_y)
+        walk_strided<IdxT>(R, g, (IdxT)g.ny, (IdxT)1, (IdxT)g.nx * g.ny,
+                           [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
+    else
+        walk<IdxT>(R, g, [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
+}
+
+// img[b][z][y][x] += imgT[b][z][x][y], through 32x32 shared tiles.
+__global__ void __launch_bounds__(256) add_transposed_kernel(float* __restrict__ img, const float* __restrict__ imgT,
+                                                             int nx, int ny) {
+    __shared__ float t[32][33];
+    const size_t plane = (size_t)blockIdx.z * nx * ny;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += 8) {  // read rows of imgT: x fixed, y contiguous
+        const int x = x0 + k, y = y0 + threadIdx.x;
+        if (x < nx && y < ny) t[k][threadIdx.x] = imgT[plane + (size_t)x * ny + y];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int y = y0 + k, x = x0 + threadIdx.x;
+        if (x < nx && y < ny) img[plane + (size_t)y * nx + x] += t[threadIdx.x][k];
+    }
 }
 
 __global__ void __launch_bounds__(256) siddon_count_kernel(unsigned long long* __restrict__ count,
@@ -347,16 +382,33 @@ template <typename IdxT>
 int launch_siddon_bp(void* img, const void* prj, const float* dc, const float* du_, const float* dv_,
                      const float* sr, const ctp_geometry& g, unsigned flags, cudaStream_t s) {
     dim3 grid = ray_grid(g, g.nbatch);
+    // the transposed scatter target (zeroed), when the scratch can be had
+    const size_t vox = g.nbatch * g.nz * g.ny * g.nx;
+    Scratch scr;
+    float* imgT = nullptr;
+    if (!scr.acquire(nullptr, 0, vox * sizeof(float), s)) {
+        imgT = reinterpret_cast<float*>(scr.base());
+        cudaError_t e = cudaMemsetAsync(imgT, 0, vox * sizeof(float), s);
+        if (e != cudaSuccess) return set_error((int)e, "siddon_bp memset: %s", cudaGetErrorString(e));
+    } else {
+        cudaGetLastError();  // fall back to the plain layout
+    }
     if (flags & CTP_FLAG_IN_BF16)
-        siddon_bp_kernel<__nv_bfloat16, IdxT><<<grid, 256, 0, s>>>((float*)img, (const __nv_bfloat16*)prj, dc, du_,
-                                                                   dv_, sr, (int)g.nview, make_grid(g), make_det(g));
+        siddon_bp_kernel<__nv_bfloat16, IdxT><<<grid, 256, 0, s>>>((float*)img, imgT, (const __nv_bfloat16*)prj, dc,
+                                                                   du_, dv_, sr, (int)g.nview, make_grid(g),
+                                                                   make_det(g));
     else if (flags & CTP_FLAG_IN_FP16)
-        siddon_bp_kernel<__half, IdxT><<<grid, 256, 0, s>>>((float*)img, (const __half*)prj, dc, du_, dv_, sr,
+        siddon_bp_kernel<__half, IdxT><<<grid, 256, 0, s>>>((float*)img, imgT, (const __half*)prj, dc, du_, dv_, sr,
                                                             (int)g.nview, make_grid(g), make_det(g));
     else
-        siddon_bp_kernel<float, IdxT><<<grid, 256, 0, s>>>((float*)img, (const float*)prj, dc, du_, dv_, sr,
+        siddon_bp_kernel<float, IdxT><<<grid, 256, 0, s>>>((float*)img, imgT, (const float*)prj, dc, du_, dv_, sr,
                                                            (int)g.nview, make_grid(g), make_det(g));
-    return check_launch("siddon_bp_kernel");
+    int rc = check_launch("siddon_bp_kernel");
+    if (rc || !imgT) return rc;
+    add_transposed_kernel<<<dim3((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 31) / 32),
+                                 (unsigned)(g.nbatch * g.nz)),
+                            dim3(32, 8), 0, s>>>((float*)img, imgT, (int)g.nx, (int)g.ny);
+    return check_launch("add_transposed_kernel");
 }
 
 }  // namespace
