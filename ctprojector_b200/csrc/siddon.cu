@@ -322,8 +322,11 @@ __global__ void __launch_bounds__(256) siddon_fan_fp_kernel(float* __restrict__ 
     *o = (accumulate ? *o : 0.f) + acc;
 }
 
+// As siddon_bp_kernel: views whose detector tangent runs mainly along y
+// scatter into the [z][x][y] copy imgT (when given).
 template <typename IdxT>
-__global__ void __launch_bounds__(256) siddon_fan_bp_kernel(float* __restrict__ img, const float* __restrict__ prj,
+__global__ void __launch_bounds__(256) siddon_fan_bp_kernel(float* __restrict__ img, float* __restrict__ imgT,
+                                                            const float* __restrict__ prj,
                                                             const float* __restrict__ deg, int nview, Grid g, Det d,
                                                             double dsd, double dso) {
     int iu = blockIdx.x * 32 + (threadIdx.x & 31);
@@ -336,8 +339,14 @@ __global__ void __launch_bounds__(256) siddon_fan_bp_kernel(float* __restrict__ 
     fan_ray_ends(src, dst, deg[view], iu, iv, d, dsd, dso);
     Ray R = init_ray(src, dst, g);
     if (!R.hit) return;
-    float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
-    walk<IdxT>(R, g, [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
+    const float th = deg[view];
+    const bool across_y = imgT && fabsf(sinf(th)) > fabsf(cosf(th));
+    float* vol = (across_y ? imgT : img) + (size_t)b * g.nx * g.ny * g.nz;
+    if (across_y)
+        walk_strided<IdxT>(R, g, (IdxT)g.ny, (IdxT)1, (IdxT)g.nx * g.ny,
+                           [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
+    else
+        walk<IdxT>(R, g, [&](IdxT idx, float len) { atomicAdd(vol + idx, p * len); });
 }
 
 dim3 ray_grid(const ctp_geometry& g, size_t nz_mult) {
@@ -467,13 +476,29 @@ int siddon_fan_bp(float* img, const float* prj, const float* deg, const ctp_geom
         cudaError_t e = cudaMemsetAsync(img, 0, g.nbatch * g.nz * g.ny * g.nx * sizeof(float), s);
         if (e != cudaSuccess) return set_error((int)e, "siddon_fan_bp memset: %s", cudaGetErrorString(e));
     }
+    const size_t vox = g.nbatch * g.nz * g.ny * g.nx;
+    Scratch scr;
+    float* imgT = nullptr;
+    if (!scr.acquire(nullptr, 0, vox * sizeof(float), s)) {
+        imgT = reinterpret_cast<float*>(scr.base());
+        cudaError_t e = cudaMemsetAsync(imgT, 0, vox * sizeof(float), s);
+        if (e != cudaSuccess) return set_error((int)e, "siddon_fan_bp memset: %s", cudaGetErrorString(e));
+    } else {
+        cudaGetLastError();  // fall back to the plain layout
+    }
     if (small_volume(g))
-        siddon_fan_bp_kernel<int><<<ray_grid(g, g.nbatch), 256, 0, s>>>(img, prj, deg, (int)g.nview, make_grid(g),
-                                                                       make_det(g), (double)g.dsd, (double)g.dso);
+        siddon_fan_bp_kernel<int><<<ray_grid(g, g.nbatch), 256, 0, s>>>(img, imgT, prj, deg, (int)g.nview,
+                                                                       make_grid(g), make_det(g), (double)g.dsd,
+                                                                       (double)g.dso);
     else
         siddon_fan_bp_kernel<long long><<<ray_grid(g, g.nbatch), 256, 0, s>>>(
-            img, prj, deg, (int)g.nview, make_grid(g), make_det(g), (double)g.dsd, (double)g.dso);
-    return check_launch("siddon_fan_bp_kernel");
+            img, imgT, prj, deg, (int)g.nview, make_grid(g), make_det(g), (double)g.dsd, (double)g.dso);
+    int rc = check_launch("siddon_fan_bp_kernel");
+    if (rc || !imgT) return rc;
+    add_transposed_kernel<<<dim3((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 31) / 32),
+                                 (unsigned)(g.nbatch * g.nz)),
+                            dim3(32, 8), 0, s>>>(img, imgT, (int)g.nx, (int)g.ny);
+    return check_launch("add_transposed_kernel");
 }
 
 }  // namespace ctp

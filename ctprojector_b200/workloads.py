@@ -2,12 +2,14 @@
 
     python -m ctprojector_b200.workloads <op> <workload> [--repeat N]
 
-op: fp, bp, bp_fbp, bp_adjoint, filter, siddon_fp, siddon_bp
+op: fp, bp, bp_fbp, bp_adjoint, filter, siddon_fp, siddon_bp, tomo_fp, tomo_bp
 workload:
   par512x16   parallel 16 x 512^2 at 0.8 mm, 720 views over pi, 768 cells
   fan512x4    fan 4 x 512^2 at 0.8 mm, 984 views over 2 pi, 888 cells
   fan256      fan 1 x 256^2 at 1.0 mm, 360 views over 2 pi, 736 cells
   cone64      helical cone 1 x 64 x 512^2 at 0.7 x 0.7 x 1.0 mm, 360 views, 736 x 64 panel
+  tomo64      tomosynthesis 1 x 64 x 256 x 512 (z, y, x) at 0.4 x 0.4 x 1.0 mm, 25 views over 30 degrees,
+              1024 x 512 detector of 0.25 mm cells 20 mm below the volume centre, source arc radius 650 mm
 
 Inputs are seeded uniform random arrays of the workload's shapes (the
 operations' cost does not depend on the values).  The operation runs once
@@ -38,6 +40,10 @@ def _workload(name):
         scan = S.Scan(512, 512, 64, 0.7, 0.7, 1.0, 736, 64, 1.2858, 1.0, 360)
         geo = S.helical(360, 1.0, scan.dso, scan.dsd, 64 * scan.dso / scan.dsd)
         return "cone", scan, geo, 1
+    if name == "tomo64":
+        scan = S.Scan(512, 256, 64, 0.4, 0.4, 1.0, 1024, 512, 0.25, 0.25, 25)
+        dc, src = S.tomo_geometry(25, 30.0, 650.0, -52.0)
+        return "tomo", scan, (dc, src), 1
     raise SystemExit(f"unknown workload {name!r}")
 
 
@@ -55,7 +61,12 @@ def main(argv=None) -> int:
     kind, scan, geo, nb = _workload(a.workload)
     rng = np.random.default_rng(0)
     dev = torch.device("cuda")
-    if kind == "cone":
+    if kind == "tomo":
+        g = [torch.tensor(x, device=dev) for x in geo]
+        img = torch.tensor(rng.uniform(0, 1, (nb, scan.nz, scan.ny, scan.nx)).astype(np.float32), device=dev)
+        prj = torch.tensor(rng.uniform(0, 1, (nb, len(geo[0]), scan.nv, scan.nu)).astype(np.float32), device=dev)
+        ops = {"tomo_fp": lambda: D.tomo_fp(scan, img, *g), "tomo_bp": lambda: D.tomo_bp(scan, prj, *g)}
+    elif kind == "cone":
         g = [torch.tensor(x, device=dev) for x in geo]
         img = torch.tensor(rng.uniform(0, 1, (nb, scan.nz, scan.ny, scan.nx)).astype(np.float32), device=dev)
         prj = torch.tensor(rng.uniform(0, 1, (nb, len(geo[0]), scan.nv, scan.nu)).astype(np.float32), device=dev)
