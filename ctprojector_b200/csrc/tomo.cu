@@ -47,6 +47,41 @@ __device__ float box2d(const float* __restrict__ p, float x1, float y1, float x2
     return v;
 }
 
+// The same integral when the rectangle spans at most K pixels along each axis
+// (x2 - x1 <= K - 1 and y2 - y1 <= K - 1, K = 2 or 3): the pixel weights are
+// the overlaps of the clamped rectangle with K consecutive columns and rows,
+// straight-line code with K*K loads (indices clamped, weights 0 past the
+// edge) instead of the general loops.
+template <int K>
+__device__ __forceinline__ float box2d_small(const float* __restrict__ p, float x1, float y1, float x2, float y2,
+                                             int nx, int ny) {
+    x1 = clampf(x1, 0.f, (float)nx);
+    y1 = clampf(y1, 0.f, (float)ny);
+    x2 = clampf(x2, 0.f, (float)nx);
+    y2 = clampf(y2, 0.f, (float)ny);
+    if (x2 <= x1 || y2 <= y1) return 0.f;
+    const int ix = min((int)x1, nx - 1), iy = min((int)y1, ny - 1);
+    float wx[K], wy[K];
+    int cx[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        // overlap of [x1, x2] with column ix + k (and of [y1, y2] with row iy + k)
+        wx[k] = fmaxf(fminf(x2, (float)(ix + k + 1)) - fmaxf(x1, (float)(ix + k)), 0.f);
+        wy[k] = fmaxf(fminf(y2, (float)(iy + k + 1)) - fmaxf(y1, (float)(iy + k)), 0.f);
+        cx[k] = min(ix + k, nx - 1);
+    }
+    float v = 0.f;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const float* row = p + (size_t)min(iy + j, ny - 1) * nx;
+        float r = 0.f;
+#pragma unroll
+        for (int k = 0; k < K; ++k) r = fmaf(wx[k], __ldg(row + cx[k]), r);
+        v = fmaf(wy[j], r, v);
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(256) tomo_fp_kernel(float* __restrict__ prj, const float* __restrict__ img,
                                                       const float* __restrict__ dc, const float* __restrict__ sr,
                                                       int nview, Grid g, Det d, int accumulate) {
@@ -72,11 +107,28 @@ __global__ void __launch_bounds__(256) tomo_fp_kernel(float* __restrict__ prj, c
     double ry1 = (ya - sy) / (cz - sz), ry2 = (yb - sy) / (cz - sz);
     const float* vol = img + (size_t)b * g.nx * g.ny * g.nz;
     float val = 0.f;
-    for (int iz = 0; iz < g.nz; ++iz) {
-        double dz = iz - sz;
-        float x1 = (float)(sx + rx1 * dz), x2 = (float)(sx + rx2 * dz);
-        float y1 = (float)(sy + ry1 * dz), y2 = (float)(sy + ry2 * dz);
-        val += box2d(vol + (size_t)iz * g.nx * g.ny, x1, y1, x2, y2, g.nx, g.ny) / ((x2 - x1) * (y2 - y1));
+    // footprint widths grow linearly with the distance from the source: the
+    // widest is on the end plane farther from it
+    const double dmax = fmax(fabs(0.0 - sz), fabs((double)(g.nz - 1) - sz));
+    if (fabs(rx2 - rx1) * dmax <= 1.0 && fabs(ry2 - ry1) * dmax <= 1.0) {
+        // at most 2 x 2 pixels per plane; edges in FP32 from per-ray FP32
+        // coefficients (the width and the integral see the same rounded edges)
+        const float fsx = (float)sx, fsy = (float)sy, fsz = (float)sz;
+        const float frx1 = (float)rx1, frx2 = (float)rx2, fry1 = (float)ry1, fry2 = (float)ry2;
+        for (int iz = 0; iz < g.nz; ++iz) {
+            const float dz = (float)iz - fsz;
+            const float x1 = fmaf(frx1, dz, fsx), x2 = fmaf(frx2, dz, fsx);
+            const float y1 = fmaf(fry1, dz, fsy), y2 = fmaf(fry2, dz, fsy);
+            val += __fdividef(box2d_small<2>(vol + (size_t)iz * g.nx * g.ny, x1, y1, x2, y2, g.nx, g.ny),
+                              (x2 - x1) * (y2 - y1));
+        }
+    } else {
+        for (int iz = 0; iz < g.nz; ++iz) {
+            double dz = iz - sz;
+            float x1 = (float)(sx + rx1 * dz), x2 = (float)(sx + rx2 * dz);
+            float y1 = (float)(sy + ry1 * dz), y2 = (float)(sy + ry2 * dz);
+            val += box2d(vol + (size_t)iz * g.nx * g.ny, x1, y1, x2, y2, g.nx, g.ny) / ((x2 - x1) * (y2 - y1));
+        }
     }
     double D[3] = {C[0] + u, C[1] + v, C[2]};
     double L = sqrt((S[2] - D[2]) * (S[2] - D[2]) + (S[1] - D[1]) * (S[1] - D[1]) + (S[0] - D[0]) * (S[0] - D[0]));
@@ -121,7 +173,13 @@ __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, c
         float u2 = (Sx - Cx + r * (x + g.dx / 2 - Sx)) / d.du + d.off_u + (d.nu - 1) / 2.0f;
         float v1 = (Sy - Cy + r * (y - g.dy / 2 - Sy)) / d.dv + d.off_v + (d.nv - 1) / 2.0f;
         float v2 = (Sy - Cy + r * (y + g.dy / 2 - Sy)) / d.dv + d.off_v + (d.nv - 1) / 2.0f;
-        val += box2d(pb + (size_t)view * d.nv * d.nu, u1, v1, u2, v2, d.nu, d.nv) / ((u2 - u1) * (v2 - v1));
+        const float* pv = pb + (size_t)view * d.nv * d.nu;
+        const float w = fabsf(u2 - u1), h = fabsf(v2 - v1);
+        float box;
+        if (w <= 1.f && h <= 1.f) box = box2d_small<2>(pv, u1, v1, u2, v2, d.nu, d.nv);
+        else if (w <= 2.f && h <= 2.f) box = box2d_small<3>(pv, u1, v1, u2, v2, d.nu, d.nv);
+        else box = box2d(pv, u1, v1, u2, v2, d.nu, d.nv);
+        val += box / ((u2 - u1) * (v2 - v1));
     }
     float* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
     *o = (accumulate ? *o : 0.f) + val;

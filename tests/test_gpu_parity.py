@@ -208,6 +208,29 @@ def test_tomo_matches_oracle(oracle):
     assert rel_l2(img, ref_bp) <= TOL
 
 
+@pytest.mark.parametrize("cell", [0.1, 0.25, 0.5, 1.3])
+def test_tomo_footprint_sizes_match_oracle(oracle, cell):
+    """Detector cells of 0.1 to 1.3 mm under 0.4 mm voxels: the forward
+    projector's footprints span up to 2 x 2 pixels per plane (straight-line
+    path) or more (general loop), the back projector's up to 2 x 2, 3 x 3 or
+    more cells per view; every path against the FP64 oracle."""
+    from cases import Proj
+
+    from ctprojector_b200 import synthetic as S
+    from ctprojector_b200.projector.cupy import tomo
+
+    n = int(round(64 * 0.25 / cell))
+    p = Proj(nx=96, ny=64, nz=10, dx=0.4, dy=0.4, dz=1.0, nu=2 * n, nv=n, du=cell, dv=cell, nview=9)
+    dc, sr = S.tomo_geometry(9, 30.0, 650.0, -12.0)
+    rng = np.random.default_rng(int(cell * 100))
+    img = S.ellipsoid_phantom(rng, 10, 64, 96, 1.0, 0.4, 0.4, supersample=1)[None]
+    prj = host(tomo.distance_driven_fp(p, dev(img), dev(dc), dev(sr)))
+    ref = oracle.tomo_fp(p, img, dc, sr)
+    assert rel_l2(prj, ref) <= TOL
+    bp = host(tomo.distance_driven_bp(p, dev(ref), dev(dc), dev(sr)))
+    assert rel_l2(bp, oracle.tomo_bp(p, ref, dc, sr)) <= TOL
+
+
 # ----------------------------------------------------------------- vs the reference itself
 @pytest.mark.parametrize("name", DD_CASES + ["kat", "par_wide", "fan_wide", "fan_45"])
 def test_dd_matches_reference_golden(name):
