@@ -55,19 +55,20 @@ def test_numpy_module_equals_device_module(fan):
     np.testing.assert_allclose(f_n, f_c, rtol=0, atol=1e-6 * np.abs(f_c).max())
 
 
-def test_host_entries_large_arrays_through_pinned_staging():
+@pytest.mark.parametrize("nb,nview", [(6, 500), (11, 900)])
+def test_host_entries_large_arrays_through_pinned_staging(nb, nview):
     """Host arrays above the staging threshold cross the link in 8 MB pinned
-    chunks (worker threads copy the pageable side): 6 × 400² slices and a
-    500-view, 700-cell sinogram (8.4 MB, ragged last chunk) give the same
-    bits as the device entries, from pageable and from pinned host arrays."""
+    chunks (worker threads copy the pageable side; 12 and 26 MB sinograms,
+    ragged last chunks): the results have the same bits as the device
+    entries, from pageable and from pinned host arrays."""
     from ctprojector_b200.projector.cupy import parallel as CP
     from ctprojector_b200.projector.numpy import parallel as NP
     from cases import Proj
 
-    p = Proj(nx=400, ny=400, nz=1, dx=1.0, dy=1.0, nu=700, nv=1, du=0.9, dv=1.0, nview=500)
+    p = Proj(nx=400, ny=400, nz=1, dx=1.0, dy=1.0, nu=700, nv=1, du=0.9, dv=1.0, nview=nview)
     rng = np.random.default_rng(21)
-    img = rng.uniform(0, 1, (6, 1, 400, 400)).astype(np.float32)
-    ang = (np.arange(500) * np.pi / 500).astype(np.float32)
+    img = rng.uniform(0, 1, (nb, 1, 400, 400)).astype(np.float32)
+    ang = (np.arange(nview) * np.pi / nview).astype(np.float32)
     prj_c = host(CP.distance_driven_fp(p, dev(img), dev(ang)))
     assert prj_c.nbytes > 8 << 20 and prj_c.nbytes % (8 << 20) != 0
     np.testing.assert_array_equal(NP.distance_driven_fp(p, img, ang), prj_c)
