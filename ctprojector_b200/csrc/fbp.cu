@@ -750,6 +750,7 @@ __global__ void fbp_fan_bp_kernel(float* __restrict__ img, const float* __restri
     float acc[kFbpZ];
 #pragma unroll
     for (int q = 0; q < kFbpZ; ++q) acc[q] = 0.f;
+    const float inv_du = 1.f / d.du;
     const float* pb = prj + (size_t)b * nview * d.nv * d.nu;
     for (int v0 = 0; v0 < nview; v0 += kFbpViews) {
         int nvc = min(kFbpViews, nview - v0);
@@ -764,9 +765,11 @@ __global__ void fbp_fan_bp_kernel(float* __restrict__ img, const float* __restri
             for (int vi = 0; vi < nvc; ++vi) {
                 float c = s_c[vi], s = s_s[vi];
                 float rx = x * c + y * s, ry = -x * s + y * c;
-                float a = atanf(rx / (ry + dso));
-                float dist = dso * dso / (rx * rx + (dso + ry) * (dso + ry));
-                float pu = -(a / d.du + d.off_u) + (d.nu - 1.0f) / 2.0f;
+                // fast divides and a reciprocal for 1/du: a few ulp, against
+                // the IEEE divide sequences of the reference's expressions
+                float a = atanf(__fdividef(rx, ry + dso));
+                float dist = __fdividef(dso * dso, rx * rx + (dso + ry) * (dso + ry));
+                float pu = -(a * inv_du + d.off_u) + (d.nu - 1.0f) / 2.0f;
                 if (pu < 0 || pu >= d.nu) continue;
                 int i0 = (int)pu;
                 int i1 = min(i0 + 1, d.nu - 1);
@@ -818,6 +821,7 @@ __global__ void pixel_bp_par_kernel(float* __restrict__ img, const float* __rest
     float acc[kFbpZ];
 #pragma unroll
     for (int q = 0; q < kFbpZ; ++q) acc[q] = 0.f;
+    const float inv_du = 1.f / d.du;
     const float* pb = prj + (size_t)b * nview * d.nv * d.nu;
     for (int v0 = 0; v0 < nview; v0 += kFbpViews) {
         int nvc = min(kFbpViews, nview - v0);
@@ -830,7 +834,7 @@ __global__ void pixel_bp_par_kernel(float* __restrict__ img, const float* __rest
         __syncthreads();
         if (ix < g.nx && iy < g.ny) {
             for (int vi = 0; vi < nvc; ++vi) {
-                float pu = -((x * s_c[vi] + y * s_s[vi]) / d.du + d.off_u) + (d.nu - 1.0f) / 2.0f;
+                float pu = -((x * s_c[vi] + y * s_s[vi]) * inv_du + d.off_u) + (d.nu - 1.0f) / 2.0f;
                 if (pu < 0 || pu >= d.nu) continue;
                 int i0 = (int)pu;
                 int i1 = min(i0 + 1, d.nu - 1);
