@@ -133,3 +133,20 @@ def test_view_split_back_projection_two_ranks():
     assert out[0][1] == (0, 3) and out[1][1] == (3, 5)
     for r in range(world):
         assert out[r][2] <= 1e-12 and out[r][3] <= 1e-12
+
+
+def test_view_shares_and_slabs_partition():
+    """Round-robin view shares and z slabs cover every view and slice once,
+    also with more ranks than slices (trailing ranks own empty slabs)."""
+    from ctprojector_b200.multigpu import view_shares, z_slabs
+
+    for nview, world in [(1, 1), (7, 2), (360, 8), (5, 8)]:
+        shares = [view_shares(nview, r, world) for r in range(world)]
+        assert sorted(v for s in shares for v in s) == list(range(nview))
+    for nz, world in [(1, 1), (5, 2), (64, 8), (3, 8)]:
+        slabs = z_slabs(nz, world)
+        assert slabs[0][0] == 0 and slabs[-1][1] == nz
+        assert all(a[1] == b[0] for a, b in zip(slabs, slabs[1:]))
+        assert all(z1 >= z0 for z0, z1 in slabs)
+    with pytest.raises(ValueError):
+        view_shares(10, 2, 2)
