@@ -643,13 +643,6 @@ constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr int kRoundMagicBits = 0x4B400000;
 
-__device__ __forceinline__ float prefix_eval_mid(const float2* __restrict__ T, float xs) {
-    float t = xs + kRoundMagic;
-    int i = __float_as_int(t) - kRoundMagicBits;
-    float2 e = T[i];
-    return fmaf(e.y, xs - (t - kRoundMagic), e.x);
-}
-
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = a + b;
     float bb = s - a;

@@ -102,7 +102,6 @@ class Workers {
         done_cv_.wait(lk, [this] { return remaining_ == 0 && active_ == 0; });
         job_ = nullptr;
     }
-    int size() const { return (int)threads_.size() + 1; }
 
    private:
     void work() {
