@@ -639,7 +639,8 @@ constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
 // F(x) = entry.x + r_i (x - 1/2 - i) for the cell i nearest x - 1/2.  The
 // nearest integer comes from the float adder (x' + 1.5*2^23 rounds x' to an
 // integer in the low mantissa bits), which keeps the lookup off the
-// conversion pipe.  x' = x - 1/2 must lie in [-1/2, n - 1/2].
+// conversion pipe.  x' = x - 1/2 must lie in [-1/2, n - 1/2] (for the
+// parallel forward projector, that range moved by its even origin h).
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr int kRoundMagicBits = 0x4B400000;
 
