@@ -1571,7 +1571,7 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
 #pragma unroll
             for (int k = 0; k < 5; ++k) {
                 const float rx = fmaf((float)k, drx, rx0), ry = fmaf((float)k, dry, ry0);
-                j[k] = fmaf(atanf(rx / (ry + dso)), jscale, joff);
+                j[k] = fmaf(atanf(__fdividef(rx, ry + dso)), jscale, joff);  // fast divide: a few ulp
             }
             float wgt[4];
 #pragma unroll
@@ -1579,7 +1579,7 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
                 wgt[k] = 1.f;
                 if (fbp) {
                     const float rxc = fmaf((float)k + 0.5f, drx, rx0), ryc = fmaf((float)k + 0.5f, dry, ry0);
-                    wgt[k] = dso2 / (rxc * rxc + (dso + ryc) * (dso + ryc));
+                    wgt[k] = __fdividef(dso2, rxc * rxc + (dso + ryc) * (dso + ryc));
                 }
             }
             float val[S][4];
