@@ -164,22 +164,24 @@ __global__ void __launch_bounds__(256) tomo_bp_kernel(float* __restrict__ img, c
     float y = ((float)iy - (g.ny - 1) / 2.0f) * g.dy + g.cy;
     float z = ((float)iz - (g.nz - 1) / 2.0f) * g.dz + g.cz;
     const float* pb = wprj + (size_t)b * nview * d.nv * d.nu;
+    // fast divides and reciprocals of the cell sizes (a few ulp each)
+    const float idu = 1.f / d.du, idv = 1.f / d.dv;
     float val = 0.f;
     for (int view = 0; view < nview; ++view) {
         float Sx = sr[view * 3], Sy = sr[view * 3 + 1], Sz = sr[view * 3 + 2];
         float Cx = dc[view * 3], Cy = dc[view * 3 + 1], Cz = dc[view * 3 + 2];
-        float r = (Cz - Sz) / (z - Sz);
-        float u1 = (Sx - Cx + r * (x - g.dx / 2 - Sx)) / d.du + d.off_u + (d.nu - 1) / 2.0f;
-        float u2 = (Sx - Cx + r * (x + g.dx / 2 - Sx)) / d.du + d.off_u + (d.nu - 1) / 2.0f;
-        float v1 = (Sy - Cy + r * (y - g.dy / 2 - Sy)) / d.dv + d.off_v + (d.nv - 1) / 2.0f;
-        float v2 = (Sy - Cy + r * (y + g.dy / 2 - Sy)) / d.dv + d.off_v + (d.nv - 1) / 2.0f;
+        float r = __fdividef(Cz - Sz, z - Sz);
+        float u1 = (Sx - Cx + r * (x - g.dx / 2 - Sx)) * idu + d.off_u + (d.nu - 1) / 2.0f;
+        float u2 = (Sx - Cx + r * (x + g.dx / 2 - Sx)) * idu + d.off_u + (d.nu - 1) / 2.0f;
+        float v1 = (Sy - Cy + r * (y - g.dy / 2 - Sy)) * idv + d.off_v + (d.nv - 1) / 2.0f;
+        float v2 = (Sy - Cy + r * (y + g.dy / 2 - Sy)) * idv + d.off_v + (d.nv - 1) / 2.0f;
         const float* pv = pb + (size_t)view * d.nv * d.nu;
         const float w = fabsf(u2 - u1), h = fabsf(v2 - v1);
         float box;
         if (w <= 1.f && h <= 1.f) box = box2d_small<2>(pv, u1, v1, u2, v2, d.nu, d.nv);
         else if (w <= 2.f && h <= 2.f) box = box2d_small<3>(pv, u1, v1, u2, v2, d.nu, d.nv);
         else box = box2d(pv, u1, v1, u2, v2, d.nu, d.nv);
-        val += box / ((u2 - u1) * (v2 - v1));
+        val += __fdividef(box, (u2 - u1) * (v2 - v1));
     }
     float* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
     *o = (accumulate ? *o : 0.f) + val;
