@@ -1758,21 +1758,21 @@ bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
     return nrows * line <= 200 * 1024;
 }
 
-// View group and edge groups per warp (one of the compiled counts) of the
-// streamed forward projector: the most views per CTA whose edge groups fill
-// the 8 warps with the least waste.
-bool fp_stream_shape(const ctp_geometry& g, int& vgroup, int& ni) {
+// View group and edge groups per warp (one of the compiled counts, at most
+// max_ni) of the streamed forward projector: the most views per CTA whose
+// edge groups fill the 8 warps with the least waste.
+bool fp_stream_shape(const ctp_geometry& g, int& vgroup, int& ni, int max_ni = 16) {
     static const int set[4] = {4, 8, 12, 16};
     const int ipv = (int)((g.nu + 30) / 31);
     vgroup = 0;
     ni = 0;
     if (ipv == 0 || g.nview == 0) return false;
     double best = 1e30;
-    for (int v = 1; v * ipv <= set[3] * 8 && v <= (int)g.nview; ++v) {
+    for (int v = 1; v * ipv <= max_ni * 8 && v <= (int)g.nview; ++v) {
         const int per_warp = (v * ipv + 7) / 8;
         int n = 0;
         for (int i = 0; i < 4 && !n; ++i)
-            if (set[i] >= per_warp) n = set[i];
+            if (set[i] >= per_warp && set[i] <= max_ni) n = set[i];
         if (!n) continue;
         const double waste = (double)(n * 8) / (v * ipv) + 0.05 / v;  // prefer more views per table chunk
         if (waste < best) {
@@ -1820,6 +1820,16 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         const int nslices = (int)(g.nbatch * g.nz);
         int sv = 0, ni = 0;
         fp_stream_shape(g, sv, ni);
+        // a grid short of one wave of resident CTAs (few slices) takes smaller
+        // view groups: more CTAs, each streaming the slice's tables
+        int sms = 148, dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        for (int cap = 8; cap >= 4 && ((g.nview + sv - 1) / sv) * (size_t)nslices < 2 * (size_t)sms; cap /= 2) {
+            int sv2 = 0, ni2 = 0;
+            if (!fp_stream_shape(g, sv2, ni2, cap)) break;
+            sv = sv2;
+            ni = ni2;
+        }
         const int rc_s = rchunk;
         size_t shm = 2 * (size_t)rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)nslices);
