@@ -1179,11 +1179,14 @@ inline size_t par_fast_smem(int win, int S) {
 // S slices of the same geometry per CTA: the per-view constants, the edge
 // positions and each lookup's index and fraction are shared; only the table
 // reads and the sums repeat per slice.
+// Views are split over blockIdx.z in parts of vper (a multiple of kPViews)
+// when the tile grid alone leaves SMs idle; part z writes its own partial
+// volume at img + z * part_elems (summed by bp_parts_sum_kernel).
 template <typename Tp, typename Tout, int S>
 __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ prj,
                                                                const float* __restrict__ deg, int nview, Grid g,
                                                                Det d, int fbp, int accumulate, int win,
-                                                               int nslices) {
+                                                               int nslices, int vper, size_t part_elems) {
     extern __shared__ float4 smem_f4[];
     const int stride = win + 1;
     float2* s_tab = reinterpret_cast<float2*>(smem_f4);                       // [S][kPViews][stride]
@@ -1223,8 +1226,10 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
     const size_t vstride = (size_t)d.nv * d.nu;
     const size_t tstride = (size_t)kPViews * stride;  // per slice
 
-    for (int v0 = 0; v0 < nview && any_row; v0 += kPViews) {
-        const int nvc = min(kPViews, nview - v0);
+    img += blockIdx.z * part_elems;
+    const int vb = blockIdx.z * vper, ve = min(nview, vb + vper);
+    for (int v0 = vb; v0 < ve && any_row; v0 += kPViews) {
+        const int nvc = min(kPViews, ve - v0);
         if (threadIdx.x < nvc) {
             const int vi = threadIdx.x, view = v0 + vi;
             double s, c;
@@ -1432,7 +1437,7 @@ template <typename Tp, typename Tout, int S>
 __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ src,
                                                                const float* __restrict__ deg, int nview, Grid g,
                                                                Det d, float dso, int fbp, int accumulate, int win,
-                                                               int nslices) {
+                                                               int nslices, int vper, size_t part_elems) {
     extern __shared__ float4 smem_f4[];
     const int stride = win + 1;
     float2* s_tab = reinterpret_cast<float2*>(smem_f4);                        // [S][kPViews][stride]
@@ -1476,8 +1481,10 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
 #pragma unroll
         for (int k = 0; k < 4; ++k) ax[s][k] = ay[s][k] = 0.f;
 
-    for (int v0 = 0; v0 < nview && any_row; v0 += kPViews) {
-        const int nvc = min(kPViews, nview - v0);
+    img += blockIdx.z * part_elems;
+    const int vb = blockIdx.z * vper, ve = min(nview, vb + vper);
+    for (int v0 = vb; v0 < ve && any_row; v0 += kPViews) {
+        const int nvc = min(kPViews, ve - v0);
         if (threadIdx.x < nvc) {
             const int vi = threadIdx.x, view = v0 + vi;
             double s, c;
@@ -1936,11 +1943,61 @@ int dd2d_nnz(unsigned long long* nnz_host, const float* deg, const ctp_geometry&
 
 namespace {
 
+// Sum of the view parts of a split back projection into the output.
+template <typename Tout>
+__global__ void bp_parts_sum_kernel(Tout* __restrict__ img, const float* __restrict__ parts, int nparts,
+                                    size_t elems, int accumulate) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < elems; i += (size_t)gridDim.x * blockDim.x) {
+        float a = accumulate ? rdf(img + i) : 0.f;
+        for (int q = 0; q < nparts; ++q) a += parts[(size_t)q * elems + i];
+        stf(img + i, a);
+    }
+}
+
+// View parts of a fast back projection whose grid (ctas) leaves SMs idle:
+// enough parts of whole kPViews chunks (at most 8) for about two CTAs per SM.
+// vper receives the views per part.
+int bp_view_parts(size_t ctas, int nview, int& vper) {
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int chunks = (nview + kPViews - 1) / kPViews;
+    if (chunks <= 0) {
+        vper = kPViews;
+        return 1;
+    }
+    int parts = 1;
+    if (ctas > 0 && ctas < (size_t)sms) parts = (int)std::min<size_t>(8, (2 * (size_t)sms + ctas - 1) / ctas);
+    parts = std::max(1, std::min(parts, chunks));
+    vper = ((chunks + parts - 1) / parts) * kPViews;
+    return (nview + vper - 1) / vper;
+}
+
+// CTAs of the fast back-projection grid (0 when the fast path does not apply).
+size_t bp_fast_ctas(const ctp_geometry& g, int geom) {
+    const size_t nslices = g.nbatch * g.nz;
+    const size_t tiles = ((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT);
+    if (geom == 0) {
+        if (fan_fast_window(g) <= 0) return 0;
+        return tiles * ((nslices + (nslices >= 2 ? 1 : 0)) / (nslices >= 2 ? 2 : 1));
+    }
+    if (par_fast_window(g) <= 0) return 0;
+    const size_t S = nslices >= 4 ? 4 : nslices >= 2 ? 2 : 1;
+    return tiles * ((nslices + S - 1) / S);
+}
+
+size_t bp_pre_bytes(const ctp_geometry& g, int geom, int type) {
+    bool fbp = type & (CTP_TYPE_FBP | CTP_TYPE_FORCE_FBP);
+    return (geom == 0 && !fbp) ? align_up(g.nbatch * g.nview * g.nv * g.nu * sizeof(float)) : 0;
+}
+
 size_t bp_workspace(const ctp_geometry& g, int geom, int type, unsigned flags) {
     if (flags & CTP_FLAG_ADJOINT) return align_up(table_floats(g.nview, g.nu) * sizeof(float));
-    bool fbp = type & (CTP_TYPE_FBP | CTP_TYPE_FORCE_FBP);
-    if (geom == 0 && !fbp) return align_up(g.nbatch * g.nview * g.nv * g.nu * sizeof(float));
-    return 0;
+    size_t need = bp_pre_bytes(g, geom, type);
+    const size_t ctas = bp_fast_ctas(g, geom);
+    int vper = 0;
+    const int parts = ctas ? bp_view_parts(ctas, (int)g.nview, vper) : 1;
+    if (parts > 1) need += align_up((size_t)parts * g.nbatch * g.nz * g.ny * g.nx * sizeof(float));
+    return need;
 }
 
 template <typename Tin, typename Tout>
@@ -1983,18 +2040,29 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
         const int nslices = (int)(g.nbatch * g.nz);
         const int FS = nslices >= 2 ? 2 : 1;
         size_t fshm = fan_fast_smem(fwin, FS);
-        dim3 fgrid((unsigned)tiles_f, (unsigned)((nslices + FS - 1) / FS));
-        auto fan_fast = [&](auto k1, auto k2, const auto* srcp, int fbp_mode) {
-            if (FS == 2) {
-                cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
-                k2<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), srcp, deg, nview, gr, dt, dso, fbp_mode, accumulate, fwin,
-                                            nslices);
-            } else {
-                cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
-                k1<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), srcp, deg, nview, gr, dt, dso, fbp_mode, accumulate, fwin,
-                                            nslices);
+        // few tiles and slices: the views split into parts summed at the end
+        int vper = nview;
+        const int parts = fwin > 0 ? bp_view_parts(bp_fast_ctas(g, 0), nview, vper) : 1;
+        const size_t elems = g.nbatch * g.nz * g.ny * g.nx;
+        float* partial = reinterpret_cast<float*>(ws + bp_pre_bytes(g, geom, type));
+        dim3 fgrid((unsigned)tiles_f, (unsigned)((nslices + FS - 1) / FS), (unsigned)parts);
+        auto fan_fast = [&](auto k1, auto k2, auto kp1, auto kp2, const auto* srcp, int fbp_mode) {
+            if (parts == 1) {
+                auto k = FS == 2 ? k2 : k1;
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
+                k<<<fgrid, 256, fshm, s>>>(mptr<Tout>(img), srcp, deg, nview, gr, dt, dso, fbp_mode, accumulate, fwin,
+                                           nslices, nview, (size_t)0);
+                return check_launch("dd2d_bp_fan_fast_kernel");
             }
-            return check_launch("dd2d_bp_fan_fast_kernel");
+            auto k = FS == 2 ? kp2 : kp1;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fshm);
+            k<<<fgrid, 256, fshm, s>>>(partial, srcp, deg, nview, gr, dt, dso, fbp_mode, 0, fwin, nslices, vper,
+                                       elems);
+            int r = check_launch("dd2d_bp_fan_fast_kernel");
+            if (r) return r;
+            bp_parts_sum_kernel<Tout><<<(unsigned)std::min<size_t>((elems + 255) / 256, 148 * 8), 256, 0, s>>>(
+                mptr<Tout>(img), partial, parts, elems, accumulate);
+            return check_launch("bp_parts_sum_kernel");
         };
         if (fwin > 0 && !fbp) {
             float* wprj = reinterpret_cast<float*>(ws);
@@ -2003,10 +2071,12 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
                                                                                     nview, dt, gr, total);
             if ((rc = check_launch("fan_preweight_kernel"))) return rc;
             return fan_fast(dd2d_bp_fan_fast_kernel<float, Tout, 1>, dd2d_bp_fan_fast_kernel<float, Tout, 2>,
+                            dd2d_bp_fan_fast_kernel<float, float, 1>, dd2d_bp_fan_fast_kernel<float, float, 2>,
                             (const float*)wprj, 0);
         }
         if (fwin > 0)
             return fan_fast(dd2d_bp_fan_fast_kernel<Tin, Tout, 1>, dd2d_bp_fan_fast_kernel<Tin, Tout, 2>,
+                            dd2d_bp_fan_fast_kernel<Tin, float, 1>, dd2d_bp_fan_fast_kernel<Tin, float, 2>,
                             cptr<Tin>(prj), 1);
         if (!fbp) {
             float* wprj = reinterpret_cast<float*>(ws);
@@ -2030,24 +2100,31 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
             const int nslices = (int)(g.nbatch * g.nz);
             const int S = nslices >= 4 ? 4 : nslices >= 2 ? 2 : 1;
             size_t pshm = par_fast_smem(pwin, S);
-            dim3 pg((unsigned)tiles_p, (unsigned)((nslices + S - 1) / S));
-            if (S == 4) {
-                auto kf = dd2d_bp_par_fast_kernel<Tin, Tout, 4>;
-                cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
-                kf<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin,
-                                         nslices);
-            } else if (S == 2) {
-                auto kf = dd2d_bp_par_fast_kernel<Tin, Tout, 2>;
-                cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
-                kf<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin,
-                                         nslices);
-            } else {
-                auto kf = dd2d_bp_par_fast_kernel<Tin, Tout, 1>;
-                cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
-                kf<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate, pwin,
-                                         nslices);
-            }
-            return check_launch("dd2d_bp_par_fast_kernel");
+            // few tiles and slices: the views split into parts summed at the end
+            int vper = nview;
+            const int parts = bp_view_parts(bp_fast_ctas(g, 1), nview, vper);
+            const size_t elems = g.nbatch * g.nz * g.ny * g.nx;
+            float* partial = reinterpret_cast<float*>(ws + bp_pre_bytes(g, geom, type));
+            dim3 pg((unsigned)tiles_p, (unsigned)((nslices + S - 1) / S), (unsigned)parts);
+            auto par_fast = [&](auto kout, auto kpart) {
+                if (parts == 1) {
+                    cudaFuncSetAttribute(kout, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
+                    kout<<<pg, 256, pshm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, fbp, accumulate,
+                                               pwin, nslices, nview, (size_t)0);
+                    return check_launch("dd2d_bp_par_fast_kernel");
+                }
+                cudaFuncSetAttribute(kpart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pshm);
+                kpart<<<pg, 256, pshm, s>>>(partial, cptr<Tin>(prj), deg, nview, gr, dt, fbp, 0, pwin, nslices, vper,
+                                            elems);
+                int r = check_launch("dd2d_bp_par_fast_kernel");
+                if (r) return r;
+                bp_parts_sum_kernel<Tout><<<(unsigned)std::min<size_t>((elems + 255) / 256, 148 * 8), 256, 0, s>>>(
+                    mptr<Tout>(img), partial, parts, elems, accumulate);
+                return check_launch("bp_parts_sum_kernel");
+            };
+            if (S == 4) return par_fast(dd2d_bp_par_fast_kernel<Tin, Tout, 4>, dd2d_bp_par_fast_kernel<Tin, float, 4>);
+            if (S == 2) return par_fast(dd2d_bp_par_fast_kernel<Tin, Tout, 2>, dd2d_bp_par_fast_kernel<Tin, float, 2>);
+            return par_fast(dd2d_bp_par_fast_kernel<Tin, Tout, 1>, dd2d_bp_par_fast_kernel<Tin, float, 1>);
         }
         auto k = dd2d_bp_parity_kernel<false, Tin, Tout>;
         k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, fbp,
