@@ -6,7 +6,7 @@ its host-pointer C entries with the argument conventions of its numpy
 wrappers (ct_projector/projector/numpy/*.py), on the seeded cases of
 cases.py, and stores inputs and outputs.  Needs a GPU:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py [--out DIR] [--only CASE ...]   # default: tests/golden
 
 This script is test infrastructure; the product never runs the reference.
 """
@@ -207,7 +207,7 @@ def run_case(ref: Ref, fn):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--only", nargs="*", default=None, help="case names to (re)generate")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
