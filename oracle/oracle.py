@@ -1,8 +1,8 @@
 """CPU FP64 oracle for the CTProjector projector pair.
 
 TEST INFRASTRUCTURE ONLY.  The parity tests, ``__graft_entry__.smoke()`` and
-the ``cpu_baseline`` leg of ``bench.py`` use this module as the checker; the
-``ctprojector_b200`` product never imports it.
+the ``cpu_baseline`` leg of ``bench.py`` use this module to check results and
+to time the CPU baseline; the ``ctprojector_b200`` product never imports it.
 
 The distance-driven, Siddon, tomosynthesis and ``fbp_bp`` operators are the C
 restatement in ``ctp_oracle.c`` (FP64, OpenMP).  The ramp filter is restated
