@@ -173,8 +173,10 @@ __device__ __forceinline__ void walk(const Ray& R, const Grid& g, F&& emit) {
     walk_strided<IdxT>(R, g, (IdxT)1, (IdxT)g.nx, (IdxT)g.nx * g.ny, emit);
 }
 
+// Five CTAs per SM (48 registers): the walk is latency-bound on its
+// dependent loads, and the extra warps hide ~1% more of it.
 template <typename Tin, typename Tout, typename IdxT>
-__global__ void __launch_bounds__(256) siddon_fp_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
+__global__ void __launch_bounds__(256, 5) siddon_fp_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
                                                         const float* __restrict__ dc, const float* __restrict__ du_,
                                                         const float* __restrict__ dv_, const float* __restrict__ sr,
                                                         int nview, Grid g, Det d, int accumulate) {
