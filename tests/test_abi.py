@@ -81,6 +81,21 @@ def test_workspace_queries_need_no_gpu():
     assert lib().ctp_tomo_bp_workspace(ctypes.byref(g)) >= 16 * 720 * 768 * 4
 
 
+def test_bp_workspace_holds_view_parts():
+    """One 256 x 256 fan slice gives the fast back projector 64 tiles, fewer
+    than the SMs, so its views are split into parts with FP32 partial
+    volumes in the workspace (besides the pre-weighted sinogram); the
+    16-slice batch needs no parts."""
+    from ctprojector_b200._lib import Geometry, lib
+
+    da = 1.2858 / 1085.6
+    one = Geometry(1, 256, 256, 1, 1.0, 1.0, 1, 0, 0, 0, 736, 1, 360, da, 1, 0, 0, 1085.6, 595.0)
+    stack = Geometry(16, 256, 256, 1, 1.0, 1.0, 1, 0, 0, 0, 736, 1, 360, da, 1, 0, 0, 1085.6, 595.0)
+    pre = 360 * 736 * 4
+    assert lib().ctp_dd2d_bp_workspace(ctypes.byref(one), 0, 0, 0) >= pre + 2 * 256 * 256 * 4
+    assert lib().ctp_dd2d_bp_workspace(ctypes.byref(stack), 0, 0, 0) < 16 * pre + 4096
+
+
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     import ctprojector_b200._lib as L
     from ctprojector_b200.errors import CTProjectorError
