@@ -53,6 +53,8 @@ struct DDTab {
     const float* eB[2];  // [nview][nu+1] edge slope per row/col
     const float* cL[2];  // [nview][nu] ray length factor dy/|cos| or dx/|sin|
     const float* wx;     // [nview] blend weight of the row (y main axis) sweep
+    const float* sP[2];  // [nview] fan source: position across the lines
+    const float* sS[2];  // [nview] fan source: line coordinate from the anchor line's centre
     int ym, xm;          // anchor row / column
 };
 
@@ -61,9 +63,11 @@ struct DDTabW {
     float* eB[2];
     float* cL[2];
     float* wx;
+    float* sP[2];
+    float* sS[2];
 };
 
-size_t table_floats(size_t nview, size_t nu) { return 2 * (2 * nview * (nu + 1) + nview * nu) + nview; }
+size_t table_floats(size_t nview, size_t nu) { return 2 * (2 * nview * (nu + 1) + nview * nu) + 5 * nview; }
 
 // Table carve-out in a float buffer; the same layout for readers and writers.
 void carve_table(float* base, size_t nview, size_t nu, DDTabW& w) {
@@ -74,7 +78,11 @@ void carve_table(float* base, size_t nview, size_t nu, DDTabW& w) {
         w.eB[o] = p; p += ne;
         w.cL[o] = p; p += nc;
     }
-    w.wx = p;
+    w.wx = p; p += nview;
+    for (int o = 0; o < 2; ++o) {
+        w.sP[o] = p; p += nview;
+        w.sS[o] = p; p += nview;
+    }
 }
 
 DDTab as_read(const DDTabW& w, int ym, int xm) {
@@ -82,6 +90,7 @@ DDTab as_read(const DDTabW& w, int ym, int xm) {
     for (int o = 0; o < 2; ++o) {
         t.eA[o] = w.eA[o]; t.eB[o] = w.eB[o];
         t.cL[o] = w.cL[o];
+        t.sP[o] = w.sP[o]; t.sS[o] = w.sS[o];
     }
     t.wx = w.wx;
     t.ym = ym;
@@ -152,6 +161,12 @@ __global__ void dd_table_kernel(DDTabW t, const float* __restrict__ deg, int nvi
         sincos(th, &s, &c);
         double r = (fabs(c) - fabs(s) + kDDMarginD) / (2 * kDDMarginD);
         t.wx[view] = (float)(r < 0 ? 0.0 : (r > 1 ? 1.0 : r));
+        // fan source in line coordinates: edge j sits at sP + eB_j (t - sS) on
+        // line t (counted from the anchor line)
+        t.sP[0][view] = (float)sx;
+        t.sS[0][view] = (float)(sy - ym - 0.5);
+        t.sP[1][view] = (float)sy;
+        t.sS[1][view] = (float)(sx - xm - 0.5);
     }
 }
 
@@ -622,161 +637,109 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
 // A CTA owns a group of views of one slice and streams the image through
 // shared memory a few lines at a time (rows of the image for the views traced
 // along y, rows of the transposed image for those traced along x).  Each staged
-// line is stored as its running integral F (double-float (hi, lo) for fan
-// beams, FP64 for parallel beams) plus the pixel value r, so the integral of
-// the line over [a, b] is F(b) - F(a) with no cancellation.  Detector cells
-// share their edges, so each lane of a warp evaluates F at one edge (x = A + B t
-// from the FP64 edge table): 31 rays per warp, one table read per ray and
-// line.  Fan beams take the neighbour edge's value with a shuffle and divide
-// by the footprint width on every line; parallel beams, whose width is the
-// same on every line, sum F per edge and difference once (fp_line).  The
-// normalisation by the footprint width, the ray-length factor and the blend
-// weight are those of DDFPTracing (distanceDriven2DBoxInt.cu:21-106).
-constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
+// line is stored as its running integral F in FP64 plus the pixel value r, so
+// the integral of the line over [a, b] is F(b) - F(a) with no cancellation.
+// Detector cells share their edges, so each lane of a warp evaluates F at one
+// edge: 31 rays per warp, one table read per ray and line.  On every line the
+// footprint of a cell is the same multiple of one per-ray constant (parallel
+// beams: the width itself; fan beams: the slope difference of the two edge
+// rays times the line's distance tau from the source), so each lane sums F at
+// its own edge over the lines, weighted by 1/tau for fan beams, and the cell
+// is the difference of two neighbouring sums taken once, after the last line:
+// no shuffle or divide per line (fp_line).  The normalisation by the
+// footprint width, the ray-length factor and the blend weight are those of
+// DDFPTracing (distanceDriven2DBoxInt.cu:21-106).
+constexpr int kFMaxItems = 16;     // edge groups (of 32 edges) per warp
+constexpr int kFMaxItemsFan = 8;   // fan beams (one more register per group): 3 CTAs per SM, no spills
 
 // Running integral at x' + 1/2 from a midpoint table: entry i holds
 // (C_i + r_i / 2, r_i) with C_i the integral up to cell i, so
 // F(x) = entry.x + r_i (x - 1/2 - i) for the cell i nearest x - 1/2.  The
 // nearest integer comes from the float adder (x' + 1.5*2^23 rounds x' to an
 // integer in the low mantissa bits), which keeps the lookup off the
-// conversion pipe.  x' = x - 1/2 must lie in [-1/2, n - 1/2] (for the
-// parallel forward projector, that range moved by its even origin h).
+// conversion pipe.  x' = x - 1/2 must lie in [-1/2, n - 1/2], moved by the
+// origin h of the positions (fp_origin).
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr int kRoundMagicBits = 0x4B400000;
 
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-    s = a + b;
-    float bb = s - a;
-    e = (a - (s - bb)) + (b - bb);
+// Approximate reciprocal (the PTX rcp.approx instruction, flushing
+// subnormals): one instruction, relative error about 1 ulp.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
-// One image line's contribution to a thread's NI edge groups (edge position
-// minus 1/2 on line t: x = A + B t, clamped to [lo_lim, hi_lim]; T the
-// line's midpoint table).
-//   FAN: acc += (F(x_j+1) - F(x_j)) / (x_j+1 - x_j), the neighbour edge taken
-//        from the next lane (the footprint width changes from line to line);
-//        double-float table entries {hi, lo, r, 0}.
-//   parallel: every edge of a view has the same slope, so the width is the
-//        same on every line; each lane sums F at its own edge over the lines
-//        and the cell difference is taken once, after the last line
-//        (fp_cell_sum): no shuffle or divide per line.  The table entries
-//        hold C + r/2 as an FP64 value {lo word, hi word, r, 0}, summed in
-//        FP64 (accd); the small r * frac parts go to an FP32 sum (alo) that
-//        is folded into accd every 16 lines.  Positions are measured from
-//        the middle of the line (T points at the middle entry) so that their
-//        FP32 rounding is half as large.
+// One image line's contribution to a thread's NI edge groups.  T is the
+// line's midpoint table (FP64 entries {C + r/2 as the low and high words of a
+// double, r, 0}, pointing at the origin entry h), t the line's coordinate
+// from the anchor line, positions clamped to [lo_lim, hi_lim].
+//   parallel: edge position A + B t, the same slope B for every edge of a
+//        view, so a cell's footprint has the same width on every line; the
+//        lane adds F at its edge (accd += entry in FP64, the small r * frac
+//        part in FP32 in alo, folded into accd every 16 lines).
+//   FAN: edge position A + B tau with A, S the source's position and line
+//        coordinate and tau = t - S the line's distance from the source
+//        (the same for every edge of the view), so the footprint between
+//        edges j and j+1 is (B_j+1 - B_j) tau wide; the lane adds F / tau
+//        (the FP32 weight 1/tau is common to the cell's two edges, so its
+//        rounding only reweights the line).
+// Positions are measured from the middle of the line so that their FP32
+// rounding is half as large.
 template <bool FAN, int NI>
 __device__ __forceinline__ void fp_line(const float4* __restrict__ T, float t, float lo_lim, float hi_lim,
-                                        const float (&A)[NI], const float (&B)[NI], float (&acc)[NI],
+                                        const float (&A)[NI], const float (&B)[NI], const float (&S)[NI],
                                         double (&accd)[NI], float (&alo)[NI]) {
 #pragma unroll
     for (int q = 0; q < NI; ++q) {
-        const float xr = fmaf(B[q], t, A[q]);
+        float tau = t, wgt = 1.f;
+        if constexpr (FAN) {
+            tau = t - S[q];  // |tau| >= 1/2 (dummies) or the source's distance
+            wgt = rcp_approx(tau);
+        }
+        const float xr = fmaf(B[q], tau, A[q]);
         const float xs = clampf(xr, lo_lim, hi_lim);
         const float tt = xs + kRoundMagic;
         const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
         const float frac = xs - (tt - kRoundMagic);
+        const double F = __hiloint2double(__float_as_int(e.y), __float_as_int(e.x));
         if constexpr (FAN) {
-            const float hi = e.x, lo = fmaf(e.z, frac, e.y);
-            const float hin = __shfl_down_sync(0xffffffffu, hi, 1);
-            const float lon = __shfl_down_sync(0xffffffffu, lo, 1);
-            const float xn = __shfl_down_sync(0xffffffffu, xr, 1);
-            // signed integral over [x_j, x_j+1] over the signed width of the
-            // rounded footprint
-            acc[q] += __fdividef((hin - hi) + (lon - lo), xn - xr);
+            accd[q] = fma((double)wgt, F, accd[q]);
+            alo[q] = fmaf(wgt * e.z, frac, alo[q]);
         } else {
-            accd[q] += __hiloint2double(__float_as_int(e.y), __float_as_int(e.x));
+            accd[q] += F;
             alo[q] = fmaf(e.z, frac, alo[q]);
         }
     }
 }
 
-// Parallel sums: fold the FP32 part (at most 16 lines of r * frac) into the
-// FP64 sum.
-template <bool FAN, int NI>
+// Fold the FP32 parts (at most 16 lines of r * frac) into the FP64 sums.
+template <int NI>
 __device__ __forceinline__ void fp_renorm(double (&accd)[NI], float (&alo)[NI]) {
-    if constexpr (!FAN) {
 #pragma unroll
-        for (int q = 0; q < NI; ++q) {
-            accd[q] += (double)alo[q];
-            alo[q] = 0.f;
-        }
+    for (int q = 0; q < NI; ++q) {
+        accd[q] += (double)alo[q];
+        alo[q] = 0.f;
     }
 }
 
 // Sum over lines of the cell integral over the footprint width, for the cell
-// between this lane's edge and the next lane's (all lanes call it; parallel
-// sums renormalised first).
-template <bool FAN>
-__device__ __forceinline__ float fp_cell_sum(float acc, double accd, float A) {
-    if constexpr (FAN) {
-        return acc;
-    } else {
-        const double dn = __shfl_down_sync(0xffffffffu, accd, 1);
-        const float An = __shfl_down_sync(0xffffffffu, A, 1);
-        return __fdividef((float)(dn - accd), An - A);
-    }
+// between this lane's edge and the next lane's (all lanes call it, sums
+// renormalised first): the difference of the two edge sums over the
+// difference of W, the edge's position at the anchor line (parallel) or its
+// slope (fan).
+__device__ __forceinline__ float fp_cell_sum(double accd, float W) {
+    const double dn = __shfl_down_sync(0xffffffffu, accd, 1);
+    const float Wn = __shfl_down_sync(0xffffffffu, W, 1);
+    return __fdividef((float)(dn - accd), Wn - W);
 }
 
 // Offset of the position origin from the start of a line of n cells: the
-// middle entry for the parallel sums, the start for fan beams.  Even, so that
-// the clamped ends -h - 1/2 and n - h - 1/2 round (half to even) onto table
-// entries 0 and n or n - 1.
-template <bool FAN>
-__device__ __forceinline__ int fp_origin(int n) { return FAN ? 0 : (n >> 1) & ~1; }
+// middle entry.  Even, so that the clamped ends -h - 1/2 and n - h - 1/2
+// round (half to even) onto table entries 0 and n or n - 1.
+__device__ __forceinline__ int fp_origin(int n) { return (n >> 1) & ~1; }
 
-// Midpoint table of one line of n cells, built by one warp: n+1 entries
-// {hi, lo, r, 0} with hi + lo = integral over cells [0, i) plus r_i / 2 in
-// double-float form and r_i the cell value (0 past the end).
-template <typename Tin>
-__device__ __forceinline__ void stage_line(float4* __restrict__ T, const Tin* __restrict__ row, int n, int lane) {
-    const int E = (n + 1 + 31) / 32;
-    const int k0 = lane * E;
-    // lane total as a double-float
-    float hi = 0.f, lo = 0.f;
-    for (int q = 0; q < E; ++q) {
-        int k = k0 + q;
-        if (k < n) {
-            float e;
-            two_sum(hi, ldf(row + k), hi, e);
-            lo += e;
-        }
-    }
-    // exclusive scan of (hi, lo) across the warp
-    float ihi = hi, ilo = lo;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        float th = __shfl_up_sync(0xffffffffu, ihi, o), tl = __shfl_up_sync(0xffffffffu, ilo, o);
-        if (lane >= o) {
-            float sh, e;
-            two_sum(ihi, th, sh, e);
-            float sl = ilo + tl + e;
-            ihi = sh + sl;
-            ilo = sl - (ihi - sh);
-        }
-    }
-    float bhi, blo;
-    {
-        float e;
-        two_sum(ihi, -hi, bhi, e);
-        blo = ilo - lo + e;
-        float t = bhi + blo;
-        blo = blo - (t - bhi);
-        bhi = t;
-    }
-    for (int q = 0; q < E; ++q) {
-        int k = k0 + q;
-        if (k <= n) {
-            float r = k < n ? ldf(row + k) : 0.f;
-            T[k] = make_float4(bhi, fmaf(0.5f, r, blo), r, 0.f);  // midpoint table
-            float e;
-            two_sum(bhi, r, bhi, e);
-            blo += e;
-        }
-    }
-}
-
-// FP64 midpoint table of one line (the parallel-beam sums): n+1 entries
+// FP64 midpoint table of one line, built by one warp: n+1 entries
 // {C_i + r_i/2 as the low and high words of a double, r_i, 0} with C_i the
 // integral over cells [0, i) and r_i the cell value (0 past the end).
 template <typename Tin>
@@ -808,37 +771,32 @@ __device__ __forceinline__ void stage_line_fp64(float4* __restrict__ T, const Ti
 }
 
 // Stage lines (length n, stride n between lines) into consecutive tables.
-template <typename Tin, bool FP64>
+template <typename Tin>
 __device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ src, int nlines, int n, int warp,
                             int lane, int nwarps) {
-    for (int l = warp; l < nlines; l += nwarps) {
-        if constexpr (FP64) stage_line_fp64(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
-        else stage_line(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
-    }
+    for (int l = warp; l < nlines; l += nwarps)
+        stage_line_fp64(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
 }
 
 // The tables of every line of a stack of slices (one warp per line), for the
-// forward projector that streams them into shared memory; FP64 entries for
-// parallel beams.
-template <typename Tin, bool FP64>
+// forward projector that streams them into shared memory.
+template <typename Tin>
 __global__ void __launch_bounds__(256) line_tables_kernel(float4* __restrict__ out, const Tin* __restrict__ src,
                                                           long long nlines, int n) {
     const int lane = threadIdx.x & 31;
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long l = w0; l < nlines; l += nw) {
-        if constexpr (FP64) stage_line_fp64(out + l * (n + 1), src + l * n, n, lane);
-        else stage_line(out + l * (n + 1), src + l * n, n, lane);
-    }
+    for (long long l = w0; l < nlines; l += nw) stage_line_fp64(out + l * (n + 1), src + l * n, n, lane);
 }
 
 // NI = edge groups per warp (compile time, so the group loop is straight-line
 // code with independent dependency chains); groups beyond the CTA's views are
 // harmless dummies whose results are dropped.
-// Parallel beams hold four registers per edge group (position, slope and the
-// double-float sum): above 4 groups per warp they run two CTAs per SM.
+// An edge group holds five registers (position, slope, the FP64 sum and its
+// FP32 part; fan beams add the source's line coordinate): above 4 groups per
+// warp the staged kernel runs two CTAs per SM.
 template <bool FAN, int NI>
-constexpr int fp_fast_min_blocks() { return FAN || NI <= 4 ? 3 : 2; }
+constexpr int fp_fast_min_blocks() { return NI <= 4 ? 3 : 2; }
 
 template <bool FAN, int NI, typename Tin, typename Tout>
 __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
@@ -859,18 +817,18 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
         const int nl = o == 0 ? g.ny : g.nx;  // lines
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const Tin* src = (o == 0 ? img : imgT) + (size_t)slice * g.nx * g.ny;
-        float A[NI], B[NI], acc[NI], alo[NI];
+        float A[NI], B[NI], S[NI], alo[NI];
         double accd[NI];
         bool any = false;
-        const int h = fp_origin<FAN>(n);
+        const int h = fp_origin(n);
         const float shift = 0.5f + (float)h;  // midpoint tables, origin at entry h
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
             const int it = warp + 8 * q;
-            // dummy edge positions keep every width non-zero
+            // dummy edges (results dropped): positions in range, tau never 0
             A[q] = (float)lane - shift;
             B[q] = 0.f;
-            acc[q] = 0.f;
+            S[q] = 0.5f;
             accd[q] = 0.0;
             alo[q] = 0.f;
             if (it < nitems) {
@@ -881,8 +839,9 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
                 const int j = 31 * m + lane;
                 if (active && j <= d.nu) {
                     const size_t ie = (size_t)view * (d.nu + 1) + j;
-                    A[q] = tab.eA[o][ie] - shift;
+                    A[q] = (FAN ? tab.sP[o][view] : tab.eA[o][ie]) - shift;
                     B[q] = tab.eB[o][ie];
+                    if (FAN) S[q] = tab.sS[o][view];
                     any = true;
                 }
             }
@@ -894,19 +853,19 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
         for (int l0 = 0, c = 0; l0 < nl; l0 += nrows_chunk, ++c) {
             const int nlc = min(nrows_chunk, nl - l0);
             __syncthreads();
-            stage_lines<Tin, !FAN>(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
+            stage_lines<Tin>(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
             __syncthreads();
             for (int r = 0; r < nlc; ++r)
                 fp_line<FAN, NI>(s_lines + (size_t)r * (n + 1) + h, (float)(l0 + r - anchor), lo_lim, hi_lim, A, B,
-                                 acc, accd, alo);
-            if ((c + 1) % renorm == 0) fp_renorm<FAN, NI>(accd, alo);
+                                 S, accd, alo);
+            if ((c + 1) % renorm == 0) fp_renorm<NI>(accd, alo);
         }
-        fp_renorm<FAN, NI>(accd, alo);
+        fp_renorm<NI>(accd, alo);
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
             const int it = warp + 8 * q;
             if (it >= nitems) continue;
-            const float sum = fp_cell_sum<FAN>(acc[q], accd[q], A[q]);
+            const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]);
             const int vi = it / ipv, m = it - vi * ipv;
             const int view = v0 + vi;
             const int k = 31 * m + lane;
@@ -987,10 +946,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     return false;
 }
 
-// Parallel beams above 8 edge groups per warp (four registers per group) run
-// two CTAs per SM.
+// Above 8 edge groups per warp (five or six registers per group) two CTAs
+// per SM.
 template <bool FAN, int NI>
-constexpr int fp_stream_min_blocks() { return FAN || NI <= 8 ? 3 : 2; }
+constexpr int fp_stream_min_blocks() { return NI <= 8 ? 3 : 2; }
 
 template <bool FAN, int NI, typename Tout>
 __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
@@ -1046,7 +1005,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
     }
 
     // per edge group: edge position and slope, and the sums of fp_line
-    float A[NI], B[NI], acc[NI], alo[NI];
+    float A[NI], B[NI], S[NI], alo[NI];
     double accd[NI];
     const int renorm = max(1, 16 / rchunk);  // chunks between renormalisations of (acc, alo)
     bool failed = false;
@@ -1056,16 +1015,16 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         const int c = o == 0 ? k : k - nc0;
         const int n = o == 0 ? g.nx : g.ny, nl = o == 0 ? g.ny : g.nx;
         const int last = (o == 0 ? nc0 : nc1) - 1;
-        const int h = fp_origin<FAN>(n);
+        const int h = fp_origin(n);
         const float shift = 0.5f + (float)h;  // midpoint tables, origin at entry h
         if (c == 0) {
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
                 const int it = warp + 8 * q;
-                // dummy edge positions keep every width non-zero
+                // dummy edges (results dropped): positions in range, tau never 0
                 A[q] = (float)lane - shift;
                 B[q] = 0.f;
-                acc[q] = 0.f;
+                S[q] = 0.5f;
                 accd[q] = 0.0;
                 alo[q] = 0.f;
                 if (it < nitems) {
@@ -1076,8 +1035,9 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
                     const int j = 31 * m + lane;
                     if (active && j <= d.nu) {
                         const size_t ie = (size_t)view * (d.nu + 1) + j;
-                        A[q] = tab.eA[o][ie] - shift;
+                        A[q] = (FAN ? tab.sP[o][view] : tab.eA[o][ie]) - shift;
                         B[q] = tab.eB[o][ie];
+                        if (FAN) S[q] = tab.sS[o][view];
                     }
                 }
             }
@@ -1088,16 +1048,16 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
         const float lo_lim = -shift, hi_lim = (float)n - shift;
-        for (int r = 0; r < nlc && !failed; ++r)
-            fp_line<FAN, NI>(buf + (size_t)r * (n + 1) + h, (float)(l0 + r - anchor), lo_lim, hi_lim, A, B, acc, accd,
-                             alo);
-        if ((c + 1) % renorm == 0 || c == last) fp_renorm<FAN, NI>(accd, alo);
+        float tl = (float)(l0 - anchor);  // line coordinate, stepped exactly
+        for (int r = 0; r < nlc && !failed; ++r, tl += 1.f)
+            fp_line<FAN, NI>(buf + (size_t)r * (n + 1) + h, tl, lo_lim, hi_lim, A, B, S, accd, alo);
+        if ((c + 1) % renorm == 0 || c == last) fp_renorm<NI>(accd, alo);
         if (c == last && !failed) {
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
                 const int it = warp + 8 * q;
                 if (it >= nitems) continue;
-                const float sum = fp_cell_sum<FAN>(acc[q], accd[q], A[q]);
+                const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]);
                 const int vi = it / ipv, m = it - vi * ipv;
                 const int view = v0 + vi;
                 const int kk = 31 * m + lane;
@@ -1804,29 +1764,27 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
     int vgroup = 0, nrows = 0;
     const int rchunk = fp_stream_chunk(g);
+    // views per CTA and edge groups per warp (at most 8 for fan beams, whose
+    // groups hold one register more)
+    int sv = 0, ni = 0;
+    const bool shaped =
+        fp_fast_ok(g, vgroup, nrows) && fp_stream_shape(g, sv, ni, geom == 0 ? kFMaxItemsFan : kFMaxItems);
     // the streamed path is the faster one from a single slice up (the tables
     // are built once per slice instead of once per view group); a workspace
     // without room for the line tables runs the staged kernel
-    if (fp_fast_ok(g, vgroup, nrows) && rchunk > 0 && ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
+    if (shaped && rchunk > 0 && ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
         // streamed path: line tables of rows (from the image) and columns (from its transpose)
         float4* lt0 = reinterpret_cast<float4*>(ws + fp_workspace_min(g));
         float4* lt1 = lt0 + g.nbatch * g.nz * g.ny * (g.nx + 1);
         long long rows = (long long)(g.nbatch * g.nz * g.ny), cols = (long long)(g.nbatch * g.nz * g.nx);
         const unsigned rgrid = (unsigned)std::min<long long>((rows + 7) / 8, 148 * 16);
         const unsigned cgrid = (unsigned)std::min<long long>((cols + 7) / 8, 148 * 16);
-        if (geom == 0) {
-            line_tables_kernel<Tin, false><<<rgrid, 256, 0, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
-            line_tables_kernel<Tin, false><<<cgrid, 256, 0, s>>>(lt1, imgT, cols, (int)g.ny);
-        } else {
-            line_tables_kernel<Tin, true><<<rgrid, 256, 0, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
-            line_tables_kernel<Tin, true><<<cgrid, 256, 0, s>>>(lt1, imgT, cols, (int)g.ny);
-        }
+        line_tables_kernel<Tin><<<rgrid, 256, 0, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
+        line_tables_kernel<Tin><<<cgrid, 256, 0, s>>>(lt1, imgT, cols, (int)g.ny);
         if ((rc = check_launch("line_tables_kernel"))) return rc;
         // one slice per CTA (sharing the edge work across two slices halves the
         // lines per table chunk, and the warps then wait on the copies instead)
         const int nslices = (int)(g.nbatch * g.nz);
-        int sv = 0, ni = 0;
-        fp_stream_shape(g, sv, ni);
         // a grid short of one wave of resident CTAs (few slices) takes smaller
         // view groups: more CTAs, each streaming the slice's tables
         int sms = 148, dev = 0;
@@ -1852,32 +1810,29 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     else launch(dd2d_fp_stream_kernel<false, NI_, Tout>)
         if (ni == 4) { CTP_FP_STREAM(4); }
         else if (ni == 8) { CTP_FP_STREAM(8); }
-        else if (ni == 12) { CTP_FP_STREAM(12); }
-        else { CTP_FP_STREAM(16); }
+        else if (ni == 12) launch(dd2d_fp_stream_kernel<false, 12, Tout>);  // fan beams stop at 8
+        else launch(dd2d_fp_stream_kernel<false, 16, Tout>);
 #undef CTP_FP_STREAM
         return check_launch("dd2d_fp_stream_kernel");
     }
-    if (fp_fast_ok(g, vgroup, nrows)) {
+    if (shaped) {
         size_t shm = (size_t)nrows * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
-        dim3 fg((unsigned)((g.nview + vgroup - 1) / vgroup), (unsigned)(g.nbatch * g.nz));
-        int ipv = (int)((g.nu + 30) / 31);
-        int per_warp = (vgroup * ipv + 7) / 8;
+        dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)(g.nbatch * g.nz));
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
             cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g),
-                                      (int)g.nview, vgroup, nrows, deg, unweight);
+                                      (int)g.nview, sv, nrows, deg, unweight);
         };
-        bool fan = geom == 0;
-        if (per_warp <= 4) {
-            if (fan) launch(dd2d_fp_fast_kernel<true, 4, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 4, Tin, Tout>);
-        } else if (per_warp <= 8) {
-            if (fan) launch(dd2d_fp_fast_kernel<true, 8, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 8, Tin, Tout>);
-        } else if (per_warp <= 12) {
-            if (fan) launch(dd2d_fp_fast_kernel<true, 12, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 12, Tin, Tout>);
-        } else {
-            if (fan) launch(dd2d_fp_fast_kernel<true, 16, Tin, Tout>); else launch(dd2d_fp_fast_kernel<false, 16, Tin, Tout>);
-        }
+        const bool fan = geom == 0;
+#define CTP_FP_STAGED(NI_)                                                       \
+    if (fan) launch(dd2d_fp_fast_kernel<true, NI_, Tin, Tout>);                  \
+    else launch(dd2d_fp_fast_kernel<false, NI_, Tin, Tout>)
+        if (ni == 4) { CTP_FP_STAGED(4); }
+        else if (ni == 8) { CTP_FP_STAGED(8); }
+        else if (ni == 12) launch(dd2d_fp_fast_kernel<false, 12, Tin, Tout>);  // fan beams stop at 8
+        else launch(dd2d_fp_fast_kernel<false, 16, Tin, Tout>);
+#undef CTP_FP_STAGED
         return check_launch("dd2d_fp_fast_kernel");
     }
     dim3 grid((unsigned)((g.nu + kFPThreads - 1) / kFPThreads), (unsigned)g.nview, (unsigned)(g.nbatch * g.nv));
