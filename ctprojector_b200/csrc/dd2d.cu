@@ -685,17 +685,28 @@ __device__ __forceinline__ float rcp_approx(float x) {
 //        (the FP32 weight 1/tau is common to the cell's two edges, so its
 //        rounding only reweights the line).
 // Positions are measured from the middle of the line so that their FP32
-// rounding is half as large.
-template <bool FAN, int NI>
+// rounding is half as large.  ONEV (fan beams, one view per CTA): every edge
+// group of the warp belongs to the same view (dummy groups past the view
+// included, whose results are dropped), so tau and its weight are computed
+// once per line from group 0's source coordinate.
+template <bool FAN, int NI, bool ONEV = false>
 __device__ __forceinline__ void fp_line(const float4* __restrict__ T, float t, float lo_lim, float hi_lim,
                                         const float (&A)[NI], const float (&B)[NI], const float (&S)[NI],
                                         double (&accd)[NI], float (&alo)[NI]) {
+    float tau1 = t, wgt1 = 1.f;
+    if constexpr (FAN && ONEV) {
+        tau1 = t - S[0];
+        wgt1 = rcp_approx(tau1);
+    }
+    const double wd1 = (double)wgt1;
 #pragma unroll
     for (int q = 0; q < NI; ++q) {
-        float tau = t, wgt = 1.f;
-        if constexpr (FAN) {
+        float tau = tau1, wgt = wgt1;
+        double wd = wd1;
+        if constexpr (FAN && !ONEV) {
             tau = t - S[q];  // |tau| >= 1/2 (dummies) or the source's distance
             wgt = rcp_approx(tau);
+            wd = (double)wgt;
         }
         const float xr = fmaf(B[q], tau, A[q]);
         const float xs = clampf(xr, lo_lim, hi_lim);
@@ -704,7 +715,7 @@ __device__ __forceinline__ void fp_line(const float4* __restrict__ T, float t, f
         const float frac = xs - (tt - kRoundMagic);
         const double F = __hiloint2double(__float_as_int(e.y), __float_as_int(e.x));
         if constexpr (FAN) {
-            accd[q] = fma((double)wgt, F, accd[q]);
+            accd[q] = fma(wd, F, accd[q]);
             alo[q] = fmaf(wgt * e.z, frac, alo[q]);
         } else {
             accd[q] += F;
@@ -951,7 +962,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 template <bool FAN, int NI>
 constexpr int fp_stream_min_blocks() { return NI <= 8 ? 3 : 2; }
 
-template <bool FAN, int NI, typename Tout>
+template <bool FAN, int NI, typename Tout, bool ONEV = false>
 __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
                                                              const float4* __restrict__ ltab1, DDTab tab, Grid g,
                                                              Det d, int nview, int vgroup, int rchunk,
@@ -1050,7 +1061,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         const float lo_lim = -shift, hi_lim = (float)n - shift;
         float tl = (float)(l0 - anchor);  // line coordinate, stepped exactly
         for (int r = 0; r < nlc && !failed; ++r, tl += 1.f)
-            fp_line<FAN, NI>(buf + (size_t)r * (n + 1) + h, tl, lo_lim, hi_lim, A, B, S, accd, alo);
+            fp_line<FAN, NI, ONEV>(buf + (size_t)r * (n + 1) + h, tl, lo_lim, hi_lim, A, B, S, accd, alo);
         if ((c + 1) % renorm == 0 || c == last) fp_renorm<NI>(accd, alo);
         if (c == last && !failed) {
 #pragma unroll
@@ -1751,6 +1762,32 @@ bool fp_stream_shape(const ctp_geometry& g, int& vgroup, int& ni, int max_ni = 1
     return vgroup > 0;
 }
 
+// Views per CTA and edge groups per warp (4 or 8) of the streamed fan
+// forward projector.  The kernel is issue-bound with three CTAs resident per
+// SM, so its time goes as (waves of resident CTAs) x (edge-group slots per
+// CTA); the shape minimising that product wins, the larger view group on a
+// tie (fewer copies of the slice's tables).  A single view per CTA also
+// lets the edge groups share the per-line weight (fp_line ONEV).
+// Precondition: one view fits 8 groups per warp (fp_stream_shape with at
+// most 8 succeeded).
+void fan_stream_shape(const ctp_geometry& g, int nslices, int sms, int& vgroup, int& ni) {
+    const int ipv = (int)((g.nu + 30) / 31);
+    const long long slots = 3LL * std::max(sms, 1);
+    long long best = -1;
+    for (int v = 1; v <= (int)g.nview; ++v) {
+        const int per_warp = (v * ipv + 7) / 8;
+        const int n = per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : 0;
+        if (!n) break;
+        const long long units = (long long)((g.nview + v - 1) / v) * nslices;
+        const long long cost = (units + slots - 1) / slots * n;
+        if (best < 0 || cost <= best) {
+            best = cost;
+            vgroup = v;
+            ni = n;
+        }
+    }
+}
+
 template <typename Tin, typename Tout>
 int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
               unsigned flags, char* ws, size_t ws_bytes, cudaStream_t s) {
@@ -1785,15 +1822,20 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         // one slice per CTA (sharing the edge work across two slices halves the
         // lines per table chunk, and the warps then wait on the copies instead)
         const int nslices = (int)(g.nbatch * g.nz);
-        // a grid short of one wave of resident CTAs (few slices) takes smaller
-        // view groups: more CTAs, each streaming the slice's tables
         int sms = 148, dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        for (int cap = 8; cap >= 4 && ((g.nview + sv - 1) / sv) * (size_t)nslices < 2 * (size_t)sms; cap /= 2) {
-            int sv2 = 0, ni2 = 0;
-            if (!fp_stream_shape(g, sv2, ni2, cap)) break;
-            sv = sv2;
-            ni = ni2;
+        if (geom == 0) {
+            fan_stream_shape(g, nslices, sms, sv, ni);
+        } else {
+            // a grid short of one wave of resident CTAs (few slices) takes
+            // smaller view groups: more CTAs, each streaming the slice's tables
+            for (int cap = 8; cap >= 4 && ((g.nview + sv - 1) / sv) * (size_t)nslices < 2 * (size_t)sms;
+                 cap /= 2) {
+                int sv2 = 0, ni2 = 0;
+                if (!fp_stream_shape(g, sv2, ni2, cap)) break;
+                sv = sv2;
+                ni = ni2;
+            }
         }
         const int rc_s = rchunk;
         size_t shm = 2 * (size_t)rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
@@ -1808,7 +1850,12 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
 #define CTP_FP_STREAM(NI_)                                                       \
     if (fan) launch(dd2d_fp_stream_kernel<true, NI_, Tout>);                     \
     else launch(dd2d_fp_stream_kernel<false, NI_, Tout>)
-        if (ni == 4) { CTP_FP_STREAM(4); }
+        if (fan && sv == 1) {
+            // one view per CTA: the per-line weight is shared by the edge groups
+            if (ni == 4) launch(dd2d_fp_stream_kernel<true, 4, Tout, true>);
+            else launch(dd2d_fp_stream_kernel<true, 8, Tout, true>);
+        }
+        else if (ni == 4) { CTP_FP_STREAM(4); }
         else if (ni == 8) { CTP_FP_STREAM(8); }
         else if (ni == 12) launch(dd2d_fp_stream_kernel<false, 12, Tout>);  // fan beams stop at 8
         else launch(dd2d_fp_stream_kernel<false, 16, Tout>);
