@@ -1054,7 +1054,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
             }
         }
         if (!mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1)) failed = true;
-        failed = __any_sync(0xffffffffu, failed);  // the line loop shuffles: whole warps stop together
+        failed = __any_sync(0xffffffffu, failed);  // the cell sums shuffle: whole warps stop together
         const float4* buf = s_ring + (k & 1) * ring;
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
