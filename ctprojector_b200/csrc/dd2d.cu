@@ -649,8 +649,7 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
 // no shuffle or divide per line (fp_line).  The normalisation by the
 // footprint width, the ray-length factor and the blend weight are those of
 // DDFPTracing (distanceDriven2DBoxInt.cu:21-106).
-constexpr int kFMaxItems = 16;     // edge groups (of 32 edges) per warp
-constexpr int kFMaxItemsFan = 8;   // fan beams (one more register per group): 3 CTAs per SM, no spills
+constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
 
 // Running integral at x' + 1/2 from a midpoint table: entry i holds
 // (C_i + r_i / 2, r_i) with C_i the integral up to cell i, so
@@ -809,7 +808,7 @@ __global__ void __launch_bounds__(256) line_tables_kernel(float4* __restrict__ o
 template <bool FAN, int NI>
 constexpr int fp_fast_min_blocks() { return NI <= 4 ? 3 : 2; }
 
-template <bool FAN, int NI, typename Tin, typename Tout>
+template <bool FAN, int NI, typename Tin, typename Tout, bool ONEV = false>
 __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
                                                            const Tin* __restrict__ imgT, DDTab tab, Grid g, Det d,
                                                            int nview, int vgroup, int nrows_chunk,
@@ -867,8 +866,8 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
             stage_lines<Tin>(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
             __syncthreads();
             for (int r = 0; r < nlc; ++r)
-                fp_line<FAN, NI>(s_lines + (size_t)r * (n + 1) + h, (float)(l0 + r - anchor), lo_lim, hi_lim, A, B,
-                                 S, accd, alo);
+                fp_line<FAN, NI, ONEV>(s_lines + (size_t)r * (n + 1) + h, (float)(l0 + r - anchor), lo_lim, hi_lim,
+                                       A, B, S, accd, alo);
             if ((c + 1) % renorm == 0) fp_renorm<NI>(accd, alo);
         }
         fp_renorm<NI>(accd, alo);
@@ -1762,30 +1761,38 @@ bool fp_stream_shape(const ctp_geometry& g, int& vgroup, int& ni, int max_ni = 1
     return vgroup > 0;
 }
 
-// Views per CTA and edge groups per warp (4 or 8) of the streamed fan
-// forward projector.  The kernel is issue-bound with three CTAs resident per
-// SM, so its time goes as (waves of resident CTAs) x (edge-group slots per
-// CTA); the shape minimising that product wins, the larger view group on a
-// tie (fewer copies of the slice's tables).  A single view per CTA also
-// lets the edge groups share the per-line weight (fp_line ONEV).
-// Precondition: one view fits 8 groups per warp (fp_stream_shape with at
-// most 8 succeeded).
-void fan_stream_shape(const ctp_geometry& g, int nslices, int sms, int& vgroup, int& ni) {
+// Views per CTA and edge groups per warp of the fan forward projectors.
+// The kernels are issue-bound, so their time goes as (waves of resident
+// CTAs) x (edge-group slots per CTA) x (CTAs sharing an SM); the shape
+// minimising that product wins, the larger view group on a tie (fewer
+// copies of the slice's tables).  Several views per CTA take 4 or 8 groups
+// per warp (six registers per group, three CTAs per SM).  A single view per
+// CTA lets the edge groups share the per-line weight and the source
+// coordinate (fp_line ONEV, five registers per group), so it also takes 12 or
+// 16 groups (two CTAs per SM): detectors of up to 128 groups of 31 cells.
+// False if one view does not fit 16 groups per warp.
+bool fan_shape(const ctp_geometry& g, int nslices, int sms, int& vgroup, int& ni) {
     const int ipv = (int)((g.nu + 30) / 31);
-    const long long slots = 3LL * std::max(sms, 1);
+    vgroup = 0;
+    ni = 0;
+    if (ipv == 0 || g.nview == 0 || nslices <= 0) return false;
     long long best = -1;
     for (int v = 1; v <= (int)g.nview; ++v) {
         const int per_warp = (v * ipv + 7) / 8;
-        const int n = per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : 0;
+        int n = per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : 0;
+        if (!n && v == 1) n = per_warp <= 12 ? 12 : per_warp <= 16 ? 16 : 0;
         if (!n) break;
+        const int cpsm = n <= 8 ? 3 : 2;
+        const long long slots = (long long)cpsm * std::max(sms, 1);
         const long long units = (long long)((g.nview + v - 1) / v) * nslices;
-        const long long cost = (units + slots - 1) / slots * n;
+        const long long cost = (units + slots - 1) / slots * n * cpsm;
         if (best < 0 || cost <= best) {
             best = cost;
             vgroup = v;
             ni = n;
         }
     }
+    return vgroup > 0;
 }
 
 template <typename Tin, typename Tout>
@@ -1801,11 +1808,13 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
     int vgroup = 0, nrows = 0;
     const int rchunk = fp_stream_chunk(g);
-    // views per CTA and edge groups per warp (at most 8 for fan beams, whose
-    // groups hold one register more)
+    // views per CTA and edge groups per warp
+    const int nslices = (int)(g.nbatch * g.nz);
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int sv = 0, ni = 0;
-    const bool shaped =
-        fp_fast_ok(g, vgroup, nrows) && fp_stream_shape(g, sv, ni, geom == 0 ? kFMaxItemsFan : kFMaxItems);
+    const bool shaped = fp_fast_ok(g, vgroup, nrows) &&
+                        (geom == 0 ? fan_shape(g, nslices, sms, sv, ni) : fp_stream_shape(g, sv, ni, kFMaxItems));
     // the streamed path is the faster one from a single slice up (the tables
     // are built once per slice instead of once per view group); a workspace
     // without room for the line tables runs the staged kernel
@@ -1821,12 +1830,7 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         if ((rc = check_launch("line_tables_kernel"))) return rc;
         // one slice per CTA (sharing the edge work across two slices halves the
         // lines per table chunk, and the warps then wait on the copies instead)
-        const int nslices = (int)(g.nbatch * g.nz);
-        int sms = 148, dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (geom == 0) {
-            fan_stream_shape(g, nslices, sms, sv, ni);
-        } else {
+        if (geom != 0) {
             // a grid short of one wave of resident CTAs (few slices) takes
             // smaller view groups: more CTAs, each streaming the slice's tables
             for (int cap = 8; cap >= 4 && ((g.nview + sv - 1) / sv) * (size_t)nslices < 2 * (size_t)sms;
@@ -1853,11 +1857,13 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         if (fan && sv == 1) {
             // one view per CTA: the per-line weight is shared by the edge groups
             if (ni == 4) launch(dd2d_fp_stream_kernel<true, 4, Tout, true>);
-            else launch(dd2d_fp_stream_kernel<true, 8, Tout, true>);
+            else if (ni == 8) launch(dd2d_fp_stream_kernel<true, 8, Tout, true>);
+            else if (ni == 12) launch(dd2d_fp_stream_kernel<true, 12, Tout, true>);
+            else launch(dd2d_fp_stream_kernel<true, 16, Tout, true>);
         }
         else if (ni == 4) { CTP_FP_STREAM(4); }
         else if (ni == 8) { CTP_FP_STREAM(8); }
-        else if (ni == 12) launch(dd2d_fp_stream_kernel<false, 12, Tout>);  // fan beams stop at 8
+        else if (ni == 12) launch(dd2d_fp_stream_kernel<false, 12, Tout>);  // (fan: one view per CTA, above)
         else launch(dd2d_fp_stream_kernel<false, 16, Tout>);
 #undef CTP_FP_STREAM
         return check_launch("dd2d_fp_stream_kernel");
@@ -1875,9 +1881,15 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
 #define CTP_FP_STAGED(NI_)                                                       \
     if (fan) launch(dd2d_fp_fast_kernel<true, NI_, Tin, Tout>);                  \
     else launch(dd2d_fp_fast_kernel<false, NI_, Tin, Tout>)
-        if (ni == 4) { CTP_FP_STAGED(4); }
+        if (fan && sv == 1) {
+            if (ni == 4) launch(dd2d_fp_fast_kernel<true, 4, Tin, Tout, true>);
+            else if (ni == 8) launch(dd2d_fp_fast_kernel<true, 8, Tin, Tout, true>);
+            else if (ni == 12) launch(dd2d_fp_fast_kernel<true, 12, Tin, Tout, true>);
+            else launch(dd2d_fp_fast_kernel<true, 16, Tin, Tout, true>);
+        }
+        else if (ni == 4) { CTP_FP_STAGED(4); }
         else if (ni == 8) { CTP_FP_STAGED(8); }
-        else if (ni == 12) launch(dd2d_fp_fast_kernel<false, 12, Tin, Tout>);  // fan beams stop at 8
+        else if (ni == 12) launch(dd2d_fp_fast_kernel<false, 12, Tin, Tout>);  // (fan: one view per CTA, above)
         else launch(dd2d_fp_fast_kernel<false, 16, Tin, Tout>);
 #undef CTP_FP_STAGED
         return check_launch("dd2d_fp_fast_kernel");

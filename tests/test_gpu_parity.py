@@ -80,6 +80,20 @@ def test_streamed_fp_stack_matches_oracle(name, oracle):
     assert rel_l2(prj, ref) <= TOL
 
 
+@pytest.mark.parametrize("nu", [2300, 3000])
+def test_fan_fp_wide_detector_matches_oracle(nu, oracle):
+    """Fan detectors of more than 64 groups of 31 cells take one view per
+    CTA with 12 (2300 cells) or 16 (3000 cells) edge groups per warp."""
+    from cases import Proj
+
+    p = Proj(nx=256, ny=256, nz=1, dx=1.0, dy=1.0, nu=nu, nv=1, du=0.4, dv=1.0, off_u=0.3, nview=40)
+    rng = np.random.default_rng(nu)
+    img = rng.uniform(0, 1, (2, 1, 256, 256)).astype(np.float32)
+    ang = (np.arange(40) * 2 * np.pi / 40 + 0.05).astype(np.float32)
+    prj = host(mods(True).distance_driven_fp(p, dev(img), dev(ang)))
+    assert rel_l2(prj, oracle.dd_fp(p, img, ang, "fan")) <= TOL
+
+
 @pytest.mark.parametrize("name", DD_CASES)
 @pytest.mark.parametrize("is_fbp", [False, True])
 def test_dd_bp_parity_matches_oracle(name, is_fbp, oracle):

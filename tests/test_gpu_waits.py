@@ -33,7 +33,7 @@ def _fp(g, geom_kind, img, ang, ws_bytes):
 
 
 @pytest.mark.parametrize("geom_kind,n,nview,nu,du", [(0, 256, 360, 736, 1.2858 / 1085.6), (1, 200, 180, 300, 1.0),
-                                                     (1, 96, 90, 130, 1.0)])
+                                                     (1, 96, 90, 130, 1.0), (0, 128, 40, 2300, 0.4 / 1085.6)])
 def test_streamed_fp_equals_staged(geom_kind, n, nview, nu, du):
     from ctprojector_b200._lib import Geometry, lib
 
