@@ -96,6 +96,26 @@ def test_bp_workspace_holds_view_parts():
     assert lib().ctp_dd2d_bp_workspace(ctypes.byref(stack), 0, 0, 0) < 16 * pre + 4096
 
 
+def test_fp_workspace_line_tables_up_to_128_edge_groups():
+    """The fast forward projectors serve detectors of up to 128 groups of 31
+    cells (3937 cells): their workspace holds the streamed line tables
+    (16 B per entry, rows and columns of a 256 x 256 slice); wider detectors
+    take the general kernel, whose workspace has none."""
+    from ctprojector_b200._lib import Geometry, lib
+
+    def ws(nu):
+        g = Geometry(1, 256, 256, 1, 1.0, 1.0, 1, 0, 0, 0, nu, 1, 40, 0.4 / 1085.6, 1, 0, 0, 1085.6, 595.0)
+        return lib().ctp_dd2d_fp_workspace(ctypes.byref(g), 0, 0, 0)
+
+    def edge_table(nu, nview=40):
+        return (2 * (2 * nview * (nu + 1) + nview * nu) + 5 * nview) * 4
+
+    line_tables = 2 * 256 * 257 * 16
+    image = 256 * 256 * 4
+    assert ws(3000) >= edge_table(3000) + image + line_tables
+    assert ws(4000) < edge_table(4000) + image + line_tables
+
+
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     import ctprojector_b200._lib as L
     from ctprojector_b200.errors import CTProjectorError
