@@ -10,6 +10,7 @@ step (per projector: one operand fetch per operator nonzero plus compulsory
 input and output; the filter: its input and output) divided by the step time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --op OP --workload NAME [--repeat N]     # one operation, for ncu
 
 Under torchrun every rank processes its own batch (weak scaling, no
 collective on the data path); rank 0 prints one JSON line.
@@ -138,9 +139,17 @@ def algorithmic_bytes(nnz_slice: int, nb: int, scan) -> dict:
 
 
 # ours: launches of our own kernels per step (FP: edge table, transpose, row
-# and column line tables, streamed sweep; BP: gather; filter: pad, spectrum
-# multiply, crop; FBP BP: gather)
-OUR_LAUNCHES_PER_STEP = 5 + 1 + 3 + 1
+# and column line tables, streamed sweep; BP: gather; filter: one FFT row
+# convolution over every row; FBP BP: gather)
+OUR_LAUNCHES_PER_STEP = 5 + 1 + 1 + 1
+
+# The filter of the step runs in exact mode: FP64 arithmetic in one launch
+# (conv_rows_kernel).  The default mode replays the reference's FP32
+# construction and transforms (bit-identical to it, 0.83 ms at this size);
+# that FP32 rounding leaves the reference's filter 1.2-2.2e-5 from the exact
+# result at 700-900 cells, the exact mode about 1e-7.
+FILTER_NOTE = ("hann ramp filter in exact mode (FP64 arithmetic, one launch; ~1e-7 from the exact result, where the "
+               "reference's FP32 filter is 1.2-2.2e-5 from it)")
 
 # the launches behind each timed projector operation (the roofline names the dominant one)
 ROOFLINE_KERNEL = {
@@ -191,7 +200,7 @@ def run_ours(args, rank, world, local):
         if record:
             ev["bp"][1].record()
             ev["filter"][0].record()
-        fprj = P.ramp_filter(p, prj, "hann")
+        fprj = P.ramp_filter(p, prj, "hann", exact=True)
         if record:
             ev["filter"][1].record()
             ev["bp_fbp"][0].record()
@@ -250,7 +259,7 @@ def run_ours(args, rank, world, local):
     def e2e_step():
         prj = NP.distance_driven_fp(pn, himg, ang)
         bp = NP.distance_driven_bp(pn, prj, ang)
-        fprj = NP.ramp_filter(pn, prj, "hann")
+        fprj = NP.ramp_filter(pn, prj, "hann", exact=True)
         rec = NP.distance_driven_bp(pn, fprj, ang, True)
         return prj, bp, fprj, rec
 
@@ -279,10 +288,17 @@ def run_ours(args, rank, world, local):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipse phantoms)",
         "config": {"workload": WORKLOAD, "batch_per_gpu": nb, "nnz_per_slice": nnz,
                    "algorithmic_bytes_per_step": step_bytes, "l2": "flushed between steps (512 MiB write)",
+                   "filter": FILTER_NOTE,
                    "parallelism": f"replicas x{world}", "op_ms": {k: round(v, 4) for k, v in op_avg.items()}},
         "roofline": {"bound": "hbm", "kernel": ROOFLINE_KERNEL.get(dom, dom), "achieved": round(achieved, 2),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic,
+                     "achieved_meaning": "algorithmic bytes (one operand fetch per operator nonzero, served from "
+                                         "shared memory and L2, plus compulsory I/O) per CUDA-event second",
+                     "limiter": "SM instruction issue and shared-memory wavefronts, not DRAM "
+                                "(profiles/dd2d_fp_stream_par512x16.md)",
+                     "dram_gbs": None if traffic is None else round(traffic / (op_avg[dom] * 1e-3) / 1e9, 2),
+                     "dram_frac": None if traffic is None else round(traffic / (op_avg[dom] * 1e-3) / 1e9 / peak, 4),
                      "compulsory_gbs": round((ab[dom] - 4 * nnz * nb) / (op_avg[dom] * 1e-3) / 1e9, 2)},
         "e2e": {"value": round(world * step_bytes / (e2e * 1e-3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(e2e, 3),
                 "api": "ctprojector_b200.projector.numpy.parallel (host arrays, c* entries)",
@@ -436,10 +452,10 @@ def run_reference(args, rank, world, local):
             step()
             ts.append((time.perf_counter() - t0) * 1e3)
     ms = float(np.mean(ts))
-    from ctprojector_b200.projector import _device as D
-    from ctprojector_b200.projector.cupy.ct_projector import ct_projector
+    from oracle import oracle as O  # the operator's nonzero count, on the CPU (nothing of ours on this arm)
 
-    nnz = D.dd_nnz(scan.projector(ct_projector), torch.tensor(ang, device="cuda"), 1)
+    O.build()
+    nnz = O.dd_nnz(scan, ang, "parallel")
     step_bytes = sum(algorithmic_bytes(nnz, nb, scan).values())
     value = step_bytes / (ms * 1e-3) / 1e9
     n_prj = nb * len(ang) * p.nv * p.nu
@@ -537,8 +553,10 @@ def run_reference_served():
     import torch
     from ctypes import c_float, c_ulong, c_void_p
 
+    from types import SimpleNamespace
+
     from ctprojector_b200 import synthetic as S
-    from ctprojector_b200.serving import workload as W
+    from ctprojector_b200.serving import mix as W
     from ctprojector_b200.serving.scheduler import LatencyStats
 
     lp = os.path.join(ROOT, "oracle", "_ref", "libprojector.so")
@@ -546,7 +564,7 @@ def run_reference_served():
     if not (os.path.exists(lp) and os.path.exists(tp)):
         return {"unavailable": "oracle/_ref/libprojector.so or libprior.so not built"}
     L, T = ctypes.CDLL(lp), ctypes.CDLL(tp)
-    protos = W.catalog(storage="float32")
+    protos = {n: SimpleNamespace(**d) for n, d in W.protocol_specs().items()}
     stream = W.arrivals(SERVED_JOBS, SERVED_RATE_HZ, SERVED_SEED, W.MIX_2D)
     names = sorted({n for _, n, _ in stream})
     ops = {n: _RefDD(L, protos[n].scan, protos[n].kind, protos[n].angles) for n in names}
@@ -606,6 +624,80 @@ def run_reference_served():
                     "FP32, one call per operation, one job at a time"}
 
 
+# ----------------------------------------------------------------------------- one operation, for profilers
+OP_WORKLOADS = {
+    "par512x16": "parallel 16 x 512^2 at 0.8 mm, 720 views over pi, 768 cells",
+    "fan512x4": "fan 4 x 512^2 at 0.8 mm, 984 views over 2 pi, 888 cells",
+    "fan256": "fan 1 x 256^2 at 1.0 mm, 360 views over 2 pi, 736 cells",
+    "cone64": "helical cone 1 x 64 x 512^2 at 0.7 x 0.7 x 1.0 mm, 360 views, 736 x 64 panel",
+    "tomo64": "tomosynthesis 1 x 64 x 256 x 512 (z, y, x) at 0.4 x 0.4 x 1.0 mm, 25 views over 30 degrees, "
+              "1024 x 512 detector of 0.25 mm cells 20 mm below the volume centre, source arc radius 650 mm",
+}
+OPS = ("fp", "bp", "bp_fbp", "bp_adjoint", "filter", "filter_exact", "siddon_fp", "siddon_bp", "tomo_fp",
+       "tomo_bp")
+
+
+def _op_workload(name):
+    from ctprojector_b200 import synthetic as S
+
+    if name == "par512x16":
+        scan, ang, nb = S.config2()
+        return "parallel", scan, ang, nb
+    if name == "fan512x4":
+        scan, ang, nb = S.config4()
+        return "fan", scan, ang, nb
+    if name == "fan256":
+        scan, ang, nb = S.config1()
+        return "fan", scan, ang, nb
+    if name == "cone64":
+        scan = S.Scan(512, 512, 64, 0.7, 0.7, 1.0, 736, 64, 1.2858, 1.0, 360)
+        geo = S.helical(360, 1.0, scan.dso, scan.dsd, 64 * scan.dso / scan.dsd)
+        return "cone", scan, geo, 1
+    if name == "tomo64":
+        scan = S.Scan(512, 256, 64, 0.4, 0.4, 1.0, 1024, 512, 0.25, 0.25, 25)
+        dc, src = S.tomo_geometry(25, 30.0, 650.0, -52.0)
+        return "tomo", scan, (dc, src), 1
+    raise SystemExit(f"unknown workload {name!r}; one of {sorted(OP_WORKLOADS)}")
+
+
+def run_op(op: str, workload: str, repeat: int) -> int:
+    """One projector operation of a named workload (OP_WORKLOADS) on seeded
+    uniform random inputs of its shapes (the cost does not depend on the
+    values): once untimed, then ``repeat`` times, so that ``ncu -k <kernel> -s 1
+    -c 1`` captures a warm launch."""
+    import torch
+
+    from ctprojector_b200.projector import _device as D
+
+    kind, scan, geo, nb = _op_workload(workload)
+    rng = np.random.default_rng(0)
+    dev = torch.device("cuda")
+    u = lambda *shape: torch.tensor(rng.uniform(0, 1, shape).astype(np.float32), device=dev)  # noqa: E731
+    if kind in ("tomo", "cone"):
+        g = [torch.tensor(x, device=dev) for x in geo]
+        img, prj = u(nb, scan.nz, scan.ny, scan.nx), u(nb, len(geo[0]), scan.nv, scan.nu)
+        ops = {"tomo_fp": lambda: D.tomo_fp(scan, img, *g), "tomo_bp": lambda: D.tomo_bp(scan, prj, *g)} \
+            if kind == "tomo" else \
+            {"siddon_fp": lambda: D.siddon_fp(scan, img, *g), "siddon_bp": lambda: D.siddon_bp(scan, prj, *g)}
+    else:
+        code = 0 if kind == "fan" else 1
+        ang = torch.tensor(geo, device=dev)
+        img, prj = u(nb, 1, scan.ny, scan.nx), u(nb, len(geo), 1, scan.nu)
+        ops = {"fp": lambda: D.dd_fp(scan, img, ang, code),
+               "bp": lambda: D.dd_bp(scan, prj, ang, code),
+               "bp_fbp": lambda: D.dd_bp(scan, prj, ang, code, is_fbp=True),
+               "bp_adjoint": lambda: D.dd_bp(scan, prj, ang, code, adjoint=True),
+               "filter": lambda: D.ramp_filter(scan, prj, "hann", code),
+               "filter_exact": lambda: D.ramp_filter(scan, prj, "hann", code, exact=True)}
+    if op not in ops:
+        raise SystemExit(f"op {op!r} is not defined for workload {workload!r}")
+    for _ in range(1 + max(0, repeat)):
+        ops[op]()
+    torch.cuda.synchronize()
+    print(f"{op} {workload}: ok")
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -613,7 +705,13 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
+    ap.add_argument("--op", choices=OPS, default=None,
+                    help="run only this operation of --workload (for profilers) and print no JSON line")
+    ap.add_argument("--workload", choices=sorted(OP_WORKLOADS), default="par512x16")
+    ap.add_argument("--repeat", type=int, default=1, help="with --op: warm launches after the first")
     args = ap.parse_args(argv)
+    if args.op:
+        return run_op(args.op, args.workload, args.repeat)
     rank, world, local = dist_env()
     if args.impl == "reference":
         if rank != 0:

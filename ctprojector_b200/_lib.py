@@ -22,6 +22,8 @@ CTP_ERR_UNSUPPORTED = 1002
 CTP_ERR_WORKSPACE = 1003
 CTP_ERR_CUFFT = 1004
 CTP_ERR_TOO_LARGE = 1005
+CTP_ERR_WAIT_TIMEOUT = 1006
+CTP_WAIT_POLLS_DEFAULT = 4194304
 
 FLAG_ZERO_OUT = 0x1
 FLAG_ADJOINT = 0x2
@@ -107,6 +109,9 @@ _SIGNATURES = {
     "cTVSQS3D": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F],
     "ctp_tv_sqs": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F, _P],
     "ctp_wait_timeouts": [_P],
+    "ctp_ramp_filter_host": [_P, _P, _GP, c_int, c_int, c_uint],
+    "ctp_set_wait_limit": [c_uint],
+    "ctp_scratch_allocations": [_P],
     "cSiddonFanProjection": [_P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, _F, _F, _F, _S, _S, _S, _F, _F, _F, _F, _F, _F],
     "cSiddonFanBackprojection": [_P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, _F, _F, _F, _S, _S, _S, _F, _F, _F, _F, _F,
                                  _F],

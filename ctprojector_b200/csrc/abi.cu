@@ -33,6 +33,7 @@ int tomo_bp(float*, const float*, const float*, const float*, const ctp_geometry
             cudaStream_t);
 size_t tomo_bp_workspace(const ctp_geometry&);
 int wait_timeouts(unsigned*);
+int set_first_wait_polls(unsigned);
 int siddon_fan_fp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 int siddon_fan_bp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 int pixel_bp_parallel(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
@@ -125,6 +126,26 @@ int finish_sync(int rc, cudaStream_t s) {
     return CTP_OK;
 }
 
+// Synchronous forward projections: a bounded device wait that gave up during
+// the call (its CTA leaves its part of the output unwritten) is reported as
+// CTP_ERR_WAIT_TIMEOUT, from the device counter read before and after.
+struct WaitCheck {
+    unsigned before = 0;
+    bool armed = false;
+    WaitCheck() { armed = wait_timeouts(&before) == CTP_OK; }
+    int finish(int rc) {
+        if (rc || !armed) return rc;
+        unsigned after = before;
+        if (wait_timeouts(&after) != CTP_OK) return CTP_OK;
+        if (after != before)
+            return set_error(CTP_ERR_WAIT_TIMEOUT,
+                             "%u bounded device waits gave up during the forward projection; its output is "
+                             "incomplete",
+                             after - before);
+        return CTP_OK;
+    }
+};
+
 // Host-pointer call: pooled device buffers, copies in (through pinned
 // staging chunks), op, copy out.
 struct HostCall {
@@ -198,7 +219,8 @@ static int dd_fp_dev(float* prj, const float* img, const float* deg, const ctp_g
     if (rc) return rc;
     if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g.nbatch == 0) return CTP_OK;
-    return finish_sync(dd2d_fp(prj, img, deg, g, geom, type, 0, nullptr, 0, 0), 0);
+    WaitCheck wc;
+    return wc.finish(finish_sync(dd2d_fp(prj, img, deg, g, geom, type, 0, nullptr, 0, 0), 0));
 }
 
 static int dd_bp_dev(float* img, const float* prj, const float* deg, const ctp_geometry& g, int geom, int type) {
@@ -235,6 +257,7 @@ static int dd_fp_host(float* prj, const float* img, const float* deg, const ctp_
     if (rc) return rc;
     if (!prj || !img || !deg) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
     if (g.nbatch == 0) return CTP_OK;
+    WaitCheck wc;
     HostCall hc;
     size_t ni = g.nbatch * g.nz * g.ny * g.nx, np = g.nbatch * g.nview * g.nv * g.nu;
     float* dimg = hc.upload(img, ni);
@@ -242,7 +265,7 @@ static int dd_fp_host(float* prj, const float* img, const float* deg, const ctp_
     float* dprj = hc.dev<float>(np);
     if (!hc.rc) hc.rc = dd2d_fp(dprj, dimg, ddeg, g, geom, type, 0, nullptr, 0, hc.s);
     hc.download(prj, dprj, np);
-    return hc.finish();
+    return wc.finish(hc.finish());
 }
 
 static int dd_bp_host(float* img, const float* prj, const float* deg, const ctp_geometry& g, int geom, int type) {
@@ -429,7 +452,8 @@ int cupyfbpParallelFilter(float* pFPrj, const float* pPrj, int nBatches, size_t 
     return finish_sync(filter_dev(pFPrj, pPrj, g, 1, typeFilter, 0), 0);
 }
 
-static int filter_host(float* out, const float* in, const ctp_geometry& g, int geom, int filter) {
+static int filter_host(float* out, const float* in, const ctp_geometry& g, int geom, int filter,
+                       unsigned flags = 0) {
     int rc = check_geometry(&g, false, true);
     if (rc) return rc;
     if (!out || !in) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
@@ -438,7 +462,7 @@ static int filter_host(float* out, const float* in, const ctp_geometry& g, int g
     size_t np = g.nbatch * g.nview * g.nv * g.nu;
     float* din = hc.upload(in, np);
     float* dout = hc.dev<float>(np);
-    if (!hc.rc) hc.rc = ramp_filter(dout, din, g, geom, filter, 0, nullptr, 0, hc.s);
+    if (!hc.rc) hc.rc = ramp_filter(dout, din, g, geom, filter, flags, nullptr, 0, hc.s);
     hc.download(out, dout, np);
     return hc.finish();
 }
@@ -623,6 +647,13 @@ int ctp_ramp_filter(float* fprj, const float* prj, const ctp_geometry* g, int ge
     return ramp_filter(fprj, prj, *g, geom, typeFilter, flags, workspace, workspace_bytes, as_stream(stream));
 }
 
+int ctp_ramp_filter_host(float* fprj, const float* prj, const ctp_geometry* g, int geom, int typeFilter,
+                         unsigned flags) {
+    if (!g) return set_error(CTP_ERR_INVALID_ARGUMENT, "geometry pointer is null");
+    if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
+    return filter_host(fprj, prj, *g, geom, typeFilter, flags);
+}
+
 size_t ctp_ramp_filter_workspace(const ctp_geometry* g, int geom, int typeFilter, unsigned flags) {
     return g ? ramp_filter_workspace(*g, geom, typeFilter, flags) : 0;
 }
@@ -720,6 +751,14 @@ int ctp_sqs_tv_update(float* x_out, void* x_lp, const float* x, const float* bp,
 }
 
 int ctp_wait_timeouts(unsigned int* count) { return wait_timeouts(count); }
+
+int ctp_set_wait_limit(unsigned int first_chunk_polls) { return set_first_wait_polls(first_chunk_polls); }
+
+int ctp_scratch_allocations(unsigned long long* count) {
+    if (!count) return set_error(CTP_ERR_INVALID_ARGUMENT, "count pointer is null");
+    *count = scratch_allocations();
+    return CTP_OK;
+}
 
 int cupyFbpTomoFilter(float* fprj, const float* prj, const float* detCenter, const float* src, int nBatches,
                       size_t nu, size_t nv, size_t nview, float du, float dx, float dz, int typeFilter,

@@ -30,6 +30,7 @@ inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 // cudaMallocAsync under graph capture), and copies between pageable host
 // arrays and the device through pinned chunks (synchronous for downloads).
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+unsigned long long scratch_allocations();  // successful scratch_alloc calls since load
 int staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t s);
 int staged_download(void* dst, const void* src, size_t bytes, cudaStream_t s);
 

@@ -34,7 +34,6 @@
 #include <algorithm>
 #include <climits>
 #include <type_traits>
-#include <mutex>
 
 #include "ctp_common.cuh"
 
@@ -948,13 +947,19 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 // Wait for phase `parity` of `bar`, giving up (and counting it) after a bounded
 // number of polls instead of spinning forever.
-constexpr unsigned kWaitPolls = 1u << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (unsigned i = 0; i < kWaitPolls; ++i)
+constexpr unsigned kWaitPolls = CTP_WAIT_POLLS_DEFAULT;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned polls = kWaitPolls) {
+    for (unsigned i = 0; i < polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     atomicAdd(&g_wait_timeouts, 1u);
     return false;
 }
+
+// Poll limit of each CTA's first chunk wait (ctp_set_wait_limit).  Lowering it
+// lets a test make that wait give up; the waits that let in-flight copies land
+// before a CTA exits keep kWaitPolls.
+__device__ unsigned int g_first_wait_polls = kWaitPolls;
 
 // Above 8 edge groups per warp (five or six registers per group) two CTAs
 // per SM.
@@ -1018,6 +1023,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
     float A[NI], B[NI], S[NI], alo[NI];
     double accd[NI];
     const int renorm = max(1, 16 / rchunk);  // chunks between renormalisations of (acc, alo)
+    const unsigned first_polls = g_first_wait_polls;
     bool failed = false;
     int k = 0;
     for (; k < K; ++k) {
@@ -1052,7 +1058,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
                 }
             }
         }
-        if (!mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1)) failed = true;
+        if (!mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1, k == 0 ? first_polls : kWaitPolls)) failed = true;
         failed = __any_sync(0xffffffffu, failed);  // the cell sums shuffle: whole warps stop together
         const float4* buf = s_ring + (k & 1) * ring;
         const int anchor = o == 0 ? tab.ym : tab.xm;
@@ -2193,27 +2199,15 @@ constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 
 static __device__ __align__(256) unsigned char g_fp_scratch[kNoAllocScratchBytes];
 
-namespace {
-std::mutex g_fp_scratch_mu;
-void* g_fp_scratch_addr[256] = {nullptr};
-}  // namespace
-
-// Device address of g_fp_scratch on the current device, looked up once per
-// device (the host-side symbol is only a stand-in, not a device address).
+// Device address of g_fp_scratch on the current device (the host-side symbol
+// is only a stand-in, not a device address).  Looked up on every call: the
+// lookup allocates nothing, and a cached address would go stale if the
+// device were reset and the module loaded again.
 static int fp_scratch_address(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return set_error((int)e, "cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= 256) return set_error(CTP_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
-    std::lock_guard<std::mutex> lk(g_fp_scratch_mu);
-    if (!g_fp_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_fp_scratch);
-        if (e != cudaSuccess)
-            return set_error((int)e, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
-        g_fp_scratch_addr[dev] = p;
-    }
-    *out = g_fp_scratch_addr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_fp_scratch);
+    if (e != cudaSuccess) return set_error((int)e, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    *out = p;
     return CTP_OK;
 }
 
@@ -2232,6 +2226,12 @@ int dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geom
 }
 
 size_t dd2d_fp_noalloc_capacity() { return kNoAllocScratchBytes; }
+
+int set_first_wait_polls(unsigned polls) {
+    cudaError_t e = cudaMemcpyToSymbol(g_first_wait_polls, &polls, sizeof(unsigned));
+    if (e != cudaSuccess) return set_error((int)e, "setting the wait limit: %s", cudaGetErrorString(e));
+    return CTP_OK;
+}
 
 int wait_timeouts(unsigned* count) {
     if (!count) return set_error(CTP_ERR_INVALID_ARGUMENT, "count pointer is null");

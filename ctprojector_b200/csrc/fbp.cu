@@ -450,7 +450,285 @@ int ramp_filter_reference(float* fprj, const float* prj, const ctp_geometry& g, 
     return check_launch("ref_crop_kernel");
 }
 
+// ------------------------------------------------------------------ exact mode: one-launch row convolution
+// The exact filter evaluates  out[i] = scale * sum_j w_j p[j] g[i-j]  (g the
+// FP64 windowed ramp, w the fan pre-weight) as a circular convolution of a
+// smooth size N = 2^a 3^b >= 2nu-1 (exact, since g spans offsets
+// -(nu-1)..nu-1), in FP64 arithmetic, in one launch over every row of the
+// batch with no scratch memory: a CTA takes two detector rows as the real and
+// imaginary parts of one complex row (a convolution with a real kernel acts
+// on both parts separately), zero pads it to N in shared memory, transforms
+// it (Stockham autosort, radix 8/4/3/2 stages ping-ponging between two
+// shared-memory buffers), multiplies by the kernel's spectrum, transforms back
+// (the inverse as the conjugate of the forward transform of the conjugate),
+// and writes the first nu samples of both parts, scaled and cropped.
+constexpr int kConvMaxN = 6912;  // two FP64 complex buffers of N fit 227 KB of shared memory
+constexpr int kConvMaxStages = 16;
+
+struct ConvPlan {
+    int n = 0;                    // transform size
+    int nstages = 0;              // number of radix stages
+    unsigned long long code = 0;  // the radices, 4 bits each, first stage lowest
+};
+
+// The smooth size with the least work (elements x passes over shared memory)
+// and its radices (8s first, then a 4 or a 2, then 3s); n = 0 if 2nu-1 >
+// kConvMaxN.
+ConvPlan conv_plan(int nu) {
+    ConvPlan best;
+    long best_cost = -1;
+    const long need = 2L * nu - 1;
+    for (long p2 = 1, a = 0; p2 <= kConvMaxN; p2 *= 2, ++a)
+        for (long p3 = p2, b = 0; p3 <= kConvMaxN; p3 *= 3, ++b) {
+            if (p3 < need) continue;
+            int radix[kConvMaxStages], ns = 0;
+            for (long i = 0; i < a / 3; ++i) radix[ns++] = 8;
+            if (a % 3) radix[ns++] = a % 3 == 2 ? 4 : 2;
+            for (long i = 0; i < b; ++i) radix[ns++] = 3;
+            long cost = p3 * (ns + 1);
+            if (best_cost < 0 || cost < best_cost || (cost == best_cost && p3 < best.n)) {
+                best = ConvPlan();
+                best.n = (int)p3;
+                best.nstages = ns;
+                for (int i = 0; i < ns; ++i) best.code |= (unsigned long long)radix[i] << (4 * i);
+                best_cost = cost;
+            }
+            break;  // larger powers of 3 at this power of 2 only cost more
+        }
+    return best;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }  // a * (-i)
+
+// In-register DFT of length R, forward sign (exp(-2 pi i nk/R)).
+template <int R>
+__device__ __forceinline__ void small_dft(double2* v);
+
+template <>
+__device__ __forceinline__ void small_dft<2>(double2* v) {
+    const double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+}
+
+template <>
+__device__ __forceinline__ void small_dft<4>(double2* v) {
+    const double2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+    const double2 s13 = cadd(v[1], v[3]), d13 = mul_mi(csub(v[1], v[3]));
+    v[0] = cadd(s02, s13);
+    v[2] = csub(s02, s13);
+    v[1] = cadd(d02, d13);
+    v[3] = csub(d02, d13);
+}
+
+template <>
+__device__ __forceinline__ void small_dft<8>(double2* v) {
+    double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    small_dft<4>(e);
+    small_dft<4>(o);
+    const double h = 0.70710678118654752440;  // cos(pi/4)
+    const double2 o1 = make_double2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));   // * exp(-i pi/4)
+    const double2 o2 = mul_mi(o[2]);                                                // * exp(-i pi/2)
+    const double2 o3 = make_double2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));  // * exp(-3i pi/4)
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+}
+
+template <>
+__device__ __forceinline__ void small_dft<3>(double2* v) {
+    const double s = 0.86602540378443864676;  // sin(pi/3)
+    const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    const double2 m = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
+    const double2 r = make_double2(s * t2.y, -s * t2.x);  // -i s t2
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(m, r);
+    v[2] = csub(m, r);
+}
+
+// One radix-R stage: sub-transforms of length ns are merged R at a time
+// (twiddle t of stage ns is tw[t * n / (ns R)], tw[t] = exp(-2 pi i t / n)).
+template <int R>
+__device__ __forceinline__ void fft_stage(const double2* __restrict__ src, double2* __restrict__ dst,
+                                          const double2* __restrict__ tw, int n, int ns) {
+    const int nr = n / R, tstep = n / (ns * R);
+    for (int j = threadIdx.x; j < nr; j += blockDim.x) {
+        const int k = j % ns;
+        double2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[j + r * nr];
+        if (ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + k * r * tstep));
+        }
+        small_dft<R>(v);
+        const int d = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[d + r * ns] = v[r];
+    }
+}
+
+// Forward transform of the buffer at offset a of smem (the other buffer at
+// offset b); returns the offset of the buffer that holds the result.
+__device__ __forceinline__ int fft_forward(double2* smem, int a, int b, const double2* __restrict__ tw,
+                                           const ConvPlan& plan) {
+    int ns = 1;
+    unsigned long long code = plan.code;
+    for (int s = 0; s < plan.nstages; ++s, code >>= 4) {
+        const int R = (int)(code & 15);
+        if (R == 8)
+            fft_stage<8>(smem + a, smem + b, tw, plan.n, ns);
+        else if (R == 4)
+            fft_stage<4>(smem + a, smem + b, tw, plan.n, ns);
+        else if (R == 3)
+            fft_stage<3>(smem + a, smem + b, tw, plan.n, ns);
+        else
+            fft_stage<2>(smem + a, smem + b, tw, plan.n, ns);
+        __syncthreads();
+        const int t = a;
+        a = b;
+        b = t;
+        ns *= R;
+    }
+    return a;
+}
+
+// fbpParallel.cu:44-86 / fbp.cu:81-134 for every row of the batch at once:
+// pre-weight (fan), convolution with the windowed ramp, crop and scale.
+__global__ void __launch_bounds__(256) conv_rows_kernel(float* __restrict__ out, const float* __restrict__ in,
+                                                        const double* __restrict__ weight,
+                                                        const double* __restrict__ spec,
+                                                        const double2* __restrict__ tw, const ConvPlan plan, int nu,
+                                                        size_t rows, double scale) {
+    extern __shared__ double2 conv_smem[];
+    const size_t r0 = (size_t)blockIdx.x * 2;
+    const bool two = r0 + 1 < rows;
+    const float* x0 = in + r0 * nu;
+    const float* x1 = x0 + nu;
+    for (int j = threadIdx.x; j < plan.n; j += blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        if (j < nu) {
+            const double w = weight ? __ldg(weight + j) : 1.0;
+            v.x = (double)__ldg(x0 + j) * w;
+            v.y = two ? (double)__ldg(x1 + j) * w : 0.0;
+        }
+        conv_smem[j] = v;
+    }
+    __syncthreads();
+    int a = fft_forward(conv_smem, 0, plan.n, tw, plan);
+    double2* buf = conv_smem + a;
+    for (int j = threadIdx.x; j < plan.n; j += blockDim.x) {
+        const double k = __ldg(spec + j);
+        const double2 y = buf[j];
+        buf[j] = make_double2(y.x * k, -y.y * k);  // conjugate of the product with the real spectrum
+    }
+    __syncthreads();
+    a = fft_forward(conv_smem, a, plan.n - a, tw, plan);
+    buf = conv_smem + a;
+    float* y0 = out + r0 * nu;
+    float* y1 = y0 + nu;
+    for (int n = threadIdx.x; n < nu; n += blockDim.x) {
+        const double2 v = buf[n];
+        y0[n] = (float)(v.x * scale);
+        if (two) y1[n] = (float)(-v.y * scale);
+    }
+}
+
+// Cached per (device, nu, da, filter, kind, off_u): plan, spectrum, twiddles
+// and the fan pre-weight, all FP64.
+struct ConvTables {
+    ConvPlan plan;
+    double* spec = nullptr;   // [N] DFT_N of the circular kernel (real: g is even)
+    double2* tw = nullptr;    // [N] exp(-2 pi i t / N)
+    double* weight = nullptr; // [nu] fan pre-weight, or null
+};
+
+std::mutex g_conv_mu;
+std::map<std::tuple<int, int, long long, int, int, long long>, ConvTables> g_conv;
+
+int get_conv_tables(int nu, double da, int filter, bool fan, double off_u, const ConvPlan& plan,
+                    ConvTables* out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    long long dkey, okey;
+    memcpy(&dkey, &da, sizeof(dkey));
+    memcpy(&okey, &off_u, sizeof(okey));
+    auto key = std::make_tuple(dev, nu, dkey, filter, (int)fan, fan ? okey : 0LL);
+    std::lock_guard<std::mutex> lk(g_conv_mu);
+    auto it = g_conv.find(key);
+    if (it != g_conv.end()) {
+        *out = it->second;
+        return CTP_OK;
+    }
+    const int N = plan.n;
+    std::vector<double> g = ramp_kernel(nu, da, filter, fan);
+    std::vector<double> c(N), spec(N), w(nu);
+    std::vector<double2> tw(N);
+    for (int t = 0; t < N; ++t) {
+        c[t] = cos(2 * M_PI * t / N);
+        tw[t] = make_double2(c[t], -sin(2 * M_PI * t / N));
+    }
+    for (int m = 0; m < N; ++m) {
+        double acc = g[0];
+        long long idx = 0;
+        for (int k = 1; k < nu; ++k) {
+            idx += m;
+            if (idx >= N) idx -= N;
+            acc += 2 * g[k] * c[idx];
+        }
+        spec[m] = acc;
+    }
+    for (int n = 0; n < nu; ++n) w[n] = cos(((n - (nu - 1) / 2.0) - off_u) * da);  // fbp.cu:62-66
+    ConvTables t;
+    t.plan = plan;
+    // one-time tables for this geometry, kept for the process
+    cudaError_t e = cudaMalloc(&t.spec, sizeof(double) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&t.tw, sizeof(double2) * N);
+    if (e == cudaSuccess && fan) e = cudaMalloc(&t.weight, sizeof(double) * nu);
+    if (e == cudaSuccess) e = cudaMemcpy(t.spec, spec.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t.tw, tw.data(), sizeof(double2) * N, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && fan) e = cudaMemcpy(t.weight, w.data(), sizeof(double) * nu, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return set_error((int)e, "ramp convolution tables: %s", cudaGetErrorString(e));
+    g_conv[key] = t;
+    *out = t;
+    return CTP_OK;
+}
+
+int ramp_filter_conv(float* fprj, const float* prj, const ctp_geometry& g, bool fan, int filter,
+                     const ConvPlan& plan, cudaStream_t s) {
+    const int nu = (int)g.nu, N = plan.n;
+    const size_t rows = g.nbatch * g.nview * g.nv;
+    if (rows == 0) return CTP_OK;
+    ConvTables t;
+    int rc = get_conv_tables(nu, (double)g.du, filter, fan, (double)g.off_u, plan, &t);
+    if (rc) return rc;
+    const double scale = M_PI / (double)g.nview * (double)g.du / (fan ? (double)g.dso : 1.0) / N;
+    int threads = (N / 8 + 31) / 32 * 32;
+    threads = threads < 64 ? 64 : threads > 256 ? 256 : threads;
+    const size_t smem = 2 * sizeof(double2) * N;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(conv_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return set_error((int)e, "conv_rows_kernel shared memory: %s", cudaGetErrorString(e));
+    }
+    const size_t blocks = (rows + 1) / 2;
+    if (blocks > 0x7fffffffULL) return set_error(CTP_ERR_TOO_LARGE, "ramp filter: %zu rows", rows);
+    conv_rows_kernel<<<(unsigned)blocks, threads, smem, s>>>(fprj, prj, t.weight, t.spec, t.tw, plan, nu, rows,
+                                                             scale);
+    return check_launch("conv_rows_kernel");
+}
+
 size_t exact_workspace(const ctp_geometry& g) {
+    if (conv_plan((int)g.nu).n > 0) return 0;  // conv_rows_kernel needs no scratch
     size_t rows = g.nbatch * g.nview * g.nv;
     int N = fft_size((int)g.nu);
     size_t chunk = rows < (size_t)kMaxRowsPerExec ? rows : (size_t)kMaxRowsPerExec;
@@ -461,6 +739,9 @@ size_t exact_workspace(const ctp_geometry& g) {
 
 int ramp_filter_exact(float* fprj, const float* prj, const ctp_geometry& g, int geom, int filter, void* workspace,
                       size_t workspace_bytes, cudaStream_t s) {
+    const ConvPlan cp = conv_plan((int)g.nu);
+    if (cp.n > 0) return ramp_filter_conv(fprj, prj, g, geom == 0, filter, cp, s);
+    // wider detectors: batched FP64 cuFFT transforms of the same convolution
     int nu = (int)g.nu;
     size_t rows = g.nbatch * g.nview * g.nv;
     int N = fft_size(nu), M = N / 2 + 1, stride = 2 * M;

@@ -42,6 +42,7 @@ constexpr size_t kPiece = 1u << 20;            // bytes per worker task
 constexpr size_t kDirect = 256u << 10;         // smaller transfers go straight through the driver
 
 // ------------------------------------------------------------ scratch pool
+std::atomic<unsigned long long> g_scratch_allocs{0};  // successful scratch_alloc calls (all devices)
 std::mutex g_pool_mu;
 std::map<int, cudaMemPool_t> g_pools;
 
@@ -265,8 +266,11 @@ int scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
         *p = nullptr;
         return set_error((int)e, "scratch allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     }
+    g_scratch_allocs.fetch_add(1, std::memory_order_relaxed);
     return CTP_OK;
 }
+
+unsigned long long scratch_allocations() { return g_scratch_allocs.load(std::memory_order_relaxed); }
 
 int staged_upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (bytes == 0) return CTP_OK;

@@ -58,4 +58,20 @@ def call(name: str, *args):
     check(getattr(lib(), name)(*args), name)
 
 
-__all__ = ["f32", "out_array", "p", "geom_args", "call", "c_float", "c_int", "c_size_t"]
+def exact_filter(projector, prj: np.ndarray, filter_type: str, geom: int, du: float) -> np.ndarray:
+    """The FP64 ramp filter (ctp_ramp_filter_host with CTP_FLAG_FILTER_EXACT)
+    on a float32 host sinogram; du is the cell size the reference passes
+    (angular for fan beams)."""
+    from ..._lib import FLAG_FILTER_EXACT, Geometry
+    from .._device import filter_code
+
+    nb, nview, nv, nu = prj.shape
+    g = Geometry(nb, 1, 1, 1, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, nu, nv, nview, float(du), float(projector.dv),
+                 float(projector.off_u), float(projector.off_v), float(getattr(projector, "dsd", 0.0)),
+                 float(getattr(projector, "dso", 0.0)))
+    fprj = out_array(prj.shape)
+    call("ctp_ramp_filter_host", p(fprj), p(prj), ctypes.byref(g), geom, filter_code(filter_type), FLAG_FILTER_EXACT)
+    return fprj
+
+
+__all__ = ["f32", "out_array", "p", "geom_args", "call", "exact_filter", "c_float", "c_int", "c_size_t"]

@@ -12,12 +12,17 @@ from typing import Union
 import numpy as np
 
 from .._device import filter_code
-from ._host import c_float, c_int, call, f32, geom_args, out_array, p
+from ._host import c_float, c_int, call, exact_filter, f32, geom_args, out_array, p
 from .ct_projector import ct_projector
 
 
-def ramp_filter(projector: ct_projector, prj: np.ndarray, filter_type: str = "hann") -> np.ndarray:
+def ramp_filter(projector: ct_projector, prj: np.ndarray, filter_type: str = "hann", *,
+                exact: bool = False) -> np.ndarray:
+    """Default: the reference's FP32 filter construction (its rounding
+    reproduced); exact=True: the FP64 filter (one-launch FFT convolution)."""
     prj = f32(prj)
+    if exact:
+        return exact_filter(projector, prj, filter_type, 1, projector.du)
     fprj = out_array(prj.shape)
     call("cfbpParallelFilter", p(fprj), p(prj), c_int(prj.shape[0]), c_size_t(prj.shape[3]), c_size_t(prj.shape[2]),
          c_size_t(prj.shape[1]), c_float(projector.du), c_float(projector.dv), c_float(projector.off_u),

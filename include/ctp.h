@@ -49,6 +49,11 @@ extern "C" {
 #define CTP_ERR_WORKSPACE 1003        /* caller workspace smaller than required */
 #define CTP_ERR_CUFFT 1004            /* cuFFT plan or execution failure */
 #define CTP_ERR_TOO_LARGE 1005        /* request exceeds a fixed-size internal buffer */
+#define CTP_ERR_WAIT_TIMEOUT 1006     /* a bounded device-side wait gave up during a synchronous call; the
+                                         output is incomplete (see ctp_wait_timeouts) */
+
+/* Default poll limit of the bounded device-side waits (ctp_set_wait_limit). */
+#define CTP_WAIT_POLLS_DEFAULT 4194304u
 
 /* ---- flags for the extended entries ------------------------------------ */
 #define CTP_FLAG_ZERO_OUT 0x1  /* treat the output as zero (write instead of accumulate) */
@@ -244,12 +249,17 @@ size_t ctp_dd2d_bp_workspace(const ctp_geometry* g, int geom, int typeProjector,
  * or allocation is not allowed once their service runs).  It allocates
  * nothing: its scratch is a fixed 32 MiB array inside the library's device
  * memory, held by every GPU that loads the library until the process exits
- * (ctp_dd2d_fp_noalloc_capacity() returns the size).  Requests needing more
- * scratch return CTP_ERR_TOO_LARGE.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
- * All calls on a device share the array: calls that overlap on the GPU race,
- * so the caller must order them (one stream, or events).  Output semantics and
- * flags as ctp_dd2d_fp.  This entry has no counterpart in the reference. */
+ * (ctp_dd2d_fp_noalloc_capacity() returns the size).  The driver commits that
+ * memory when it loads the library's device code on a device -- with lazy
+ * module loading (CUDA_MODULE_LOADING=LAZY, the default) that can be the first
+ * call of any entry of this library on the device -- so callers make one
+ * early call (for example at start-up, before they reserve the rest of the
+ * GPU, and before any stream capture).  Each call looks up the array's device
+ * address (the lookup allocates nothing).  Requests needing more scratch
+ * return CTP_ERR_TOO_LARGE.  All calls on a device share the array: calls that
+ * overlap on the GPU race, so the caller must order them (one stream, or
+ * events).  Output semantics and flags as ctp_dd2d_fp.  This entry has no
+ * counterpart in the reference. */
 int ctp_dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geometry* g, int geom,
                         int typeProjector, unsigned flags, void* stream);
 size_t ctp_dd2d_fp_noalloc_capacity(void);
@@ -261,12 +271,19 @@ int ctp_dd2d_nnz(unsigned long long* nnz_host, const float* deg, const ctp_geome
 /* Ramp filter (fbp.cu:15-162 fan, fbpParallel.cu:14-109 parallel); overwrites
  * fprj.  geom 0 = fan (g->du angular), 1 = parallel.  By default the windowed
  * ramp is built and applied in FP32 with transforms of length 2nu-1, the
- * construction of the reference (fbpMath.cu:90-241), which keeps the result
- * within FP32 rounding of the reference; CTP_FLAG_FILTER_EXACT builds the
- * kernel in FP64 and filters with a smooth transform size (more accurate). */
+ * construction of the reference (fbpMath.cu:90-241), which reproduces the
+ * reference's own FP32 rounding (its output is 1-2e-5 from the exact result
+ * at 700-900 cells).  CTP_FLAG_FILTER_EXACT builds the kernel in FP64 and
+ * applies it in FP64 arithmetic: one launch over every row with no scratch
+ * (workspace 0) up to 3456 cells, batched FP64 transforms above. */
 int ctp_ramp_filter(float* fprj, const float* prj, const ctp_geometry* g, int geom, int typeFilter, unsigned flags,
                     void* workspace, size_t workspace_bytes, void* stream);
 size_t ctp_ramp_filter_workspace(const ctp_geometry* g, int geom, int typeFilter, unsigned flags);
+/* The same on host arrays, synchronous, as cfbpFanFilter / cfbpParallelFilter
+ * (fbp.cu:204, fbpParallel.cu:146) with flags; no counterpart entry in the
+ * reference. */
+int ctp_ramp_filter_host(float* fprj, const float* prj, const ctp_geometry* g, int geom, int typeFilter,
+                         unsigned flags);
 
 /* Pixel-driven fan FBP back projection (fbp.cu:265-359); img += BP. */
 int ctp_fbp_fan_bp(float* img, const float* prj, const float* deg, const ctp_geometry* g, unsigned flags,
@@ -335,9 +352,28 @@ int ctp_pixel_bp_parallel(float* img, const float* prj, const float* deg, const 
 /* Bounded device-side waits that gave up on the current device since the
    library was loaded (the streamed forward projector polls an mbarrier for
    each chunk of line tables with an iteration limit, and counts a limit that
-   ran out instead of spinning for ever).  0 in a healthy process.  No
-   counterpart in the reference.  Synchronises with the device. */
+   ran out instead of spinning for ever; a CTA whose wait gave up lets its
+   in-flight copies land and exits without writing its part of the output).
+   0 in a healthy process.  The synchronous entries (c*, cupy*) compare this
+   counter before and after the call and return CTP_ERR_WAIT_TIMEOUT when it
+   went up; the asynchronous ctp_* entries return before their kernels run,
+   so their callers read the counter.  No counterpart in the reference.
+   Synchronises with the device. */
 int ctp_wait_timeouts(unsigned int* count);
+
+/* Poll limit of the first chunk wait of every CTA of the streamed forward
+   projector on the current device (default CTP_WAIT_POLLS_DEFAULT).  A test
+   of the failure path sets 0, so that the wait gives up at once (the waits
+   that let in-flight copies land before a CTA exits keep the default), and
+   restores CTP_WAIT_POLLS_DEFAULT afterwards.  No counterpart in the
+   reference. */
+int ctp_set_wait_limit(unsigned int first_chunk_polls);
+
+/* Number of scratch allocations the library has made since it was loaded
+   (stream-ordered pool, or cudaMallocAsync under graph capture), on every
+   device: calls that get a workspace, and ctp_dd2d_fp_noalloc, add none.  No
+   counterpart in the reference. */
+int ctp_scratch_allocations(unsigned long long* count);
 
 /* One SQS iteration with the TV prior, fused into one pass (no counterpart
    entry in the reference: there it is sqs_one_step, recon/cupy/sqs_algorithms.py

@@ -137,8 +137,9 @@ def test_dd_adjoint_identity(name):
 # The default filter replays the reference's FP32 construction of the windowed
 # ramp (length 2nu-1 transforms); its distance to the exact FP64 filter is the
 # reference's own rounding, up to REF_FILTER_TOL on these cases.  The exact
-# mode (FP64 kernel) meets TOL against the oracle.
+# mode (FP64 kernel, FP64 arithmetic) meets EXACT_FILTER_TOL against the oracle.
 REF_FILTER_TOL = 1e-4
+EXACT_FILTER_TOL = 1e-6
 
 
 @pytest.mark.parametrize("name", DD_CASES + ["par_wide", "fan_wide"])
@@ -148,9 +149,10 @@ def test_ramp_filter_matches_oracle(name, ftype, oracle):
     fan = name.startswith("fan")
     M = mods(fan)
     geom = "fan" if fan else "parallel"
-    prj = oracle.dd_fp(p, inp["img"], inp["angles"], geom)
+    # the same FP32 input on both sides (the filter magnifies input rounding)
+    prj = oracle.dd_fp(p, inp["img"], inp["angles"], geom).astype(np.float32)
     ref = oracle.ramp_filter(p, prj, ftype, geom)
-    assert rel_l2(host(M.ramp_filter(p, dev(prj), ftype, exact=True)), ref) <= TOL
+    assert rel_l2(host(M.ramp_filter(p, dev(prj), ftype, exact=True)), ref) <= EXACT_FILTER_TOL
     assert rel_l2(host(M.ramp_filter(p, dev(prj), ftype)), ref) <= REF_FILTER_TOL
 
 
@@ -351,3 +353,17 @@ def test_pixel_driven_bp_matches_oracle_and_reference(oracle, name):
     _, ginp, ref = load_golden(name)
     if "pixel_bp" in ref:
         assert rel_l2(host(P.pixel_driven_bp(p, dev(ref["filter_hann"]), dev(ginp["angles"]))), ref["pixel_bp"]) <= TOL
+
+
+@pytest.mark.parametrize("name", ["fan_wide", "par_wide", "fan_offsets"])
+def test_host_module_exact_filter_matches_device(name, oracle):
+    """The numpy modules' exact=True (host-array entry ctp_ramp_filter_host)
+    runs the same one-launch FP64 filter as the device path."""
+    from ctprojector_b200.projector.numpy import fan_equiangluar, parallel
+
+    p, inp = _case(name)
+    fan = name.startswith("fan")
+    prj = oracle.dd_fp(p, inp["img"], inp["angles"], "fan" if fan else "parallel").astype(np.float32)
+    a = (fan_equiangluar if fan else parallel).ramp_filter(p, prj, "hann", exact=True)
+    b = host(mods(fan).ramp_filter(p, dev(prj), "hann", exact=True))
+    assert np.array_equal(a, b)

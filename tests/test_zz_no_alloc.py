@@ -97,3 +97,53 @@ def test_noalloc_rejects_requests_beyond_its_buffer():
     rc = L.ctp_dd2d_fp_noalloc(p, p, p, ctypes.byref(g), 1, 0, 0, None)
     assert rc == CTP_ERR_TOO_LARGE
     assert "scratch" in last_error_string()
+
+
+def _scratch_allocations():
+    from ctprojector_b200._lib import lib
+
+    c = ctypes.c_ulonglong(0)
+    assert lib().ctp_scratch_allocations(ctypes.byref(c)) == 0
+    return c.value
+
+
+def test_noalloc_staged_path_allocates_nothing():
+    """The 16-slice 512 x 512 stack with 60 views of 768 cells: its edge table
+    and transposed image fit the fixed scratch but its line tables (134 MB) do
+    not, so the call runs the staged kernel (tables built per CTA in shared
+    memory).  Three calls in a row: each equals ctp_dd2d_fp, none makes a
+    scratch allocation, and the device's free memory does not move between
+    the second and the third."""
+    from ctprojector_b200._lib import lib
+
+    L = lib()
+    rng = np.random.default_rng(99)
+    nb, n, nview, nu = 16, 512, 60, 768
+    g = _geometry(nb, n, nview, nu, 0.8, 0.8)
+    cap = L.ctp_dd2d_fp_noalloc_capacity()
+    assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) > cap  # line tables do not fit
+    img = torch.tensor(rng.uniform(0, 0.03, (nb, 1, n, n)).astype(np.float32), device="cuda")
+    ang = torch.tensor(np.sort(rng.uniform(0, np.pi, nview)).astype(np.float32), device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    shape = (nb, nview, 1, nu)
+    ws_bytes = L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    ref = torch.empty(shape, dtype=torch.float32, device="cuda")
+    assert L.ctp_dd2d_fp(ctypes.c_void_p(ref.data_ptr()), ctypes.c_void_p(img.data_ptr()),
+                         ctypes.c_void_p(ang.data_ptr()), ctypes.byref(g), 1, 0, 0,
+                         ctypes.c_void_p(ws.data_ptr()), ws_bytes, stream) == 0
+    outs = [torch.full(shape, float("nan"), dtype=torch.float32, device="cuda") for _ in range(3)]
+    torch.cuda.synchronize()
+    allocs0 = _scratch_allocations()
+    free = []
+    for out in outs:
+        assert L.ctp_dd2d_fp_noalloc(ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(img.data_ptr()),
+                                     ctypes.c_void_p(ang.data_ptr()), ctypes.byref(g), 1, 0, 0, stream) == 0
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
+    assert _scratch_allocations() == allocs0
+    assert free[1] == free[2]
+    r = ref.cpu().numpy()
+    assert np.isfinite(r).all() and np.abs(r).max() > 0
+    for out in outs:
+        assert rel_l2(out.cpu().numpy(), r) <= TOL
