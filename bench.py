@@ -158,10 +158,17 @@ ROOFLINE_KERNEL = {
     "bp_fbp": "dd2d_bp_par_fast_kernel (FBP weighting)",
 }
 
-# served stream: seeded Poisson arrivals of 2D reconstruction jobs
-SERVED_JOBS = 150
+# served streams: seeded Poisson arrivals of reconstruction jobs
+SERVED_JOBS = 150  # 2D jobs only
+SERVED_MIX_JOBS = 40  # the full mix, a third of it helical cone volumes
 SERVED_RATE_HZ = 50.0
 SERVED_SEED = 5
+SERVED_MIX_SEED = 7
+SERVED_STORAGE = ("sinograms in 16-bit affine storage on the device (uint16 codes, one FP32 offset and step per "
+                  "view: half the bytes of FP32); iterate, projections and sums FP32")
+SERVED_ACCURACY = ("q16 results within 1e-4 relative L2 of the FP64 oracle reconstruction of the FP32 sinograms "
+                   "(tests/test_gpu_serving.py, tests/test_gpu_lowp.py); BF16 / FP16 sinograms measured at 6e-3 / "
+                   "7e-4 (FBP) and 7e-4-1.3e-3 / 0.9-1.6e-4 (20 SQS-TV iterations) from it, so not served")
 
 
 def run_ours(args, rank, world, local):
@@ -311,28 +318,30 @@ def run_ours(args, rank, world, local):
     return line
 
 
-def run_served(dev):
-    """The reconstruction server on a seeded stream of 2D jobs (fan 256^2 and
-    512^2, parallel 512^2; FBP or 20 SQS-TV iterations; 1-16 slices) arriving
-    at SERVED_RATE_HZ, sinograms stored in bf16 on the device, iterate and sums
-    in FP32; then the same jobs, same arrivals, through the plain FP32 per-call
-    path (one public-API call per operation, one job at a time).  Latency is
-    arrival to result on the host; recons/s is jobs over the time to the last
-    result."""
+def _serve_stream(dev, n_jobs, mix, seed, label):
+    """One seeded Poisson stream of ``n_jobs`` jobs drawn from ``mix`` at
+    SERVED_RATE_HZ: through the reconstruction server with q16 sinograms
+    (16-bit codes, one FP32 offset and step per view; iterate and sums FP32),
+    then the same jobs and arrivals through the plain FP32 per-call path (one
+    public-API call per operation, one job at a time).  Latency is arrival to
+    result on the host; recons/s is jobs over the time to the last result; GPU
+    busy is the union of the CUDA-event intervals of the work over the wall
+    time of the run."""
     import torch
 
+    from ctprojector_b200 import quant
     from ctprojector_b200.serving import Engine
     from ctprojector_b200.serving import workload as W
     from ctprojector_b200.serving.per_call import reconstruct, run_per_call
 
     p32 = W.catalog(storage="float32")
-    plp = W.catalog(storage="bfloat16")
-    stream = W.arrivals(SERVED_JOBS, SERVED_RATE_HZ, SERVED_SEED, W.MIX_2D)
+    plp = W.catalog(storage="q16")
+    stream = W.arrivals(n_jobs, SERVED_RATE_HZ, seed, mix)
     names = sorted({n for _, n, _ in stream})
     pools32 = {n: W.sinogram_pool(p32[n], 2, 16, seed=i) for i, n in enumerate(names)}
-    poolslp = {n: [t.to(torch.bfloat16).pin_memory() for t in v] for n, v in pools32.items()}
+    poolslp = {n: [quant.quantize(t.cuda()).cpu().pin_memory() for t in v] for n, v in pools32.items()}
     jobs = W.make_jobs(plp, stream, poolslp)
-    eng = Engine(device=dev)
+    eng = Engine(device=dev, track_busy=True)
     t0 = time.perf_counter()
     eng.warmup([plp[n] for n in names])
     warm = time.perf_counter() - t0
@@ -340,28 +349,46 @@ def run_served(dev):
     eng.close()
     del eng
     jobs32 = W.same_jobs(jobs, p32, pools32)
-    for n in names:  # first-call costs (filter plans, kernel attributes) outside the stream
+    for n in names:  # first-call costs (filter tables, kernel attributes) outside the stream
         reconstruct(next(j for j in jobs32 if j.protocol.name == n))
     torch.cuda.synchronize()
-    per_call = run_per_call(jobs32, realtime=True)
+    per_call = run_per_call(jobs32, realtime=True, track_busy=True)
     by = {}
     for j in jobs:
         by.setdefault(j.protocol.name, []).append(j.latency)
+    counts = {n: sum(1 for _, m, _ in stream if m == n) for n in names}
     r = lambda x: round(x, 3)  # noqa: E731
     return {
         "recons_per_s": r(served["recons_per_s"]), "p50_ms": r(served["p50_ms"]), "p99_ms": r(served["p99_ms"]),
-        "jobs": served["jobs"], "arrival_rate_hz": SERVED_RATE_HZ,
+        "jobs": served["jobs"], "arrival_rate_hz": SERVED_RATE_HZ, "gpu_busy_frac": r(served["gpu_busy_frac"]),
         "per_call_fp32": {"recons_per_s": r(per_call["recons_per_s"]), "p50_ms": r(per_call["p50_ms"]),
-                          "p99_ms": r(per_call["p99_ms"])},
+                          "p99_ms": r(per_call["p99_ms"]), "gpu_busy_frac": r(per_call["gpu_busy_frac"])},
         "served_over_per_call": r(served["recons_per_s"] / per_call["recons_per_s"]),
         "p50_ms_by_protocol": {k: r(1e3 * float(np.median(v))) for k, v in sorted(by.items())},
-        "storage": "sinograms bf16 on the device; iterate, projections and sums fp32",
-        "mix": "2D: fan 256^2 (360 views) and 512^2 (984 views), parallel 512^2 (720 views); FBP or 20 SQS-TV "
-               "iterations; 1-16 slices; Poisson arrivals, seed %d" % SERVED_SEED,
-        "accuracy": "served results vs the FP64 oracle reconstruction within 1e-4 relative L2: "
-                    "tests/test_gpu_serving.py",
+        "jobs_by_protocol": counts,
+        "mix": f"{label}; FBP or 20 SQS-TV iterations; 1-16 slices per 2D job; Poisson arrivals, seed {seed}",
         "warmup_s": r(warm),
     }
+
+
+def run_served(dev):
+    """The reconstruction server on two seeded streams: SERVED_JOBS 2D jobs
+    (fan 256^2 and 512^2, parallel 512^2), and SERVED_MIX_JOBS jobs of the full
+    mix with helical cone 64 x 512^2 volumes."""
+    out = _serve_stream(dev, SERVED_JOBS, _mix("2d"), SERVED_SEED,
+                        "2D: fan 256^2 (360 views) and 512^2 (984 views), parallel 512^2 (720 views)")
+    out["with_cone"] = _serve_stream(dev, SERVED_MIX_JOBS, _mix("all"), SERVED_MIX_SEED,
+                                     "full mix: the 2D protocols and helical cone 64 x 512^2 (360 views, 736 x 64 "
+                                     "panel; SQS only)")
+    out["storage"] = SERVED_STORAGE
+    out["accuracy"] = SERVED_ACCURACY
+    return out
+
+
+def _mix(which):
+    from ctprojector_b200.serving import mix as M
+
+    return M.MIX_2D if which == "2d" else M.MIX
 
 
 def cpu_baseline(scan, ang, img):
@@ -542,43 +569,83 @@ class _RefDD:
         return out
 
 
-def run_reference_served():
-    """The served 2D job stream of the ours arm (same seeded arrivals, mix and
-    slice counts; sinograms made here with the reference's own projector and
-    the same noise model) through the reference's per-call path: its cupy
-    entries for FP, BP and the filters and its TV prior (cupyTVSQS3D), FP32,
-    array arithmetic in between, one job at a time."""
-    import ctypes
+class _RefCone:
+    """The reference library's device-pointer Siddon cone entries for one
+    helical protocol, with the argument conventions of its cupy cone module
+    (cone.py:15-170): outputs zero-filled per call, both accumulate."""
 
+    def __init__(self, L, scan, cone):
+        import torch
+
+        self.L, self.s = L, scan
+        self.geo = [torch.tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda") for a in cone]
+        self.nview = int(cone[0].shape[0])
+
+    def _args(self):
+        from ctypes import c_float, c_ulong, c_void_p
+
+        s = self.s
+        return ([c_void_p(g.data_ptr()) for g in self.geo] +
+                [c_ulong(1), c_ulong(s.nx), c_ulong(s.ny), c_ulong(s.nz), c_float(s.dx), c_float(s.dy), c_float(s.dz),
+                 c_float(s.cx), c_float(s.cy), c_float(s.cz), c_ulong(s.nu), c_ulong(s.nv), c_ulong(self.nview),
+                 c_float(s.du), c_float(s.dv), c_float(s.off_u), c_float(s.off_v)])
+
+    def fp(self, x):
+        import torch
+        from ctypes import c_void_p
+
+        out = torch.zeros(1, self.nview, self.s.nv, self.s.nu, device="cuda")
+        rc = self.L.cupySiddonConeProjectionArbitrary(c_void_p(out.data_ptr()), c_void_p(x.data_ptr()), *self._args())
+        assert rc == 0, rc
+        return out
+
+    def bp(self, y):
+        import torch
+        from ctypes import c_void_p
+
+        out = torch.zeros(1, self.s.nz, self.s.ny, self.s.nx, device="cuda")
+        rc = self.L.cupySiddonConeBackprojectionArbitrary(c_void_p(out.data_ptr()), c_void_p(y.data_ptr()),
+                                                          *self._args())
+        assert rc == 0, rc
+        return out
+
+
+def _ref_serve_stream(L, T, n_jobs, mix, seed):
+    """A served stream of the ours arm (same seeded arrivals, mix and slice
+    counts; sinograms made here with the reference's own projectors and the
+    same noise model) through the reference's per-call path: its cupy entries
+    for FP, BP and the filters and its TV prior (cupyTVSQS3D), FP32, array
+    arithmetic in between, one job at a time."""
     import torch
     from ctypes import c_float, c_ulong, c_void_p
-
     from types import SimpleNamespace
 
     from ctprojector_b200 import synthetic as S
     from ctprojector_b200.serving import mix as W
     from ctprojector_b200.serving.scheduler import LatencyStats
 
-    lp = os.path.join(ROOT, "oracle", "_ref", "libprojector.so")
-    tp = os.path.join(ROOT, "oracle", "_ref", "libprior.so")
-    if not (os.path.exists(lp) and os.path.exists(tp)):
-        return {"unavailable": "oracle/_ref/libprojector.so or libprior.so not built"}
-    L, T = ctypes.CDLL(lp), ctypes.CDLL(tp)
     protos = {n: SimpleNamespace(**d) for n, d in W.protocol_specs().items()}
-    stream = W.arrivals(SERVED_JOBS, SERVED_RATE_HZ, SERVED_SEED, W.MIX_2D)
+    stream = W.arrivals(n_jobs, SERVED_RATE_HZ, seed, mix)
     names = sorted({n for _, n, _ in stream})
-    ops = {n: _RefDD(L, protos[n].scan, protos[n].kind, protos[n].angles) for n in names}
+    ops = {n: (_RefCone(L, protos[n].scan, protos[n].cone) if protos[n].kind == "cone"
+               else _RefDD(L, protos[n].scan, protos[n].kind, protos[n].angles)) for n in names}
     pools = {}
     for i, n in enumerate(names):
         rng = np.random.default_rng(i)
         sc = protos[n].scan
         pools[n] = []
         for _ in range(2):
-            img = np.stack([S.ellipse_phantom(rng, sc.nx, sc.ny, sc.dx, sc.dy)[None] for _ in range(16)])
-            y = ops[n].fp(torch.tensor(img, device="cuda")).cpu().numpy()
+            if protos[n].kind == "cone":
+                vol = S.ellipsoid_phantom(rng, int(sc.nz), int(sc.ny), int(sc.nx), sc.dz, sc.dy, sc.dx,
+                                          supersample=1)[None]
+                y = ops[n].fp(torch.tensor(vol, device="cuda")).cpu().numpy()
+            else:
+                img = np.stack([S.ellipse_phantom(rng, sc.nx, sc.ny, sc.dx, sc.dy)[None] for _ in range(16)])
+                y = ops[n].fp(torch.tensor(img, device="cuda")).cpu().numpy()
             pools[n].append(torch.tensor(S.poisson_log(y, 1e5, rng)).pin_memory())
     rng = np.random.default_rng(0)
-    jobs = [(t, n, nz, pools[n][int(rng.integers(2))][:nz]) for t, n, nz in stream]
+    jobs = [(t, n, nz, pools[n][int(rng.integers(2))] if protos[n].kind == "cone"
+             else pools[n][int(rng.integers(2))][:nz]) for t, n, nz in stream]
 
     def tv(x, w, eps):  # prior/cupy/recon_prior.py:85-135
         s1, s2, var = torch.zeros_like(x), torch.zeros_like(x), torch.zeros_like(x)
@@ -591,20 +658,25 @@ def run_reference_served():
     def reconstruct(n, ysino):
         pr, op = protos[n], ops[n]
         y = ysino.cuda()
+        sc = pr.scan
         if pr.algo == "fbp":
             return op.bp(op.filt(y), True).cpu()
-        sc = pr.scan
-        nz = y.shape[0]
-        norm = op.bp(op.fp(torch.ones(1, 1, sc.ny, sc.nx, device="cuda")))
-        x = torch.zeros(nz, 1, sc.ny, sc.nx, device="cuda")
+        if pr.kind == "cone":
+            shape = (1, int(sc.nz), int(sc.ny), int(sc.nx))
+            norm = op.bp(op.fp(torch.ones(shape, device="cuda")))
+        else:
+            shape = (y.shape[0], 1, sc.ny, sc.nx)
+            norm = op.bp(op.fp(torch.ones(1, 1, sc.ny, sc.nx, device="cuda")))
+        x = torch.zeros(shape, device="cuda")
+        vol = (1, -1, int(sc.ny), int(sc.nx))
         for _ in range(pr.n_iter):
             g = op.bp(op.fp(x) - y)
-            s1, s2 = tv(x.reshape(1, nz, sc.ny, sc.nx).contiguous(), pr.tv_weights, pr.eps)
+            s1, s2 = tv(x.reshape(vol).contiguous(), pr.tv_weights, pr.eps)
             x = x - (g + pr.beta * s1.reshape(x.shape)) / (norm + pr.beta * s2.reshape(x.shape))
         return x.cpu()
 
     for n in names:  # first-call costs outside the stream
-        reconstruct(n, pools[n][0][:1])
+        reconstruct(n, pools[n][0] if protos[n].kind == "cone" else pools[n][0][:1])
     torch.cuda.synchronize()
     stats = LatencyStats()
     t0 = time.perf_counter()
@@ -619,9 +691,24 @@ def run_reference_served():
     sm = stats.summary(0.0)
     r = lambda x: round(x, 3)  # noqa: E731
     return {"recons_per_s": r(sm["recons_per_s"]), "p50_ms": r(sm["p50_ms"]), "p99_ms": r(sm["p99_ms"]),
-            "jobs": sm["jobs"], "arrival_rate_hz": SERVED_RATE_HZ,
+            "jobs": sm["jobs"], "arrival_rate_hz": SERVED_RATE_HZ, "seed": seed,
+            "jobs_by_protocol": {n: sum(1 for _, m, _ in stream if m == n) for n in names},
             "path": "reference libprojector.so + libprior.so (built from its sources for sm_100a), cupy entries, "
                     "FP32, one call per operation, one job at a time"}
+
+
+def run_reference_served():
+    """The served streams of the ours arm through the reference's per-call path."""
+    import ctypes
+
+    lp = os.path.join(ROOT, "oracle", "_ref", "libprojector.so")
+    tp = os.path.join(ROOT, "oracle", "_ref", "libprior.so")
+    if not (os.path.exists(lp) and os.path.exists(tp)):
+        return {"unavailable": "oracle/_ref/libprojector.so or libprior.so not built"}
+    L, T = ctypes.CDLL(lp), ctypes.CDLL(tp)
+    out = _ref_serve_stream(L, T, SERVED_JOBS, _mix("2d"), SERVED_SEED)
+    out["with_cone"] = _ref_serve_stream(L, T, SERVED_MIX_JOBS, _mix("all"), SERVED_MIX_SEED)
+    return out
 
 
 # ----------------------------------------------------------------------------- one operation, for profilers

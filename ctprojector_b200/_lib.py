@@ -32,6 +32,7 @@ FLAG_IN_FP16 = 0x20
 FLAG_OUT_BF16 = 0x40
 FLAG_OUT_FP16 = 0x80
 FLAG_FILTER_EXACT = 0x100
+FLAG_SUBTRACT = 0x400
 FLAG_TOMO_FIRST_VIEW_KERNEL = 0x200
 
 TYPE_FBP = 0x1
@@ -110,6 +111,9 @@ _SIGNATURES = {
     "ctp_tv_sqs": [_P, _P, _P, _P, _F, _F, _F, _S, _S, _S, _S, _F, _P],
     "ctp_wait_timeouts": [_P],
     "ctp_ramp_filter_host": [_P, _P, _GP, c_int, c_int, c_uint],
+    "ctp_quantize_u16": [_P, _P, _P, _P, _S, _S, _P],
+    "ctp_dequantize_u16": [_P, _P, _P, _P, _S, _S, c_uint, _P],
+    "ctp_ramp_filter_u16": [_P, _P, _P, _P, _GP, c_int, c_int, _P],
     "ctp_set_wait_limit": [c_uint],
     "ctp_scratch_allocations": [_P],
     "cSiddonFanProjection": [_P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, _F, _F, _F, _S, _S, _S, _F, _F, _F, _F, _F, _F],

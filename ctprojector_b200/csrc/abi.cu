@@ -34,6 +34,10 @@ int tomo_bp(float*, const float*, const float*, const float*, const ctp_geometry
 size_t tomo_bp_workspace(const ctp_geometry&);
 int wait_timeouts(unsigned*);
 int set_first_wait_polls(unsigned);
+int quantize_u16(unsigned short*, float*, float*, const float*, size_t, size_t, cudaStream_t);
+int dequantize_u16(float*, const unsigned short*, const float*, const float*, size_t, size_t, bool, cudaStream_t);
+int ramp_filter_u16(float*, const unsigned short*, const float*, const float*, const ctp_geometry&, int, int,
+                    cudaStream_t);
 int siddon_fan_fp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 int siddon_fan_bp(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
 int pixel_bp_parallel(float*, const float*, const float*, const ctp_geometry&, unsigned, cudaStream_t);
@@ -753,6 +757,25 @@ int ctp_sqs_tv_update(float* x_out, void* x_lp, const float* x, const float* bp,
 int ctp_wait_timeouts(unsigned int* count) { return wait_timeouts(count); }
 
 int ctp_set_wait_limit(unsigned int first_chunk_polls) { return set_first_wait_polls(first_chunk_polls); }
+
+int ctp_quantize_u16(unsigned short* code, float* lo, float* step, const float* y, size_t nrows, size_t row_len,
+                     void* stream) {
+    return quantize_u16(code, lo, step, y, nrows, row_len, as_stream(stream));
+}
+
+int ctp_dequantize_u16(float* y, const unsigned short* code, const float* lo, const float* step, size_t nrows,
+                       size_t row_len, unsigned flags, void* stream) {
+    return dequantize_u16(y, code, lo, step, nrows, row_len, (flags & CTP_FLAG_SUBTRACT) != 0, as_stream(stream));
+}
+
+int ctp_ramp_filter_u16(float* fprj, const unsigned short* code, const float* lo, const float* step,
+                        const ctp_geometry* g, int geom, int typeFilter, void* stream) {
+    int rc = check_geometry(g, false, true);
+    if (rc) return rc;
+    if (!fprj || !code || !lo || !step) return set_error(CTP_ERR_INVALID_ARGUMENT, "null array pointer");
+    if (g->nbatch == 0) return CTP_OK;
+    return ramp_filter_u16(fprj, code, lo, step, *g, geom, typeFilter, as_stream(stream));
+}
 
 int ctp_scratch_allocations(unsigned long long* count) {
     if (!count) return set_error(CTP_ERR_INVALID_ARGUMENT, "count pointer is null");

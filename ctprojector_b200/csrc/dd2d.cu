@@ -126,8 +126,10 @@ __device__ void edge_ray(int geom, double th, int j, const Grid& g, const Det& d
     ey = (ey - g.cy) / g.dy + 0.5 * g.ny;
 }
 
+// hard != 0: the branchless tracer's weights (distanceDriven2DBranchless.cu:
+// 68-118): the main axis alone, chosen by |__cosf| > |__sinf| as there.
 __global__ void dd_table_kernel(DDTabW t, const float* __restrict__ deg, int nview, Grid g, Det d, double dsd,
-                                double dso, int geom, int ym, int xm) {
+                                double dso, int geom, int ym, int xm, int hard) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     int view = blockIdx.y;
     if (j > d.nu || view >= nview) return;
@@ -159,7 +161,8 @@ __global__ void dd_table_kernel(DDTabW t, const float* __restrict__ deg, int nvi
         double s, c;
         sincos(th, &s, &c);
         double r = (fabs(c) - fabs(s) + kDDMarginD) / (2 * kDDMarginD);
-        t.wx[view] = (float)(r < 0 ? 0.0 : (r > 1 ? 1.0 : r));
+        t.wx[view] = hard ? (fabsf(__cosf(deg[view])) > fabsf(__sinf(deg[view])) ? 1.f : 0.f)
+                          : (float)(r < 0 ? 0.0 : (r > 1 ? 1.0 : r));
         // fan source in line coordinates: edge j sits at sP + eB_j (t - sS) on
         // line t (counted from the anchor line)
         t.sP[0][view] = (float)sx;
@@ -372,10 +375,14 @@ __device__ void tile_window(bool fan, int tx0, int ty0, const Grid& g, const Det
 //   fan:      DDBPFanKernel distanceDriven2DBoxInt.cu:319-396
 //   parallel: DDBPParallelKernel :409-497
 // src is the (pre-weighted, for fan non-FBP) sinogram of this batch item.
+// branchless != 0: the reference's branchless back projection
+// (distanceDriven2DBranchless.cu:384-530): the parallel beam's main axis alone
+// (no blend band), and the detector row interpolated linearly at the pixel's
+// v between the two nearest rows (clamped to [0, nv-1]) instead of truncated.
 template <bool FAN, typename Tp, typename Tout>
 __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
     Tout* __restrict__ img, const Tp* __restrict__ src, const float* __restrict__ deg, int nview, Grid g, Det d,
-    float dso, int fbp, int accumulate, int win) {
+    float dso, int fbp, int accumulate, int win, int branchless) {
     extern __shared__ float smem[];
     float* s_win = smem;                               // [kBPViews][win]
     float* s_cos = s_win + kBPViews * win;             // [kBPViews]
@@ -400,10 +407,29 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
     float ivf = zc / d.dv + d.off_v + d.nv / 2.f - 0.5f;
     int iv = (int)ivf;  // float passed to an int parameter: truncation (:383)
     bool row_ok = iv >= 0 && iv < d.nv;
-    const Tp* rows = src + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
+    float wrow = 1.f;    // weight of the row of this pass
+    int npass = 1, iv_next = iv;
+    float w_next = 0.f;
+    if (branchless) {  // InterpolateXY of the row prefix sums, cudaMath.cu:227-258
+        const float v = clampf(ivf, 0.f, (float)d.nv);
+        const int i0 = min((int)v, d.nv - 1), i1 = min((int)v + 1, d.nv - 1);
+        w_next = v - (float)i0;
+        iv = i0;
+        row_ok = true;
+        wrow = 1.f - w_next;
+        iv_next = i1;
+        npass = (w_next != 0.f && i1 != i0) ? 2 : 1;
+        if (npass == 1) wrow = 1.f;
+    }
     size_t view_stride = (size_t)d.nv * d.nu;
 
     float acc = 0.f;
+    for (int pass = 0; pass < npass; ++pass) {
+    if (pass == 1) {
+        iv = iv_next;
+        wrow = w_next;
+    }
+    const Tp* rows = src + ((size_t)b * nview * d.nv + (row_ok ? iv : 0)) * d.nu;
     for (int v0 = 0; v0 < nview && row_ok; v0 += kBPViews) {
         int nvc = min(kBPViews, nview - v0);
         if (tid < nvc) {
@@ -449,31 +475,33 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_parity_kernel(
                         float rx = xc * c + yc * s, ry = -xc * s + yc * c;
                         val *= dso * dso / (rx * rx + (dso + ry) * (dso + ry));
                     }
-                    acc += val;
+                    acc += val * wrow;
                 } else {
                     float valx = 0.f, valy = 0.f;
-                    if (fabsf(c) > fabsf(s) - kDDMargin) {
+                    const float wx = branchless ? (s_ym[vi] ? 1.f : 0.f)
+                                                : clampf((fabsf(c) - fabsf(s) + kDDMargin) / (2 * kDDMargin), 0.f, 1.f);
+                    if (wx > 0.f) {
                         float u1 = det_coord(false, x1, yc, c, s, dso, d);
                         float u2 = det_coord(false, x2, yc, c, s, dso, d);
                         float lo = fminf(u1, u2), hi = fmaxf(u1, u2);
                         valx = (ok ? box_line_smem(w, lo - off, hi - off, win) : box_line(grow, 1, lo, hi, d.nu)) /
                                (hi - lo);
                     }
-                    if (fabsf(c) < fabsf(s) + kDDMargin) {
+                    if (wx < 1.f) {
                         float u1 = det_coord(false, xc, y1, c, s, dso, d);
                         float u2 = det_coord(false, xc, y2, c, s, dso, d);
                         float lo = fminf(u1, u2), hi = fmaxf(u1, u2);
                         valy = (ok ? box_line_smem(w, lo - off, hi - off, win) : box_line(grow, 1, lo, hi, d.nu)) /
                                (hi - lo);
                     }
-                    float wx = clampf((fabsf(c) - fabsf(s) + kDDMargin) / (2 * kDDMargin), 0.f, 1.f);
                     float val = valx * wx + valy * (1 - wx);
                     if (!fbp) val *= s_ym[vi] ? g.dy / fabsf(c) : g.dx / fabsf(s);  // :39-65
-                    acc += val;
+                    acc += val * wrow;
                 }
             }
         }
         __syncthreads();
+    }
     }
     if (ix < g.nx && iy < g.ny) {
         Tout* o = img + (((size_t)b * g.nz + iz) * g.ny + iy) * g.nx + ix;
@@ -1696,13 +1724,16 @@ int fp_stream_chunk(const ctp_geometry& g) {
     return std::max(1, std::min(r, 8));
 }
 
-int build_table(float* base, const float* deg, const ctp_geometry& g, int geom, cudaStream_t s, DDTab& tab) {
+// hard != 0: the branchless tracer's per-view weights (main axis alone)
+int build_table(float* base, const float* deg, const ctp_geometry& g, int geom, cudaStream_t s, DDTab& tab,
+                int hard = 0) {
     DDTabW w;
     carve_table(base, g.nview, g.nu, w);
     int ym = (int)(g.ny / 2), xm = (int)(g.nx / 2);
     double dsd = geom == 0 ? g.dsd : 1000.0, dso = geom == 0 ? g.dso : 500.0;
     dim3 grid((unsigned)((g.nu + 1 + 127) / 128), (unsigned)g.nview);
-    dd_table_kernel<<<grid, 128, 0, s>>>(w, deg, (int)g.nview, make_grid(g), make_det(g), dsd, dso, geom, ym, xm);
+    dd_table_kernel<<<grid, 128, 0, s>>>(w, deg, (int)g.nview, make_grid(g), make_det(g), dsd, dso, geom, ym, xm,
+                                         hard);
     tab = as_read(w, ym, xm);
     return check_launch("dd_table_kernel");
 }
@@ -1805,7 +1836,7 @@ template <typename Tin, typename Tout>
 int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
               unsigned flags, char* ws, size_t ws_bytes, cudaStream_t s) {
     DDTab tab;
-    int rc = build_table(reinterpret_cast<float*>(ws), deg, g, geom, s, tab);
+    int rc = build_table(reinterpret_cast<float*>(ws), deg, g, geom, s, tab, (type & CTP_TYPE_BRANCHLESS) ? 1 : 0);
     if (rc) return rc;
     Tin* imgT = reinterpret_cast<Tin*>(ws + align_up(table_floats(g.nview, g.nu) * sizeof(float)));
     dim3 tg((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 31) / 32), (unsigned)(g.nbatch * g.nz));
@@ -2052,9 +2083,12 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
         return check_launch("dd2d_bp_adjoint_kernel");
     }
     int fbp = (type & (CTP_TYPE_FBP | CTP_TYPE_FORCE_FBP)) ? 1 : 0;
+    // branchless: the same operator as the box integral for a fan beam with
+    // one detector row; otherwise the general kernel in its branchless mode
+    const int bl = (type & CTP_TYPE_BRANCHLESS) ? 1 : 0;
     size_t shm = (size_t)kBPViews * wl * 4 + kBPViews * 5 * 4;
     if (geom == 0) {
-        int fwin = fan_fast_window(g);
+        int fwin = (bl && g.nv > 1) ? 0 : fan_fast_window(g);
         int tiles_f = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
         // two slices per CTA for stacks (shared edge mappings), one otherwise
         const int nslices = (int)(g.nbatch * g.nz);
@@ -2106,14 +2140,14 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
             if ((rc = check_launch("fan_preweight_kernel"))) return rc;
             auto k = dd2d_bp_parity_kernel<true, float, Tout>;
             k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), wprj, deg, nview, gr, dt, dso, 0, accumulate,
-                                               win > 0 ? win : 0);
+                                               win > 0 ? win : 0, bl);
         } else {
             auto k = dd2d_bp_parity_kernel<true, Tin, Tout>;
             k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, 1,
-                                               accumulate, win > 0 ? win : 0);
+                                               accumulate, win > 0 ? win : 0, bl);
         }
     } else {
-        int pwin = par_fast_window(g);
+        int pwin = bl ? 0 : par_fast_window(g);
         if (pwin > 0) {
             int tiles_p = (int)(((g.nx + kPT - 1) / kPT) * ((g.ny + kPT - 1) / kPT));
             // slices per CTA for stacks (shared per-view work): 4, 2 or 1
@@ -2148,7 +2182,7 @@ int launch_bp(void* img, const void* prj, const float* deg, const ctp_geometry& 
         }
         auto k = dd2d_bp_parity_kernel<false, Tin, Tout>;
         k<<<grid, kTile * kTile, shm, s>>>(mptr<Tout>(img), cptr<Tin>(prj), deg, nview, gr, dt, dso, fbp,
-                                           accumulate, win > 0 ? win : 0);
+                                           accumulate, win > 0 ? win : 0, bl);
     }
     return check_launch("dd2d_bp_parity_kernel");
 }

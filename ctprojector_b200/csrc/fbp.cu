@@ -603,9 +603,27 @@ __device__ __forceinline__ int fft_forward(double2* smem, int a, int b, const do
     return a;
 }
 
+// Input rows of the filter: FP32 samples, or 16-bit affine codes with one
+// offset and step per view (quant.cu), dequantized as they are read.
+struct RowsF32 {
+    const float* p;
+    __device__ __forceinline__ float load(size_t row, int j, int nu) const { return __ldg(p + row * nu + j); }
+};
+struct RowsU16 {
+    const unsigned short* code;
+    const float* lo;
+    const float* step;
+    int nv;  // detector rows per view (one offset and step each view)
+    __device__ __forceinline__ float load(size_t row, int j, int nu) const {
+        const size_t v = row / (size_t)nv;
+        return fmaf(__ldg(step + v), (float)__ldg(code + row * nu + j), __ldg(lo + v));
+    }
+};
+
 // fbpParallel.cu:44-86 / fbp.cu:81-134 for every row of the batch at once:
 // pre-weight (fan), convolution with the windowed ramp, crop and scale.
-__global__ void __launch_bounds__(256) conv_rows_kernel(float* __restrict__ out, const float* __restrict__ in,
+template <typename Rows>
+__global__ void __launch_bounds__(256) conv_rows_kernel(float* __restrict__ out, const Rows in,
                                                         const double* __restrict__ weight,
                                                         const double* __restrict__ spec,
                                                         const double2* __restrict__ tw, const ConvPlan plan, int nu,
@@ -613,14 +631,12 @@ __global__ void __launch_bounds__(256) conv_rows_kernel(float* __restrict__ out,
     extern __shared__ double2 conv_smem[];
     const size_t r0 = (size_t)blockIdx.x * 2;
     const bool two = r0 + 1 < rows;
-    const float* x0 = in + r0 * nu;
-    const float* x1 = x0 + nu;
     for (int j = threadIdx.x; j < plan.n; j += blockDim.x) {
         double2 v = make_double2(0.0, 0.0);
         if (j < nu) {
             const double w = weight ? __ldg(weight + j) : 1.0;
-            v.x = (double)__ldg(x0 + j) * w;
-            v.y = two ? (double)__ldg(x1 + j) * w : 0.0;
+            v.x = (double)in.load(r0, j, nu) * w;
+            v.y = two ? (double)in.load(r0 + 1, j, nu) * w : 0.0;
         }
         conv_smem[j] = v;
     }
@@ -704,7 +720,8 @@ int get_conv_tables(int nu, double da, int filter, bool fan, double off_u, const
     return CTP_OK;
 }
 
-int ramp_filter_conv(float* fprj, const float* prj, const ctp_geometry& g, bool fan, int filter,
+template <typename Rows>
+int ramp_filter_conv(float* fprj, const Rows prj, const ctp_geometry& g, bool fan, int filter,
                      const ConvPlan& plan, cudaStream_t s) {
     const int nu = (int)g.nu, N = plan.n;
     const size_t rows = g.nbatch * g.nview * g.nv;
@@ -717,13 +734,14 @@ int ramp_filter_conv(float* fprj, const float* prj, const ctp_geometry& g, bool 
     threads = threads < 64 ? 64 : threads > 256 ? 256 : threads;
     const size_t smem = 2 * sizeof(double2) * N;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(conv_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(conv_rows_kernel<Rows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return set_error((int)e, "conv_rows_kernel shared memory: %s", cudaGetErrorString(e));
     }
     const size_t blocks = (rows + 1) / 2;
     if (blocks > 0x7fffffffULL) return set_error(CTP_ERR_TOO_LARGE, "ramp filter: %zu rows", rows);
-    conv_rows_kernel<<<(unsigned)blocks, threads, smem, s>>>(fprj, prj, t.weight, t.spec, t.tw, plan, nu, rows,
-                                                             scale);
+    conv_rows_kernel<Rows><<<(unsigned)blocks, threads, smem, s>>>(fprj, prj, t.weight, t.spec, t.tw, plan, nu,
+                                                                   rows, scale);
     return check_launch("conv_rows_kernel");
 }
 
@@ -740,7 +758,7 @@ size_t exact_workspace(const ctp_geometry& g) {
 int ramp_filter_exact(float* fprj, const float* prj, const ctp_geometry& g, int geom, int filter, void* workspace,
                       size_t workspace_bytes, cudaStream_t s) {
     const ConvPlan cp = conv_plan((int)g.nu);
-    if (cp.n > 0) return ramp_filter_conv(fprj, prj, g, geom == 0, filter, cp, s);
+    if (cp.n > 0) return ramp_filter_conv(fprj, RowsF32{prj}, g, geom == 0, filter, cp, s);
     // wider detectors: batched FP64 cuFFT transforms of the same convolution
     int nu = (int)g.nu;
     size_t rows = g.nbatch * g.nview * g.nv;
@@ -789,6 +807,17 @@ int ramp_filter_exact(float* fprj, const float* prj, const ctp_geometry& g, int 
 }
 
 }  // namespace
+
+// The exact filter of a sinogram in 16-bit affine storage (quant.cu): one
+// offset and step per view of each batch item.
+int ramp_filter_u16(float* fprj, const unsigned short* code, const float* lo, const float* step,
+                    const ctp_geometry& g, int geom, int filter, cudaStream_t s) {
+    if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
+    const ConvPlan cp = conv_plan((int)g.nu);
+    if (cp.n == 0)
+        return set_error(CTP_ERR_UNSUPPORTED, "16-bit sinogram filter: %zu cells exceed the one-launch filter", g.nu);
+    return ramp_filter_conv(fprj, RowsU16{code, lo, step, (int)g.nv}, g, geom == 0, filter, cp, s);
+}
 
 size_t ramp_filter_workspace(const ctp_geometry& g, int, int, unsigned flags) {
     return (flags & CTP_FLAG_FILTER_EXACT) ? exact_workspace(g) : ref_workspace(g);

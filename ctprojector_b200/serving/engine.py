@@ -30,8 +30,9 @@ weight 1, x0 = 0 and the projector normalisation folded into beta:
     x <- x - (A^T (A x - y) + beta s1(x)) / (A^T A 1 + beta s2(x))
 
 Storage precision: the measured sinogram is held on the device in the job's
-storage type (float32, bfloat16 or float16); the iterate, the projections of
-each iteration and every sum are float32.  Optionally the forward projector
+storage type (float32, bfloat16, float16, or "q16": 16-bit codes with one FP32
+offset and step per view, ``ctprojector_b200.quant``); the iterate, the
+projections of each iteration and every sum are float32.  Optionally the forward projector
 reads a low-precision copy of the iterate written by the fused update
 (``image_storage``).
 """
@@ -46,11 +47,15 @@ import numpy as np
 import torch
 
 from .. import _lib
+from .. import quant
 from ..projector import _device as D
 from ..recon import sqs_tv_update
+from .busy import BusyTracker
 from .scheduler import ArrivalQueue, LatencyStats, MemoryBudget, Pending, SlotPool, bucket, bucket_sizes
 
-DTYPES = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float16": torch.float16}
+# storage name -> device dtype of the sinogram buffer ("q16": the codes of
+# 16-bit affine storage, with an FP32 offset and step per view beside them)
+DTYPES = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float16": torch.float16, "q16": torch.int16}
 
 
 @dataclass(eq=False)
@@ -83,8 +88,10 @@ class Protocol:
             raise ValueError(f"unknown algorithm {self.algo!r}")
         if self.kind == "cone" and self.algo != "sqs":
             raise ValueError("cone protocols reconstruct with SQS (there is no cone FBP)")
-        if self.storage not in DTYPES or self.image_storage not in DTYPES:
-            raise ValueError("storage must be float32, bfloat16 or float16")
+        if self.storage not in DTYPES:
+            raise ValueError("storage must be float32, bfloat16, float16 or q16")
+        if self.image_storage not in DTYPES or self.image_storage == "q16":
+            raise ValueError("image_storage must be float32, bfloat16 or float16")
 
     @property
     def nview(self) -> int:
@@ -104,7 +111,8 @@ class Protocol:
 @dataclass(eq=False)
 class Job:
     """One reconstruction request.  ``sinogram`` is a host tensor of
-    ``protocol.sinogram_shape(nz)`` in any float type (it is stored in the
+    ``protocol.sinogram_shape(nz)`` in any float type, or a ``quant.Q16`` for
+    q16 protocols (it is stored in the
     protocol's storage type on the device); ``arrival`` is in seconds from the
     start of the stream.  The server fills ``result`` ([nz, ny, nx] float32,
     host) and ``t_done``."""
@@ -190,6 +198,39 @@ class Lane:
     def can_admit(self, job: Job) -> bool:
         return self.pool.fits(job.units)
 
+    # sinogram buffers: y (storage dtype), plus per-view offsets and steps for q16
+    def _alloc_sinogram(self, C: int, nview: int, nv: int, nu: int) -> None:
+        p = self.p
+        self.y = torch.zeros(C, nview, nv, nu, dtype=DTYPES[p.storage], device=self.dev)
+        self.q16 = p.storage == "q16"
+        self.ylo = torch.zeros(C, nview, device=self.dev) if self.q16 else None
+        self.ystep = torch.zeros(C, nview, device=self.dev) if self.q16 else None
+
+    def _ybufs(self) -> List[torch.Tensor]:
+        return [self.y] + ([self.ylo, self.ystep] if self.q16 else [])
+
+    def _ystored(self, b: int):
+        """The first b slots of the sinogram as stored (Tensor or quant.Q16)."""
+        return quant.Q16(self.y[:b], self.ylo[:b], self.ystep[:b]) if self.q16 else self.y[:b]
+
+    def _load_sinogram(self, start: int, n: int, sino) -> None:
+        """Copy a job's host sinogram into slots [start, start + n) (lane stream)."""
+        dst = self.y[start:start + n]
+        if self.q16:
+            if not isinstance(sino, quant.Q16):
+                raise TypeError(f"protocol {self.p.name} stores q16 sinograms: the job must bring a quant.Q16")
+            dst.copy_(sino.code.reshape(dst.shape), non_blocking=True)
+            self.ylo[start:start + n].copy_(sino.lo.reshape(n, -1), non_blocking=True)
+            self.ystep[start:start + n].copy_(sino.step.reshape(n, -1), non_blocking=True)
+        else:
+            dst.copy_(sino.reshape(dst.shape), non_blocking=True)
+
+    @staticmethod
+    def sinogram_bytes(p: Protocol, sino: int) -> int:
+        """Device bytes of ``sino`` stored samples (q16 adds 8 bytes per view)."""
+        extra = 8 * (sino // max(1, int(p.scan.nu) * (int(p.scan.nv) if p.kind == "cone" else 1)))
+        return sino * DTYPES[p.storage].itemsize + (extra if p.storage == "q16" else 0)
+
     def _record(self):
         ev = torch.cuda.Event()
         ev.record(self.stream)
@@ -208,9 +249,9 @@ class SQSLane(Lane):
         C, U = self.capacity, p.slices_per_unit
         nview = p.nview
         nv = int(s.nv) if p.kind == "cone" else 1
-        sdt, idt = DTYPES[p.storage], DTYPES[p.image_storage]
+        idt = DTYPES[p.image_storage]
         with torch.cuda.stream(self.stream):
-            self.y = torch.zeros(C, nview, nv, int(s.nu), dtype=sdt, device=self.dev)
+            self._alloc_sinogram(C, nview, nv, int(s.nu))
             self.fp = torch.zeros(C, nview, nv, int(s.nu), device=self.dev)
             self.x = [torch.zeros(C, U, self.ny, self.nx, device=self.dev) for _ in range(2)]
             self.bp = torch.zeros(C, U, self.ny, self.nx, device=self.dev)
@@ -234,7 +275,7 @@ class SQSLane(Lane):
         img = p.slices_per_unit * int(s.ny) * int(s.nx)
         lp = 2 * DTYPES[p.image_storage].itemsize * img if p.image_storage != "float32" else 0
         # y, fp; x (2), bp, fp workspace (transposed image); captured graphs' workspaces
-        return sino * (DTYPES[p.storage].itemsize + 4) + img * 4 * 4 + lp + sino * 4
+        return Lane.sinogram_bytes(p, sino) + sino * 4 + img * 4 * 4 + lp + sino * 4
 
     # projector calls on the lane stream (current stream inside the lane's context)
     def _fp(self, x, out=None):
@@ -251,7 +292,10 @@ class SQSLane(Lane):
         p = self.p
         xin = self.xlp[src][:b] if self.xlp is not None else self.x[src][:b]
         self._fp(xin, out=self.fp[:b])
-        self.fp[:b].sub_(self.y[:b])
+        if self.q16:
+            quant.sub_dequantized_(self.fp[:b], self._ystored(b))
+        else:
+            self.fp[:b].sub_(self.y[:b])
         self._bp(self.fp[:b], out=self.bp[:b])
         sqs_tv_update(self.x[src][:b], self.bp[:b], self.norm, p.beta, p.tv_weights, p.eps,
                       zlink=self.zlink[:b * p.slices_per_unit], out=self.x[dst][:b],
@@ -296,7 +340,7 @@ class SQSLane(Lane):
             start = self.pool.alloc(job.job_id, job.units)
         n = job.units
         with torch.cuda.stream(self.stream):
-            self.y[start:start + n].copy_(job.sinogram.reshape(self.y[start:start + n].shape), non_blocking=True)
+            self._load_sinogram(start, n, job.sinogram)
             self.x[self.cur][start:start + n].zero_()
             if self.xlp is not None:
                 self.xlp[self.cur][start:start + n].zero_()
@@ -308,7 +352,7 @@ class SQSLane(Lane):
         if not moves:
             return
         with torch.cuda.stream(self.stream):
-            bufs = [self.y, self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else [])
+            bufs = self._ybufs() + [self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else [])
             for m in moves:
                 for t in bufs:
                     t[m.dst:m.dst + m.n].copy_(t[m.src:m.src + m.n].clone())
@@ -339,7 +383,7 @@ class SQSLane(Lane):
                 self._apply_moves(self.pool.compact())
                 new_hw = self.pool.high_water
                 if new_hw < old_hw:
-                    for t in [self.y, self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else []):
+                    for t in self._ybufs() + [self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else []):
                         t[new_hw:old_hw].zero_()
                     if self.p.kind != "cone":
                         self.zlink[new_hw:old_hw].zero_()
@@ -359,22 +403,21 @@ class FBPLane(Lane):
         p, s = protocol, protocol.scan
         C = self.capacity
         with torch.cuda.stream(self.stream):
-            self.y = torch.zeros(C, p.nview, 1, int(s.nu), dtype=DTYPES[p.storage], device=self.dev)
+            self._alloc_sinogram(C, p.nview, 1, int(s.nu))
             self.img = torch.zeros(C, 1, self.ny, self.nx, device=self.dev)
 
     @staticmethod
     def bytes_per_unit(p: Protocol) -> int:
         s = p.scan
         sino = p.nview * int(s.nu)
-        return sino * (DTYPES[p.storage].itemsize + 8) + int(s.ny) * int(s.nx) * 4
+        return Lane.sinogram_bytes(p, sino) + sino * 8 + int(s.ny) * int(s.nx) * 4
 
     def admit(self, job: Job) -> None:
         start = self.pool.alloc(job.job_id, job.units)
         if start is None:
             raise RuntimeError("FBP lane slots are freed every step; admission checked can_admit first")
         with torch.cuda.stream(self.stream):
-            self.y[start:start + job.units].copy_(job.sinogram.reshape(self.y[start:start + job.units].shape),
-                                                  non_blocking=True)
+            self._load_sinogram(start, job.units, job.sinogram)
         self.jobs[job.job_id] = [job, 1]
 
     def prepare(self) -> None:
@@ -385,8 +428,11 @@ class FBPLane(Lane):
 
     def _filter_bp(self, b: int) -> None:
         p = self.p
-        y = self.y[:b] if self.y.dtype == torch.float32 else self.y[:b].float()
-        f = D.ramp_filter(p.scan, y, p.filter, self.geom, exact=True)
+        if self.q16:
+            f = quant.ramp_filter(p.scan, self._ystored(b), p.filter, self.geom)
+        else:
+            y = self.y[:b] if self.y.dtype == torch.float32 else self.y[:b].float()
+            f = D.ramp_filter(p.scan, y, p.filter, self.geom, exact=True)
         D.dd_bp(p.scan, f, self.ang, self.geom, is_fbp=True, out=self.img[:b])
 
     def step(self) -> List[Job]:
@@ -401,7 +447,8 @@ class FBPLane(Lane):
                 job.result.copy_(self.img[start:start + n].reshape(job.result.shape), non_blocking=True)
                 job.done_event = torch.cuda.Event()
                 job.done_event.record(self.stream)
-                self.y[start:start + n].zero_()
+                for t in self._ybufs():
+                    t[start:start + n].zero_()
                 done.append(job)
         self._record()
         self.last_used = time.perf_counter()
@@ -416,7 +463,8 @@ class Engine:
     cone volumes as a quarter of the budget holds, at most 4)."""
 
     def __init__(self, device=None, hbm_bytes: Optional[int] = None, max_wait: float = 1.0,
-                 use_graphs: bool = True, capacity: Optional[Dict[str, int]] = None, slices_per_lane: int = 64):
+                 use_graphs: bool = True, capacity: Optional[Dict[str, int]] = None, slices_per_lane: int = 64,
+                 track_busy: bool = False):
         if not torch.cuda.is_available():
             raise RuntimeError("the reconstruction server needs a CUDA device")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -435,6 +483,8 @@ class Engine:
         self.t0 = 0.0
         self.evictions = 0  # lanes torn down to make room for another protocol
         self.peak_reserved = 0
+        self.track_busy = track_busy  # bracket every lane step with timing events (busy.BusyTracker)
+        self.busy_tracker = None
 
     # lanes ---------------------------------------------------------------
     def _lane_class(self, p: Protocol):
@@ -504,7 +554,10 @@ class Engine:
         stepped = False
         for lane in list(self.lanes.values()):
             if lane.active and lane.ready():
+                start = self.busy_tracker.begin(lane.stream) if self.busy_tracker is not None else None
                 self.retiring.extend(lane.step())
+                if start is not None:
+                    self.busy_tracker.end(lane.stream, start)
                 stepped = True
         return stepped
 
@@ -541,6 +594,8 @@ class Engine:
         offered only once its arrival time has passed on the wall clock;
         otherwise all are offered at once.  Returns the latency summary."""
         pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        if self.track_busy:
+            self.busy_tracker = BusyTracker(self.device)
         self.t0 = time.perf_counter()
         now_fn = lambda: time.perf_counter() - self.t0  # noqa: E731
         while pending or self.busy():
@@ -551,7 +606,13 @@ class Engine:
             if not progressed:
                 time.sleep(idle_sleep)
         torch.cuda.synchronize(self.device)
-        return self.stats.summary(0.0)
+        wall = time.perf_counter() - self.t0
+        summary = self.stats.summary(0.0)
+        if self.busy_tracker is not None:
+            busy = self.busy_tracker.busy_seconds()
+            summary.update(wall_s=wall, gpu_busy_s=busy, gpu_busy_frac=busy / wall if wall > 0 else 0.0)
+            self.busy_tracker = None
+        return summary
 
     def close(self) -> None:
         for name, lane in list(self.lanes.items()):

@@ -13,9 +13,11 @@ from typing import Sequence
 import torch
 
 from .. import prior
+from ..quant import Q16
 from ..projector.cupy import cone as C
 from ..projector.cupy import fan_equiangular as F
 from ..projector.cupy import parallel as P
+from .busy import BusyTracker
 from .engine import Job
 from .scheduler import LatencyStats
 
@@ -24,7 +26,7 @@ def reconstruct(job: Job) -> torch.Tensor:
     """One job through the public API in FP32; returns the host image [nz, ny, nx]."""
     p = job.protocol
     s = p.scan
-    y = job.sinogram.to("cuda", torch.float32)
+    y = job.sinogram.to("cuda").float() if isinstance(job.sinogram, Q16) else job.sinogram.to("cuda", torch.float32)
     if p.kind == "cone":
         geo = [torch.as_tensor(a, device="cuda") for a in p.cone]
         fp = lambda x: C.siddon_fp_arbitrary(s, x, *geo)  # noqa: E731
@@ -49,12 +51,14 @@ def reconstruct(job: Job) -> torch.Tensor:
     return x.reshape(-1, int(s.ny), int(s.nx)).cpu()
 
 
-def run_per_call(jobs: Sequence[Job], realtime: bool = True) -> dict:
+def run_per_call(jobs: Sequence[Job], realtime: bool = True, track_busy: bool = False) -> dict:
     """Serve ``jobs`` one after another in arrival order (each starts when it
     has arrived and the previous one is done).  Fills ``result`` and
-    ``t_done``; returns the latency summary."""
+    ``t_done``; returns the latency summary (with ``track_busy``, also the
+    GPU-busy time of the jobs' work, busy.BusyTracker)."""
     stats = LatencyStats()
     pending = deque(sorted(jobs, key=lambda j: j.arrival))
+    tracker = BusyTracker() if track_busy else None
     t0 = time.perf_counter()
     while pending:
         job = pending.popleft()
@@ -62,8 +66,17 @@ def run_per_call(jobs: Sequence[Job], realtime: bool = True) -> dict:
             wait = job.arrival - (time.perf_counter() - t0)
             if wait > 0:
                 time.sleep(wait)
+        stream = torch.cuda.current_stream()
+        start = tracker.begin(stream) if tracker is not None else None
         job.result = reconstruct(job)
+        if start is not None:
+            tracker.end(stream, start)
         torch.cuda.synchronize()
         job.t_done = time.perf_counter() - t0
         stats.add(job.latency, job.t_done)
-    return stats.summary(0.0)
+    wall = time.perf_counter() - t0
+    summary = stats.summary(0.0)
+    if tracker is not None:
+        busy = tracker.busy_seconds()
+        summary.update(wall_s=wall, gpu_busy_s=busy, gpu_busy_frac=busy / wall if wall > 0 else 0.0)
+    return summary

@@ -11,6 +11,7 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import torch
 
+from .. import quant
 from .. import synthetic as S
 from ..projector import _device as D
 from .engine import DTYPES, Job, Protocol
@@ -33,7 +34,7 @@ def catalog(storage: str = "bfloat16", n_iter: int = 20, image_storage: str = "f
 
 def sinogram_pool(p: Protocol, n_variants: int, max_slices: int, seed: int, photons: float = 1e5) -> List[torch.Tensor]:
     """Pinned host sinograms of ``p`` (``max_slices`` slices for 2D, one volume
-    for cone) in the protocol's storage type."""
+    for cone) in the protocol's storage type (a ``quant.Q16`` for q16)."""
     rng = np.random.default_rng(seed)
     s = p.scan
     out = []
@@ -48,7 +49,10 @@ def sinogram_pool(p: Protocol, n_variants: int, max_slices: int, seed: int, phot
             geom = 0 if p.kind == "fan" else 1
             y = D.dd_fp(s, torch.tensor(img, device="cuda"), torch.tensor(p.angles, device="cuda"), geom)
         y = torch.tensor(S.poisson_log(y.cpu().numpy(), photons, rng))
-        out.append(y.to(DTYPES[p.storage]).pin_memory())
+        if p.storage == "q16":  # quantized on the device, kept in pinned host memory
+            out.append(quant.quantize(y.cuda()).cpu().pin_memory())
+        else:
+            out.append(y.to(DTYPES[p.storage]).pin_memory())
     return out
 
 

@@ -66,12 +66,18 @@ extern "C" {
 #define CTP_FLAG_OUT_FP16 0x80 /* the output array is float16 */
 #define CTP_FLAG_FILTER_EXACT 0x100 /* ramp filter: FP64 windowed kernel, smooth FFT size
                                        (default: the reference's FP32 construction) */
+#define CTP_FLAG_SUBTRACT 0x400 /* ctp_dequantize_u16: subtract the values from the output */
 
 /* typeProjector bits of the DD 2D entries, as in the reference
  * (distanceDriven2D.cu:12-25): bit0 FBP weighting, bit1 branchless,
- * bit2 force FBP weighting.  Branchless selects the same operator as the box
- * integral here (both are the exact integral of the piecewise-constant image);
- * this build evaluates it one way only. */
+ * bit2 force FBP weighting.  Branchless is the reference's branchless tracer
+ * (distanceDriven2DBranchless.cu): the forward projector traces the main axis
+ * alone (no 0.12 blend band), the parallel back projector likewise, and the
+ * back projectors interpolate the detector row at each pixel's v instead of
+ * truncating it.  Its prefix-sum interpolation is the same clamped box
+ * integral, evaluated here in FP64-accurate form rather than from FP32 prefix
+ * sums.  (Tomo entries: typeProjector 1 selects the reference's branchless
+ * tomo tracer, the same operator as the box integral.) */
 #define CTP_TYPE_FBP 0x1
 #define CTP_TYPE_BRANCHLESS 0x2
 #define CTP_TYPE_FORCE_FBP 0x4
@@ -368,6 +374,26 @@ int ctp_wait_timeouts(unsigned int* count);
    restores CTP_WAIT_POLLS_DEFAULT afterwards.  No counterpart in the
    reference. */
 int ctp_set_wait_limit(unsigned int first_chunk_polls);
+
+/* 16-bit affine sinogram storage (no counterpart in the reference).  Each of
+ * nrows rows of row_len samples (a view of one batch item: nv x nu samples)
+ * keeps lo = its minimum and step = (maximum - minimum) / 65535; a sample is
+ * the code round((y - lo) / step), read back as lo + step * code (error at
+ * most step / 2).  Half the bytes of FP32, like BF16/FP16, with a rounding
+ * error of 1/131070 of the view's range instead of the float formats'
+ * 2^-9 (BF16) or 2^-12 (FP16) of each value.  Asynchronous on the stream. */
+int ctp_quantize_u16(unsigned short* code, float* lo, float* step, const float* y, size_t nrows, size_t row_len,
+                     void* stream);
+/* y = lo + step * code, or y -= lo + step * code with CTP_FLAG_SUBTRACT (the
+ * residual A x - y of an SQS iteration). */
+int ctp_dequantize_u16(float* y, const unsigned short* code, const float* lo, const float* step, size_t nrows,
+                       size_t row_len, unsigned flags, void* stream);
+/* The exact (FP64) ramp filter of ctp_ramp_filter with CTP_FLAG_FILTER_EXACT
+ * on a sinogram in 16-bit affine storage (one lo / step per view of each batch
+ * item), dequantized as it is read; up to 3456 cells (CTP_ERR_UNSUPPORTED
+ * above). */
+int ctp_ramp_filter_u16(float* fprj, const unsigned short* code, const float* lo, const float* step,
+                        const ctp_geometry* g, int geom, int typeFilter, void* stream);
 
 /* Number of scratch allocations the library has made since it was loaded
    (stream-ordered pool, or cudaMallocAsync under graph capture), on every

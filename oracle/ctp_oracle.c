@@ -243,9 +243,11 @@ static double dd_sweep(const og_cell_rays* r, int ymain, const double* s0, const
     return acc;
 }
 
-/* One ray of DDFPTracing (distanceDriven2DBoxInt.cu:21-106) in any mode. */
+/* One ray of DDFPTracing (distanceDriven2DBoxInt.cu:21-106) in any mode.
+ * hard != 0: the branchless tracer's axis choice (distanceDriven2DBranchless.cu
+ * :56-120): the main axis alone by |cos| > |sin|, no blend band. */
 static double dd_ray(const og_cell_rays* r, double deg, double a, double z, const double* vol, double* out,
-                     double scat, long long* cnt, int mode, const og_grid* g)
+                     double scat, long long* cnt, int mode, const og_grid* g, int hard)
 {
     long iz, iz1;
     double wz;
@@ -257,13 +259,13 @@ static double dd_ray(const og_cell_rays* r, double deg, double a, double z, cons
     double* o1 = out ? out + iz1 * nxy : NULL;
     double c = cos(deg), s = sin(deg);
     double ac = fabs(c), as = fabs(s);
-    double wx = clampd((ac - as + DD_MARGIN) / (2 * DD_MARGIN), 0, 1);
+    double wx = hard ? (ac > as ? 1.0 : 0.0) : clampd((ac - as + DD_MARGIN) / (2 * DD_MARGIN), 0, 1);
     double valx = 0, valy = 0;
-    if (ac > as - DD_MARGIN) {
+    if (wx > 0) {
         double L = g->dy / fabs(cos(deg - a));
         valx = dd_sweep(r, 1, s0, s1, 1 - wz, wz, o0, o1, scat * L * wx, cnt, mode, g) * L;
     }
-    if (ac < as + DD_MARGIN) {
+    if (wx < 1) {
         double L = g->dx / fabs(sin(deg - a));
         valy = dd_sweep(r, 0, s0, s1, 1 - wz, wz, o0, o1, scat * L * (1 - wx), cnt, mode, g) * L;
     }
@@ -276,9 +278,11 @@ static double fan_zpos(long iv, const og_det* d, const og_grid* g) /* distanceDr
     return (z - g->cz) / g->dz + g->nz / 2.0 - 0.5;
 }
 
-/* fan: geom 0, parallel: geom 1.  Forward projection, writes prj (=). */
-void oracle_dd2d_fp(double* prj, const double* img, const double* deg, long nb, og_grid g, og_det d,
-                    long nview, double dsd, double dso, int geom)
+/* fan: geom 0, parallel: geom 1.  Forward projection, writes prj (=);
+ * branchless != 0 traces like distanceDriven2DBranchless.cu:56-258 (the
+ * prefix-sum interpolation there is the same clamped box integral). */
+void oracle_dd2d_fp_mode(double* prj, const double* img, const double* deg, long nb, og_grid g, og_det d,
+                         long nview, double dsd, double dso, int geom, int branchless)
 {
     long nxyz = g.nx * g.ny * g.nz;
     long nrays = d.nu * d.nv * nview;
@@ -290,8 +294,14 @@ void oracle_dd2d_fp(double* prj, const double* img, const double* deg, long nb, 
         double a = 0;
         if (geom == 0) fan_cell(&r, &a, deg[iview], iu, &g, &d, dsd, dso);
         else par_cell(&r, deg[iview], iu, &g, &d);
-        prj[t] = dd_ray(&r, deg[iview], a, fan_zpos(iv, &d, &g), img + ib * nxyz, NULL, 0, NULL, 0, &g);
+        prj[t] = dd_ray(&r, deg[iview], a, fan_zpos(iv, &d, &g), img + ib * nxyz, NULL, 0, NULL, 0, &g, branchless);
     }
+}
+
+void oracle_dd2d_fp(double* prj, const double* img, const double* deg, long nb, og_grid g, og_det d,
+                    long nview, double dsd, double dso, int geom)
+{
+    oracle_dd2d_fp_mode(prj, img, deg, nb, g, d, nview, dsd, dso, geom, 0);
 }
 
 /* Exact transpose of oracle_dd2d_fp: img += A^T prj. */
@@ -323,7 +333,7 @@ void oracle_dd2d_bp_adjoint(double* img, const double* prj, const double* deg, l
                         double a = 0;
                         if (geom == 0) fan_cell(&r, &a, deg[iview], iu, &g, &d, dsd, dso);
                         else par_cell(&r, deg[iview], iu, &g, &d);
-                        dd_ray(&r, deg[iview], a, fan_zpos(iv, &d, &g), NULL, acc, p, NULL, 1, &g);
+                        dd_ray(&r, deg[iview], a, fan_zpos(iv, &d, &g), NULL, acc, p, NULL, 1, &g, 0);
                     }
                 }
             }
@@ -349,7 +359,7 @@ long long oracle_dd2d_nnz(const double* deg, og_grid g, og_det d, long nview, do
                 double a = 0;
                 if (geom == 0) fan_cell(&r, &a, deg[iview], iu, &g, &d, dsd, dso);
                 else par_cell(&r, deg[iview], iu, &g, &d);
-                dd_ray(&r, deg[iview], a, fan_zpos(iv, &d, &g), NULL, NULL, 0, &cnt, 2, &g);
+                dd_ray(&r, deg[iview], a, fan_zpos(iv, &d, &g), NULL, NULL, 0, &cnt, 2, &g, 0);
             }
         total += cnt;
     }
@@ -369,12 +379,71 @@ static double preweight(double deg, long iu, const og_det* d, const og_grid* g, 
     return g->dx / fabs(sin(deg - a));
 }
 
+/* Normalised box integral of one pre-weighted detector row over the
+ * projection of pixel (xc, yc) for one view: DDBPFanKernel
+ * distanceDriven2DBoxInt.cu:354-390 + utils :96-116 (fan, hard axis switch),
+ * DDBPParallelKernel :440-491 (parallel: blend band, or the branchless hard
+ * switch, distanceDriven2DBranchless.cu:509-530). */
+static double bp_row(const double* row, const double* wr, double c, double s, double xc, double yc,
+                     const og_grid* g, const og_det* d, double dso, int geom, int fbp, int hard)
+{
+    double x1 = xc - g->dx / 2, x2 = xc + g->dx / 2, y1 = yc - g->dy / 2, y2 = yc + g->dy / 2;
+    if (geom == 0) {
+        double a1, a2;
+        if (fabs(c) > fabs(s)) {
+            a1 = atan((x1 * c + yc * s) / ((-x1 * s + yc * c) + dso));
+            a2 = atan((x2 * c + yc * s) / ((-x2 * s + yc * c) + dso));
+        } else {
+            a1 = atan((xc * c + y1 * s) / ((-xc * s + y1 * c) + dso));
+            a2 = atan((xc * c + y2 * s) / ((-xc * s + y2 * c) + dso));
+        }
+        a1 = -(a1 / d->du + d->off_u) + d->nu / 2.0;
+        a2 = -(a2 / d->du + d->off_u) + d->nu / 2.0;
+        if (a1 > a2) { double t = a1; a1 = a2; a2 = t; }
+        /* integral of the pre-weighted row */
+        double v = 0;
+        double c1 = clampd(a1, 0, (double)d->nu), c2 = clampd(a2, 0, (double)d->nu);
+        if (c2 > c1) {
+            long i1 = clampi((long)c1, 0, d->nu), i2 = clampi((long)c2, 0, d->nu);
+            for (long i = i1; i <= i2; i++) v += row[i] * wr[i];
+            v -= row[i1] * wr[i1] * (c1 - i1) + row[i2] * wr[i2] * (i2 + 1 - c2);
+        }
+        v /= (a2 - a1);
+        if (fbp) {
+            double rx = xc * c + yc * s, ry = -xc * s + yc * c;
+            v *= dso * dso / (rx * rx + (dso + ry) * (dso + ry));
+        }
+        return v;
+    }
+    double valx = 0, valy = 0;
+    double wv = wr[0];
+    double wx = hard ? (fabs(c) > fabs(s) ? 1.0 : 0.0) : clampd((fabs(c) - fabs(s) + DD_MARGIN) / (2 * DD_MARGIN), 0, 1);
+    if (wx > 0) {
+        double u1 = -((x1 * c + yc * s) / d->du + d->off_u) + d->nu / 2.0;
+        double u2 = -((x2 * c + yc * s) / d->du + d->off_u) + d->nu / 2.0;
+        if (u1 > u2) { double t = u1; u1 = u2; u2 = t; }
+        valx = box1d(row, 1, u1, u2, d->nu) * wv / (u2 - u1);
+    }
+    if (wx < 1) {
+        double u1 = -((xc * c + y1 * s) / d->du + d->off_u) + d->nu / 2.0;
+        double u2 = -((xc * c + y2 * s) / d->du + d->off_u) + d->nu / 2.0;
+        if (u1 > u2) { double t = u1; u1 = u2; u2 = t; }
+        valy = box1d(row, 1, u1, u2, d->nu) * wv / (u2 - u1);
+    }
+    return valx * wx + valy * (1 - wx);
+}
+
 /* Fan: DDBPFanKernel distanceDriven2DBoxInt.cu:319-396 + utils :96-116.
  * Parallel: DDBPParallelKernel :409-497.  img += BP(prj).
- * fbp != 0 selects the FBP weighting (no pre-weight; fan adds dso^2/L^2). */
-void oracle_dd2d_bp(double* img, const double* prj, const double* deg, long nb, og_grid g, og_det d,
-                    long nview, double dsd, double dso, int geom, int fbp)
+ * fbp != 0 selects the FBP weighting (no pre-weight; fan adds dso^2/L^2).
+ * branchless != 0: distanceDriven2DBranchless.cu:384-530 -- the parallel
+ * beam's hard axis switch, and the detector row interpolated linearly at the
+ * pixel's v (InterpolateXY of the row prefix sums, cudaMath.cu:227-258: rows
+ * clamped to [0, nv-1]) where the box-integral mode truncates it. */
+void oracle_dd2d_bp_mode(double* img, const double* prj, const double* deg, long nb, og_grid g, og_det d,
+                         long nview, double dsd, double dso, int geom, int fbp, int branchless)
 {
+    (void)dsd;
     long nxyz = g.nx * g.ny * g.nz;
     long nprj = nview * d.nv * d.nu;
     double* w = (double*)malloc(sizeof(double) * nview * d.nu);
@@ -386,71 +455,44 @@ void oracle_dd2d_bp(double* img, const double* prj, const double* deg, long nb, 
             const double* p = prj + ib * nprj;
             double zc = (iz - g.nz / 2.0) * g.dz + g.cz + g.dz / 2;
             double ivf = zc / d.dv + d.off_v + d.nv / 2.0 - 0.5;
-            long iv = (long)ivf; /* float -> int parameter: truncation, :383 */
-            if (iv < 0 || iv >= d.nv) continue; /* reference reads outside the view here */
+            long iv0, iv1;
+            double wv1;
+            if (branchless) {
+                double v = clampd(ivf, 0, (double)d.nv);
+                iv0 = (long)v;
+                iv1 = clampi(iv0 + 1, 0, d.nv);
+                iv0 = clampi(iv0, 0, d.nv);
+                wv1 = v - iv0;
+            } else {
+                iv0 = iv1 = (long)ivf; /* float -> int parameter: truncation, :383 */
+                wv1 = 0;
+                if (iv0 < 0 || iv0 >= d.nv) continue; /* reference reads outside the view here */
+            }
             for (long iy = 0; iy < g.ny; iy++)
                 for (long ix = 0; ix < g.nx; ix++) {
                     double xc = (ix - g.nx / 2.0) * g.dx + g.cx + g.dx / 2;
                     double yc = (iy - g.ny / 2.0) * g.dy + g.cy + g.dy / 2;
-                    double x1 = xc - g.dx / 2, x2 = xc + g.dx / 2, y1 = yc - g.dy / 2, y2 = yc + g.dy / 2;
                     double acc = 0;
                     for (long iview = 0; iview < nview; iview++) {
                         double c = cos(deg[iview]), s = sin(deg[iview]);
-                        const double* row = p + (iview * d.nv + iv) * d.nu;
                         const double* wr = w + iview * d.nu;
-                        double tmp[1];
-                        (void)tmp;
-                        if (geom == 0) {
-                            double a1, a2;
-                            if (fabs(c) > fabs(s)) {
-                                a1 = atan((x1 * c + yc * s) / ((-x1 * s + yc * c) + dso));
-                                a2 = atan((x2 * c + yc * s) / ((-x2 * s + yc * c) + dso));
-                            } else {
-                                a1 = atan((xc * c + y1 * s) / ((-xc * s + y1 * c) + dso));
-                                a2 = atan((xc * c + y2 * s) / ((-xc * s + y2 * c) + dso));
-                            }
-                            a1 = -(a1 / d.du + d.off_u) + d.nu / 2.0;
-                            a2 = -(a2 / d.du + d.off_u) + d.nu / 2.0;
-                            if (a1 > a2) { double t = a1; a1 = a2; a2 = t; }
-                            /* integral of the pre-weighted row */
-                            double v = 0;
-                            {
-                                double c1 = clampd(a1, 0, (double)d.nu), c2 = clampd(a2, 0, (double)d.nu);
-                                if (c2 > c1) {
-                                    long i1 = clampi((long)c1, 0, d.nu), i2 = clampi((long)c2, 0, d.nu);
-                                    for (long i = i1; i <= i2; i++) v += row[i] * wr[i];
-                                    v -= row[i1] * wr[i1] * (c1 - i1) + row[i2] * wr[i2] * (i2 + 1 - c2);
-                                }
-                            }
-                            v /= (a2 - a1);
-                            if (fbp) {
-                                double rx = xc * c + yc * s, ry = -xc * s + yc * c;
-                                v *= dso * dso / (rx * rx + (dso + ry) * (dso + ry));
-                            }
-                            acc += v;
-                        } else {
-                            double valx = 0, valy = 0;
-                            double wv = wr[0];
-                            if (fabs(c) > fabs(s) - DD_MARGIN) {
-                                double u1 = -((x1 * c + yc * s) / d.du + d.off_u) + d.nu / 2.0;
-                                double u2 = -((x2 * c + yc * s) / d.du + d.off_u) + d.nu / 2.0;
-                                if (u1 > u2) { double t = u1; u1 = u2; u2 = t; }
-                                valx = box1d(row, 1, u1, u2, d.nu) * wv / (u2 - u1);
-                            }
-                            if (fabs(c) < fabs(s) + DD_MARGIN) {
-                                double u1 = -((xc * c + y1 * s) / d.du + d.off_u) + d.nu / 2.0;
-                                double u2 = -((xc * c + y2 * s) / d.du + d.off_u) + d.nu / 2.0;
-                                if (u1 > u2) { double t = u1; u1 = u2; u2 = t; }
-                                valy = box1d(row, 1, u1, u2, d.nu) * wv / (u2 - u1);
-                            }
-                            double wx = clampd((fabs(c) - fabs(s) + DD_MARGIN) / (2 * DD_MARGIN), 0, 1);
-                            acc += valx * wx + valy * (1 - wx);
-                        }
+                        double v0 = bp_row(p + (iview * d.nv + iv0) * d.nu, wr, c, s, xc, yc, &g, &d, dso, geom, fbp,
+                                           branchless);
+                        if (wv1 != 0)
+                            v0 = v0 * (1 - wv1) + wv1 * bp_row(p + (iview * d.nv + iv1) * d.nu, wr, c, s, xc, yc,
+                                                               &g, &d, dso, geom, fbp, branchless);
+                        acc += v0;
                     }
                     img[ib * nxyz + (iz * g.ny + iy) * g.nx + ix] += acc;
                 }
         }
     free(w);
+}
+
+void oracle_dd2d_bp(double* img, const double* prj, const double* deg, long nb, og_grid g, og_det d,
+                    long nview, double dsd, double dso, int geom, int fbp)
+{
+    oracle_dd2d_bp_mode(img, prj, deg, nb, g, d, nview, dsd, dso, geom, fbp, 0);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -58,10 +58,13 @@ def lib():
         dp = POINTER(c_double)
         fp = POINTER(c_float)
         L.oracle_dd2d_fp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int]
+        L.oracle_dd2d_fp_mode.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int, c_int]
         L.oracle_dd2d_bp_adjoint.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int]
         L.oracle_dd2d_nnz.argtypes = [dp, _Grid, _Det, c_long, c_double, c_double, c_int]
         L.oracle_dd2d_nnz.restype = c_longlong
         L.oracle_dd2d_bp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int, c_int]
+        L.oracle_dd2d_bp_mode.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double, c_int, c_int,
+                                          c_int]
         L.oracle_fbp_fan_bp.argtypes = [dp, dp, dp, c_long, _Grid, _Det, c_long, c_double, c_double]
         L.oracle_siddon_fp.argtypes = [dp, dp, fp, fp, fp, fp, c_long, _Grid, _Det, c_long]
         L.oracle_siddon_bp.argtypes = [dp, dp, fp, fp, fp, fp, c_long, _Grid, _Det, c_long]
@@ -111,9 +114,11 @@ def _fan_da(p):
 
 
 # --------------------------------------------------------------------------- DD 2D
-def dd_fp(p, img, angles, geom: str):
+def dd_fp(p, img, angles, geom: str, branchless=False):
     """Fan (geom='fan') or parallel DD forward projection.  Mirrors
-    fan_equiangular.distance_driven_fp / parallel.distance_driven_fp."""
+    fan_equiangular.distance_driven_fp / parallel.distance_driven_fp;
+    branchless=True traces like the reference's branchless mode (the main
+    axis alone, no blend band)."""
     img = _d(img)
     ang = _d(angles)
     nb = img.shape[0]
@@ -121,17 +126,20 @@ def dd_fp(p, img, angles, geom: str):
     g = _grid(p, img.shape[1:])
     if geom == "fan":
         d = _det(p, p.nu, p.nv, _fan_da(p))
-        lib().oracle_dd2d_fp(_ptr(prj), _ptr(img), _ptr(ang), nb, g, d, len(ang), float(np.float32(p.dsd)),
-                             float(np.float32(p.dso)), 0)
+        lib().oracle_dd2d_fp_mode(_ptr(prj), _ptr(img), _ptr(ang), nb, g, d, len(ang), float(np.float32(p.dsd)),
+                                  float(np.float32(p.dso)), 0, int(bool(branchless)))
     else:
         d = _det(p, p.nu, p.nv)
-        lib().oracle_dd2d_fp(_ptr(prj), _ptr(img), _ptr(ang), nb, g, d, len(ang), 1000.0, 500.0, 1)
+        lib().oracle_dd2d_fp_mode(_ptr(prj), _ptr(img), _ptr(ang), nb, g, d, len(ang), 1000.0, 500.0, 1,
+                                  int(bool(branchless)))
     return prj
 
 
-def dd_bp(p, prj, angles, geom: str, is_fbp=False, adjoint=False):
+def dd_bp(p, prj, angles, geom: str, is_fbp=False, adjoint=False, branchless=False):
     """DD back projection: reference-parity normalised mode, FBP mode, or the
-    exact transpose of dd_fp (adjoint=True)."""
+    exact transpose of dd_fp (adjoint=True); branchless=True as the
+    reference's branchless mode (parallel: no blend band; detector rows
+    interpolated at the pixel's v)."""
     prj = _d(prj)
     ang = _d(angles)
     nb, nview, nv, nu = prj.shape
@@ -146,7 +154,8 @@ def dd_bp(p, prj, angles, geom: str, is_fbp=False, adjoint=False):
     if adjoint:
         lib().oracle_dd2d_bp_adjoint(_ptr(img), _ptr(prj), _ptr(ang), nb, g, d, nview, dsd, dso, gi)
     else:
-        lib().oracle_dd2d_bp(_ptr(img), _ptr(prj), _ptr(ang), nb, g, d, nview, dsd, dso, gi, int(bool(is_fbp)))
+        lib().oracle_dd2d_bp_mode(_ptr(img), _ptr(prj), _ptr(ang), nb, g, d, nview, dsd, dso, gi, int(bool(is_fbp)),
+                                  int(bool(branchless)))
     return img
 
 

@@ -7,6 +7,7 @@ wrappers (ct_projector/projector/numpy/*.py), on the seeded cases of
 cases.py, and stores inputs and outputs.  Needs a GPU:
 
     python tests/golden/make_golden.py [--out DIR] [--only CASE ...]   # default: tests/golden
+    python tests/golden/make_golden.py --branchless [--out DIR]         # branchless_*.npz
 
 This script is test infrastructure; the product never runs the reference.
 """
@@ -205,17 +206,65 @@ def run_case(ref: Ref, fn):
     return name, {**{f"in_{k}": v for k, v in inp.items()}, **{f"ref_{k}": v for k, v in out.items()}, **geom_attrs}
 
 
+# the branchless distance-driven modes (typeProjector bit 1 of the 2D entries,
+# distanceDriven2D.cu:18-19; typeProjector 1 of the tomo entries, which the
+# reference's tomo modules set for branchless=True, tomo.py:48-51)
+BRANCHLESS_CASES = ("fan_basic", "fan_offsets", "par_basic", "par_offsets", "par_wide", "fan_wide", "tomo")
+
+
+def run_branchless(ref: Ref, fn):
+    """The reference's branchless outputs on a case's inputs.  Tomo: batch item
+    0 only, and the back projection of one view, because the reference's tomo
+    branchless path indexes a one-item accumulation buffer by the batch item
+    (distanceDriven3DBranchless.cu:209) and pre-weights only view 0
+    (distanceDriven3DBranchless.cu:347)."""
+    name, p, inp = fn()
+    out = {}
+    if name == "tomo":
+        img = inp["img"][:1]
+        dc, src = inp["det_center"], inp["src"]
+        prj = np.zeros([1, dc.shape[0], p.nv, p.nu], np.float32)
+        ref.call("cDistanceDrivenTomoProjection", ptr(prj), ptr(img), ptr(dc), ptr(src),
+                 *geom(p, 1, img.shape[1:], prj.shape[1:]), c_float(p.du), c_float(p.dv), c_float(p.off_u),
+                 c_float(p.off_v), c_int(1))
+        out["fp"] = prj
+        dc1, src1 = np.ascontiguousarray(dc[:1]), np.ascontiguousarray(src[:1])
+        prj1 = np.ascontiguousarray(prj[:, :1])
+        bimg = np.zeros([1, p.nz, p.ny, p.nx], np.float32)
+        ref.call("cDistanceDrivenTomoBackprojection", ptr(bimg), ptr(prj1), ptr(dc1), ptr(src1),
+                 *geom(p, 1, bimg.shape[1:], prj1.shape[1:]), c_float(p.du), c_float(p.dv), c_float(p.off_u),
+                 c_float(p.off_v), c_int(1))
+        out["bp_view0"] = bimg
+        inp = dict(inp, img=img)
+    else:
+        fan = name.startswith("fan")
+        img, ang = inp["img"], inp["angles"]
+        prj = ref.dd_fp(p, img, ang, fan, 2)
+        out["fp"] = prj
+        out["bp"] = ref.dd_bp(p, prj, ang, fan, 2)
+        out["bp_fbp"] = ref.dd_bp(p, prj, ang, fan, 3)
+    geom_attrs = {f"geom_{k}": np.asarray(v) for k, v in p.as_dict().items()}
+    return f"branchless_{name}", {**{f"in_{k}": v for k, v in inp.items()},
+                                  **{f"ref_{k}": v for k, v in out.items()}, **geom_attrs}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--only", nargs="*", default=None, help="case names to (re)generate")
+    ap.add_argument("--branchless", action="store_true", help="write the branchless fixtures only")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     ref = Ref(REF_LIB)
     for fn in cases.ALL:
         if a.only and fn.__name__[5:] not in a.only:
             continue
-        name, arrays = run_case(ref, fn)
+        if a.branchless:
+            if fn.__name__[5:] not in BRANCHLESS_CASES:
+                continue
+            name, arrays = run_branchless(ref, fn)
+        else:
+            name, arrays = run_case(ref, fn)
         path = os.path.join(a.out, f"{name}.npz")
         np.savez_compressed(path, **arrays)
         print(f"wrote {path}: " + ", ".join(f"{k}{list(v.shape)}" for k, v in arrays.items() if k.startswith("ref_")))

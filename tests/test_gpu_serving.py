@@ -1,7 +1,11 @@
 """The continuous-batching reconstruction server on the GPU: fused SQS-TV
 update against the FP64 oracle, served results against FP64 reconstructions
 (tolerance 1e-4 relative L2), each result the same alone and in the mix,
-jobs joining a running lane, admission by HBM budget, low-precision storage."""
+jobs joining a running lane, admission by HBM budget, low-precision storage.
+
+The oracle always reconstructs from the FP32 sinogram a job was made from,
+before any storage rounding, so a low-precision storage format's rounding
+counts as error."""
 import numpy as np
 import pytest
 
@@ -39,7 +43,8 @@ def _protocols(n_iter=6, storage="float32"):
 
 
 def _sinogram(proto, nz, seed):
-    """Seeded phantom projected by the FP32 projector, with noise, on the host."""
+    """Seeded phantom projected by the FP32 projector, with noise, on the host:
+    (the sinogram in the protocol's storage, the FP32 sinogram)."""
     from ctprojector_b200 import synthetic as S
     from ctprojector_b200.projector import _device as D
     from ctprojector_b200.serving import DTYPES
@@ -56,7 +61,11 @@ def _sinogram(proto, nz, seed):
         y = D.dd_fp(s, torch.tensor(img, device="cuda"), torch.tensor(proto.angles, device="cuda"), geom)
     y = y.cpu()
     y = y + 0.01 * y.abs().max() * torch.tensor(rng.standard_normal(y.shape), dtype=torch.float32)
-    return y.to(DTYPES[proto.storage]).pin_memory()
+    if proto.storage == "q16":
+        from ctprojector_b200 import quant
+
+        return quant.quantize(y.cuda()).cpu().pin_memory(), y
+    return y.to(DTYPES[proto.storage]).pin_memory(), y
 
 
 def _jobs(protos, spec, seed0=0):
@@ -66,15 +75,18 @@ def _jobs(protos, spec, seed0=0):
     for i, (name, nz, t) in enumerate(spec):
         p = protos[name]
         nz = 1 if p.kind == "cone" else nz
-        jobs.append(Job(i, p, _sinogram(p, nz, seed0 + i), arrival=t, nz=nz))
+        stored, y32 = _sinogram(p, nz, seed0 + i)
+        jobs.append(Job(i, p, stored, arrival=t, nz=nz, tag=y32))
     return jobs
 
 
-def _oracle_result(job):
+def _oracle_result(job, y32=None):
+    """FP64 reconstruction of the job's FP32 sinogram (``y32``, or the job's
+    tag), before storage rounding."""
     from oracle import recon as R
 
     p = job.protocol
-    y = job.sinogram.float().numpy().astype(np.float64)
+    y = (job.tag if y32 is None else y32).float().numpy().astype(np.float64)
     if p.algo == "fbp":
         return R.fbp(p.scan, p.kind, y, p.angles, p.filter)
     geo = p.cone if p.kind == "cone" else p.angles
@@ -186,19 +198,30 @@ def test_admission_waits_for_memory():
     eng.close()
 
 
-@pytest.mark.parametrize("storage", ["bfloat16", "float16"])
+# Rounding of 16-bit sinogram storage against the FP32-input FP64 oracle: the
+# affine codes (q16) meet SERVE_TOL; BF16 and FP16 (relative rounding 2^-9 and
+# 2^-12, magnified by the ramp filter of the FBP jobs) do not, and are held to
+# these measured ceilings instead.
+LOWP_CEILING = {"q16": SERVE_TOL, "float16": 3e-3, "bfloat16": 3e-2}
+
+
+@pytest.mark.parametrize("storage", ["q16", "float16", "bfloat16"])
 def test_low_precision_sinogram_storage(storage):
-    """Sinograms held in bf16/fp16 on the device, iterate and sums in FP32:
-    the result matches the FP64 reconstruction of the same stored values."""
+    """Sinograms held in 16 bits on the device, iterate and sums in FP32,
+    against the FP64 reconstruction of the FP32 sinogram."""
     from ctprojector_b200.serving import Engine
 
     protos = _protocols(storage=storage)
-    jobs = _jobs(protos, [("fan_sqs", 2, 0.0), ("par_fbp", 2, 0.0), ("cone_sqs", 1, 0.0)])
+    jobs = _jobs(protos, [("fan_sqs", 2, 0.0), ("par_fbp", 2, 0.0), ("cone_sqs", 1, 0.0), ("fan_fbp", 1, 0.0)])
     eng = Engine()
     eng.run(jobs, realtime=False)
+    errs = {}
     for job in jobs:
-        assert job.sinogram.dtype != torch.float32
-        assert rel_l2(job.result.numpy(), _oracle_result(job)) <= SERVE_TOL
+        dt = job.sinogram.code.dtype if storage == "q16" else job.sinogram.dtype
+        assert dt != torch.float32
+        errs[job.protocol.name] = rel_l2(job.result.numpy(), _oracle_result(job))
+    print(storage, {k: f"{v:.3g}" for k, v in errs.items()})
+    assert all(e <= LOWP_CEILING[storage] for e in errs.values()), errs
     eng.close()
 
 
@@ -216,19 +239,24 @@ def test_per_call_path_matches_server():
 
 
 def test_full_size_protocols_match_fp64_oracle():
-    """The served stream's own protocols at full size (bf16 sinograms): the
-    results of the jobs the FP64 oracle reconstructs in seconds are within
-    1e-4 of it (relative L2)."""
+    """The served stream's own protocols at full size, with the sinograms in
+    the served storage (q16): the results of the jobs the FP64 oracle
+    reconstructs in seconds are within 1e-4 of its reconstruction of the FP32
+    sinograms (relative L2)."""
+    from ctprojector_b200 import quant
     from ctprojector_b200.serving import Engine
     from ctprojector_b200.serving import workload as W
 
-    protos = W.catalog(storage="bfloat16")
+    p32 = W.catalog(storage="float32")
+    protos = W.catalog(storage="q16")
     stream = [(0.0, "fan256_sqs", 1), (0.0, "fan256_fbp", 2), (0.0, "par512_fbp", 1), (0.0, "fan512_fbp", 1)]
-    pools = {n: W.sinogram_pool(protos[n], 1, 2, seed=i) for i, (_, n, _) in enumerate(stream)}
+    pools32 = {n: W.sinogram_pool(p32[n], 1, 2, seed=i) for i, (_, n, _) in enumerate(stream)}
+    pools = {n: [quant.quantize(t.cuda()).cpu().pin_memory() for t in v] for n, v in pools32.items()}
     jobs = W.make_jobs(protos, stream, pools)
     eng = Engine()
     eng.run(jobs, realtime=False)
     for job in jobs:
-        err = rel_l2(job.result.numpy(), _oracle_result(job))
+        name, k = job.tag
+        err = rel_l2(job.result.numpy(), _oracle_result(job, pools32[name][k][:job.nz]))
         assert err <= SERVE_TOL, (job.protocol.name, err)
     eng.close()

@@ -118,3 +118,36 @@ def test_latency_stats():
     assert s["jobs"] == 100
     assert s["recons_per_s"] == pytest.approx(100 / 1.99)
     assert s["p99_ms"] == pytest.approx(99.0)
+
+
+def test_q16_storage_is_a_sinogram_format_only():
+    import numpy as np
+
+    from ctprojector_b200 import synthetic as S
+    from ctprojector_b200.serving import Protocol
+
+    scan = S.Scan(32, 32, 1, 1.0, 1.0, 1.0, 48, 1, 1.0, 1.0, 10)
+    ang = S.angles(10, np.pi)
+    assert Protocol("p", "parallel", "sqs", scan, angles=ang, storage="q16").storage == "q16"
+    with pytest.raises(ValueError):
+        Protocol("p", "parallel", "sqs", scan, angles=ang, image_storage="q16")
+    with pytest.raises(ValueError):
+        Protocol("p", "parallel", "sqs", scan, angles=ang, storage="int8")
+
+
+def test_q16_host_values_and_slices():
+    import torch
+
+    from ctprojector_b200.quant import Q16
+
+    code = torch.tensor([[[[0, -1, 32767, 2]]], [[[5, 6, 7, 8]]]], dtype=torch.int16)  # -1 is code 65535
+    lo = torch.tensor([[1.0], [-2.0]])
+    step = torch.tensor([[0.5], [0.25]])
+    q = Q16(code, lo, step)
+    v = q.float()
+    assert v.dtype == torch.float32 and tuple(v.shape) == (2, 1, 1, 4)
+    assert v[0, 0, 0].tolist() == [1.0, 1.0 + 0.5 * 65535, 1.0 + 0.5 * 32767, 2.0]
+    assert v[1, 0, 0].tolist() == [-2.0 + 0.25 * k for k in (5, 6, 7, 8)]
+    one = q[1:]
+    assert tuple(one.shape) == (1, 1, 1, 4) and tuple(one.lo.shape) == (1, 1)
+    assert one.nbytes == 4 * 2 + 2 * 4
