@@ -112,10 +112,15 @@ class Protocol:
 class Job:
     """One reconstruction request.  ``sinogram`` is a host tensor of
     ``protocol.sinogram_shape(nz)`` in any float type, or a ``quant.Q16`` for
-    q16 protocols (it is stored in the
-    protocol's storage type on the device); ``arrival`` is in seconds from the
-    start of the stream.  The server fills ``result`` ([nz, ny, nx] float32,
-    host) and ``t_done``."""
+    q16 protocols (it is stored in the protocol's storage type on the device);
+    ``arrival`` is in seconds from the start of the stream.  The server fills
+    ``result`` ([nz, ny, nx] float32, host) and ``t_done``.
+
+    ``deadline`` (seconds after arrival) bounds the wait of a client: a job not
+    finished by then is cancelled with status "timeout".  ``resume`` continues
+    an SQS job from a ``Snapshot`` taken by ``Engine.evict``.  ``status`` is
+    one of new, queued, running, done, rejected (malformed), cancelled,
+    timeout, evicted or failed (``error`` says why)."""
 
     job_id: int
     protocol: Protocol
@@ -127,6 +132,10 @@ class Job:
     t_done: float = float("nan")
     done_event: Optional[torch.cuda.Event] = field(default=None, repr=False)
     tag: object = None  # free for the caller (the synthetic streams record the data source)
+    deadline: Optional[float] = None
+    resume: Optional["Snapshot"] = field(default=None, repr=False)
+    status: str = "new"
+    error: Optional[str] = None
 
     @property
     def units(self) -> int:
@@ -135,6 +144,28 @@ class Job:
     @property
     def latency(self) -> float:
         return self.t_done - self.arrival
+
+
+@dataclass(eq=False)
+class Snapshot:
+    """The state of an evicted SQS job: its iterate after ``done`` iterations
+    (pinned host [units * slices per unit, ny, nx], valid once ``event`` has
+    completed) and the job itself (protocol, sinogram, slices).  ``job()``
+    makes the job that resumes it; the resumed job's result equals the
+    uninterrupted one's."""
+
+    source: Job
+    x: torch.Tensor
+    done: int
+    event: torch.cuda.Event = field(repr=False)
+
+    def ready(self) -> bool:
+        return self.event.query()
+
+    def job(self, arrival: float = 0.0, job_id: Optional[int] = None, deadline: Optional[float] = None) -> Job:
+        j = self.source
+        return Job(j.job_id if job_id is None else job_id, j.protocol, j.sinogram, arrival=arrival, nz=j.nz,
+                   tag=j.tag, deadline=deadline, resume=self)
 
 
 def _zlink_pattern(n: int) -> torch.Tensor:
@@ -224,6 +255,34 @@ class Lane:
             self.ystep[start:start + n].copy_(sino.step.reshape(n, -1), non_blocking=True)
         else:
             dst.copy_(sino.reshape(dst.shape), non_blocking=True)
+
+    def _bufs(self) -> List[torch.Tensor]:
+        """Per-slot device buffers that move with their jobs when slots are
+        packed and are zeroed when freed."""
+        return self._ybufs()
+
+    def _release(self, job_ids: Sequence[int], old_hw: int) -> None:
+        """Free the slots of ``job_ids`` (already removed from ``self.jobs``),
+        pack the live slots to the front and zero the freed tail (lane stream)."""
+        for jid in job_ids:
+            self.pool.free(jid)
+        with torch.cuda.stream(self.stream):
+            self._apply_moves(self.pool.compact())
+            new_hw = self.pool.high_water
+            if new_hw < old_hw:
+                for t in self._bufs():
+                    t[new_hw:old_hw].zero_()
+                self._clear_extra(new_hw, old_hw)
+
+    def _clear_extra(self, lo: int, hi: int) -> None:
+        pass
+
+    def drop(self, job_id: int) -> Job:
+        """Remove a running job without a result (cancellation, eviction)."""
+        job = self.jobs.pop(job_id)[0]
+        self._release([job_id], self.pool.high_water)
+        self._record()
+        return job
 
     @staticmethod
     def sinogram_bytes(p: Protocol, sino: int) -> int:
@@ -339,25 +398,49 @@ class SQSLane(Lane):
             self._apply_moves(self.pool.compact())
             start = self.pool.alloc(job.job_id, job.units)
         n = job.units
+        snap = job.resume
         with torch.cuda.stream(self.stream):
             self._load_sinogram(start, n, job.sinogram)
-            self.x[self.cur][start:start + n].zero_()
+            xs = self.x[self.cur][start:start + n]
+            if snap is None:
+                xs.zero_()
+            else:  # continue from the snapshot's iterate
+                xs.copy_(snap.x.reshape(xs.shape), non_blocking=True)
             if self.xlp is not None:
-                self.xlp[self.cur][start:start + n].zero_()
+                self.xlp[self.cur][start:start + n].copy_(xs)
             if p.kind != "cone":
                 _set_zlinks(self.zlink[start:start + n])
-        self.jobs[job.job_id] = [job, p.n_iter]
+        self.jobs[job.job_id] = [job, p.n_iter - (snap.done if snap is not None else 0)]
+
+    def _bufs(self) -> List[torch.Tensor]:
+        return self._ybufs() + [self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else [])
+
+    def _clear_extra(self, lo: int, hi: int) -> None:
+        if self.p.kind != "cone":
+            self.zlink[lo:hi].zero_()
 
     def _apply_moves(self, moves):
         if not moves:
             return
         with torch.cuda.stream(self.stream):
-            bufs = self._ybufs() + [self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else [])
+            bufs = self._bufs()
             for m in moves:
                 for t in bufs:
                     t[m.dst:m.dst + m.n].copy_(t[m.src:m.src + m.n].clone())
                 if self.p.kind != "cone":
                     self.zlink[m.dst:m.dst + m.n].copy_(self.zlink[m.src:m.src + m.n].clone())
+
+    def snapshot(self, job_id: int) -> "Snapshot":
+        """Copy a running job's current iterate to pinned host memory (lane
+        stream) with its iteration count."""
+        job, left = self.jobs[job_id]
+        start, n = self.pool.range_of(job_id)
+        x = torch.empty((n * self.p.slices_per_unit, self.ny, self.nx), pin_memory=True)
+        with torch.cuda.stream(self.stream):
+            x.copy_(self.x[self.cur][start:start + n].reshape(x.shape), non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        return Snapshot(job, x, self.p.n_iter - left, ev)
 
     def step(self) -> List[Job]:
         hw = self.pool.high_water
@@ -373,20 +456,13 @@ class SQSLane(Lane):
         if done:
             with torch.cuda.stream(self.stream):
                 for job in done:
-                    start, n = self.pool.free(job.job_id)
+                    start, n = self.pool.range_of(job.job_id)
                     del self.jobs[job.job_id]
                     job.result = torch.empty((n * self.p.slices_per_unit, self.ny, self.nx), pin_memory=True)
                     job.result.copy_(self.x[self.cur][start:start + n].reshape(job.result.shape), non_blocking=True)
                     job.done_event = torch.cuda.Event()
                     job.done_event.record(self.stream)
-                old_hw = hw
-                self._apply_moves(self.pool.compact())
-                new_hw = self.pool.high_water
-                if new_hw < old_hw:
-                    for t in self._ybufs() + [self.x[self.cur]] + ([self.xlp[self.cur]] if self.xlp is not None else []):
-                        t[new_hw:old_hw].zero_()
-                    if self.p.kind != "cone":
-                        self.zlink[new_hw:old_hw].zero_()
+            self._release([j.job_id for j in done], hw)
         self._record()
         self.last_used = time.perf_counter()
         return done
@@ -419,6 +495,17 @@ class FBPLane(Lane):
         with torch.cuda.stream(self.stream):
             self._load_sinogram(start, job.units, job.sinogram)
         self.jobs[job.job_id] = [job, 1]
+
+    def drop(self, job_id: int) -> Job:
+        """Remove an admitted job before its step (its slots are zeroed and
+        left as a hole for first-fit admission)."""
+        job = self.jobs.pop(job_id)[0]
+        start, n = self.pool.free(job_id)
+        with torch.cuda.stream(self.stream):
+            for t in self._ybufs():
+                t[start:start + n].zero_()
+        self._record()
+        return job
 
     def prepare(self) -> None:
         """Run every launch size once on zeros (filter plans, workspaces)."""
@@ -460,11 +547,22 @@ class Engine:
     """The server loop.  ``hbm_bytes`` bounds the lanes' buffers (default: 80%
     of the device memory free at start); ``capacity`` maps a protocol name to
     its lane's slot count (default 64 slices for fan/parallel lanes, as many
-    cone volumes as a quarter of the budget holds, at most 4)."""
+    cone volumes as a quarter of the budget holds, at most 4).
+
+    Failures stay on the host and with the jobs they concern: a malformed job
+    is rejected at ``submit``; ``cancel`` and a passed ``Job.deadline`` remove a
+    queued or running job; a lane whose buffers cannot be allocated leaves its
+    jobs queued and is retried after idle lanes are torn down (its jobs fail
+    after ``max_alloc_retries`` failed attempts); an error raised by a lane's
+    step fails that lane's jobs and tears the lane down while the other lanes
+    go on.  ``faults`` (optional) is a host-side fault injector called as
+    ``faults(event, protocol)`` before a lane is allocated ("lane_alloc") and
+    before each lane step ("lane_step"); it may raise to simulate the failure
+    of that operation."""
 
     def __init__(self, device=None, hbm_bytes: Optional[int] = None, max_wait: float = 1.0,
                  use_graphs: bool = True, capacity: Optional[Dict[str, int]] = None, slices_per_lane: int = 64,
-                 track_busy: bool = False):
+                 track_busy: bool = False, faults=None, max_alloc_retries: int = 3):
         if not torch.cuda.is_available():
             raise RuntimeError("the reconstruction server needs a CUDA device")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -485,6 +583,13 @@ class Engine:
         self.peak_reserved = 0
         self.track_busy = track_busy  # bracket every lane step with timing events (busy.BusyTracker)
         self.busy_tracker = None
+        self.faults = faults
+        self.max_alloc_retries = int(max_alloc_retries)
+        self.alloc_failures: Dict[str, int] = {}
+        self.alloc_errors: Dict[str, str] = {}
+        self.rejected: List[Job] = []
+        self.cancelled: List[Job] = []  # cancelled, timed out or evicted
+        self.failed: List[Job] = []
 
     # lanes ---------------------------------------------------------------
     def _lane_class(self, p: Protocol):
@@ -518,9 +623,27 @@ class Engine:
         if not self.budget.try_reserve(p.name, need):
             return None
         self.peak_reserved = max(self.peak_reserved, self.budget.reserved)
-        lane = cls(self, p, cap)
+        try:
+            if self.faults is not None:
+                self.faults("lane_alloc", p)
+            lane = cls(self, p, cap)
+        except (torch.cuda.OutOfMemoryError, _lib.CTProjectorError) as e:
+            # leave the jobs queued; free what idle lanes hold before the retry
+            self.budget.release(p.name)
+            self.alloc_failures[p.name] = self.alloc_failures.get(p.name, 0) + 1
+            self.alloc_errors[p.name] = f"{type(e).__name__}: {e}"
+            self._teardown_idle()
+            return None
         self.lanes[p.name] = lane
         return lane
+
+    def _teardown_idle(self) -> None:
+        for name, l in list(self.lanes.items()):
+            if not l.active and all(e.query() for e in l.events):
+                l.release()
+                del self.lanes[name]
+                self.budget.release(name)
+                self.evictions += 1
 
     def warmup(self, protocols: Sequence[Protocol]) -> None:
         """Create the lanes of ``protocols`` ahead of the stream (normalisation
@@ -532,19 +655,97 @@ class Engine:
                 lane.prepare()
         torch.cuda.synchronize(self.device)
 
-    # loop ----------------------------------------------------------------
-    def submit(self, job: Job) -> None:
+    # jobs ------------------------------------------------------------------
+    def validate(self, job: Job) -> Optional[str]:
+        """Why ``job`` cannot be served, or None."""
+        p = job.protocol
+        if job.job_id in self.jobs:
+            return f"job id {job.job_id} is already in the server"
+        if p.kind != "cone" and not (1 <= job.nz <= self._lane_capacity(p)):
+            return f"{job.nz} slices: a {p.name} job brings 1 to {self._lane_capacity(p)} slices"
+        shape = p.sinogram_shape(job.nz)
+        sino = job.sinogram
+        if p.storage == "q16":
+            if not isinstance(sino, quant.Q16):
+                return "a q16 protocol takes a quant.Q16 sinogram"
+            if tuple(sino.code.shape) != shape or tuple(sino.lo.shape) != shape[:2] or \
+                    tuple(sino.step.shape) != shape[:2]:
+                return f"sinogram codes {tuple(sino.code.shape)} / offsets {tuple(sino.lo.shape)}, expected {shape}"
+            if not (bool(torch.isfinite(sino.lo).all()) and bool(torch.isfinite(sino.step).all())):
+                return "non-finite sinogram offsets or steps"
+        else:
+            if not isinstance(sino, torch.Tensor) or not sino.is_floating_point():
+                return "the sinogram must be a floating-point tensor"
+            if sino.numel() != int(np.prod(shape)):
+                return f"sinogram of {tuple(sino.shape)}, expected {shape}"
+        if job.resume is not None:
+            if p.algo != "sqs" or job.resume.source.protocol.name != p.name:
+                return "only an SQS job of the same protocol resumes from a snapshot"
+            if not 0 <= job.resume.done < p.n_iter:
+                return f"the snapshot has done {job.resume.done} of {p.n_iter} iterations"
+        return None
+
+    def submit(self, job: Job) -> bool:
+        """Queue a job; a malformed one is rejected (status "rejected", the
+        reason in ``error``) and False is returned."""
+        why = self.validate(job)
+        if why is not None:
+            job.status, job.error = "rejected", why
+            self.rejected.append(job)
+            return False
+        job.status = "queued"
         self.jobs[job.job_id] = job
         self.queue.push(Pending(job.arrival, job.job_id, job.protocol.name, job.units))
+        return True
 
+    def _remove(self, job: Job, status: str, error: Optional[str] = None) -> None:
+        lane = self.lanes.get(job.protocol.name)
+        if not self.queue.remove_job(job.job_id) and lane is not None and job.job_id in lane.jobs:
+            lane.drop(job.job_id)
+        del self.jobs[job.job_id]
+        job.status, job.error = status, error
+        (self.failed if status == "failed" else self.cancelled).append(job)
+
+    def cancel(self, job_id: int, status: str = "cancelled") -> bool:
+        """Remove a queued or running job without a result.  False if the job
+        is not in the server or its result is already on its way."""
+        job = self.jobs.get(job_id)
+        if job is None or job.done_event is not None:
+            return False
+        self._remove(job, status)
+        return True
+
+    def evict(self, job_id: int) -> "Snapshot":
+        """Take a running SQS job off the device: a snapshot of its iterate
+        and iteration count (copied to pinned host memory on the lane's
+        stream), from which ``Snapshot.job()`` resumes it later."""
+        job = self.jobs.get(job_id)
+        lane = self.lanes.get(job.protocol.name) if job is not None else None
+        if lane is None or job_id not in lane.jobs or not isinstance(lane, SQSLane):
+            raise ValueError(f"job {job_id} is not running in an SQS lane")
+        snap = lane.snapshot(job_id)
+        self._remove(job, "evicted")
+        return snap
+
+    def _expire(self, now: float) -> None:
+        for job in list(self.jobs.values()):
+            if job.deadline is not None and job.done_event is None and now - job.arrival > job.deadline:
+                self._remove(job, "timeout", f"not finished {job.deadline:g} s after arrival")
+
+    # loop ----------------------------------------------------------------
     def _admit(self, now: float) -> bool:
         admitted = False
         for item in self.queue.candidates(now, self.lanes.keys()):
             job = self.jobs[item.job_id]
             lane = self.lane_for(job.protocol, job.units)
-            if lane is None or not lane.can_admit(job):
+            if lane is None:
+                if self.alloc_failures.get(job.protocol.name, 0) > self.max_alloc_retries:
+                    self._remove(job, "failed", "lane allocation failed: " + self.alloc_errors[job.protocol.name])
+                continue
+            if not lane.can_admit(job):
                 continue
             lane.admit(job)
+            job.status = "running"
             job.t_admit = now
             self.queue.remove(item)
             admitted = True
@@ -552,20 +753,37 @@ class Engine:
 
     def _step(self) -> bool:
         stepped = False
-        for lane in list(self.lanes.values()):
+        for name, lane in list(self.lanes.items()):
             if lane.active and lane.ready():
                 start = self.busy_tracker.begin(lane.stream) if self.busy_tracker is not None else None
-                self.retiring.extend(lane.step())
+                try:
+                    if self.faults is not None:
+                        self.faults("lane_step", lane.p)
+                    self.retiring.extend(lane.step())
+                except Exception as e:  # noqa: BLE001 -- isolate the failure to this lane's jobs
+                    self._fail_lane(name, lane, f"{type(e).__name__}: {e}")
+                    continue
                 if start is not None:
                     self.busy_tracker.end(lane.stream, start)
                 stepped = True
         return stepped
+
+    def _fail_lane(self, name: str, lane: Lane, error: str) -> None:
+        for jid in list(lane.jobs):
+            job = lane.jobs.pop(jid)[0]
+            del self.jobs[jid]
+            job.status, job.error = "failed", error
+            self.failed.append(job)
+        lane.release()
+        del self.lanes[name]
+        self.budget.release(name)
 
     def _poll(self, now_fn) -> bool:
         finished = False
         still = []
         for job in self.retiring:
             if job.done_event.query():
+                job.status = "done"
                 job.t_done = now_fn()
                 self.stats.add(job.latency, job.t_done)
                 self.completed.append(job)
@@ -584,6 +802,7 @@ class Engine:
         clock): admit queued jobs, step the lanes, collect finished results.
         Returns whether anything happened, so a caller driving the loop from
         its own event loop knows when to yield."""
+        self._expire(now)
         progressed = self._admit(now)
         progressed |= self._step()
         progressed |= self._poll(now_fn or (lambda: now))

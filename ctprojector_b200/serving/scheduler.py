@@ -164,6 +164,14 @@ class ArrivalQueue:
     def remove(self, item: Pending) -> None:
         self._q.remove(item)
 
+    def remove_job(self, job_id: int) -> bool:
+        """Drop a queued job by id (cancellation); False if it is not queued."""
+        for i, item in enumerate(self._q):
+            if item.job_id == job_id:
+                del self._q[i]
+                return True
+        return False
+
     def oldest(self) -> Optional[Pending]:
         return self._q[0] if self._q else None
 

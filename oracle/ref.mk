@@ -6,11 +6,13 @@
 # golden fixtures under tests/golden/ and the timed reference arm of bench.py.
 # It is never linked into, or called by, the ctprojector_b200 product path.
 #
-#   make -f oracle/ref.mk REF=/root/reference        (run from the repo root)
+#   make -f oracle/ref.mk [REF=<reference checkout>]   (run from the repo root)
 #
-# The sources are read where they lie; nothing is copied into this repository.
+# REF defaults to $(CTP_REFERENCE_SRC) or the checkout of this build machine;
+# without the sources the recipe does nothing.  The sources are read where
+# they lie; nothing is copied into this repository.
 
-REF     ?= /root/reference
+REF     ?= $(or $(CTP_REFERENCE_SRC),/root/reference)
 SRC_DIR := $(REF)/src/ct_projector/kernel/projector/cuda
 PRIOR   := $(REF)/src/ct_projector/kernel/prior/cuda/TotalVariation.cu
 OUT     := oracle/_ref
@@ -23,7 +25,12 @@ OBJECTS := $(patsubst $(SRC_DIR)/%.cu,$(OBJ_DIR)/%.o,$(SOURCES))
 
 .PHONY: all clean
 
+ifeq ($(SOURCES),)
+all:
+	@echo "ref.mk: no reference sources under $(REF); oracle/_ref not built"
+else
 all: $(OUT)/libprojector.so $(OUT)/libprior.so
+endif
 
 $(OUT)/libprojector.so: $(OBJECTS)
 	$(NVCC) --shared $(ARCH) $(OBJECTS) -lcufft -o $@

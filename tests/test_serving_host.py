@@ -151,3 +151,12 @@ def test_q16_host_values_and_slices():
     one = q[1:]
     assert tuple(one.shape) == (1, 1, 1, 4) and tuple(one.lo.shape) == (1, 1)
     assert one.nbytes == 4 * 2 + 2 * 4
+
+
+def test_arrival_queue_removes_a_job_by_id():
+    q = ArrivalQueue(1.0)
+    for i, t in enumerate([0.3, 0.1, 0.2]):
+        q.push(Pending(t, i, "lane", 1))
+    assert q.remove_job(2) and not q.remove_job(2)
+    assert [p.job_id for p in q.candidates(0.5)] == [1, 0]
+    assert not q.remove_job(7) and len(q) == 2
