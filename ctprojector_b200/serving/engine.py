@@ -202,8 +202,9 @@ class Lane:
         self.jobs: Dict[int, List] = {}  # job id -> [job, steps left]
         self.events: deque = deque()
         self.last_used = time.perf_counter()
-        # launch sizes step by 4 slices (fan/parallel) or 1 volume (cone)
+        # launch sizes: exact up to 8 slices, then steps of 4 (fan/parallel); 1 volume (cone)
         self.granule = 1 if protocol.kind == "cone" else 4
+        self.exact = 0 if protocol.kind == "cone" else 8
         s = protocol.scan
         self.ny, self.nx = int(s.ny), int(s.nx)
         if protocol.kind == "cone":
@@ -387,7 +388,7 @@ class SQSLane(Lane):
         if self.jobs:
             raise RuntimeError("prepare() runs on an empty lane")
         with torch.cuda.stream(self.stream):
-            for b in bucket_sizes(self.capacity, self.granule):
+            for b in bucket_sizes(self.capacity, self.granule, self.exact):
                 for _ in range(2):
                     self._run_step(b)
 
@@ -444,7 +445,7 @@ class SQSLane(Lane):
 
     def step(self) -> List[Job]:
         hw = self.pool.high_water
-        b = bucket(hw, self.capacity, self.granule)
+        b = bucket(hw, self.capacity, self.granule, self.exact)
         with torch.cuda.stream(self.stream):
             self._run_step(b)
         done = []
@@ -510,7 +511,7 @@ class FBPLane(Lane):
     def prepare(self) -> None:
         """Run every launch size once on zeros (filter plans, workspaces)."""
         with torch.cuda.stream(self.stream):
-            for b in bucket_sizes(self.capacity, self.granule):
+            for b in bucket_sizes(self.capacity, self.granule, self.exact):
                 self._filter_bp(b)
 
     def _filter_bp(self, b: int) -> None:
@@ -523,7 +524,7 @@ class FBPLane(Lane):
         D.dd_bp(p.scan, f, self.ang, self.geom, is_fbp=True, out=self.img[:b])
 
     def step(self) -> List[Job]:
-        b = bucket(self.pool.high_water, self.capacity, self.granule)
+        b = bucket(self.pool.high_water, self.capacity, self.granule, self.exact)
         done = []
         with torch.cuda.stream(self.stream):
             self._filter_bp(b)

@@ -88,20 +88,23 @@ class SlotPool:
         return moves
 
 
-def bucket(n: int, capacity: int, granule: int = 1) -> int:
-    """Launch size for ``n`` live slots: ``n`` rounded up to a multiple of
-    ``granule``, at most ``capacity`` (one captured graph per size, so the
-    granule bounds the number of graphs; empty slots in the launch are work
-    done on zeros)."""
+def bucket(n: int, capacity: int, granule: int = 1, exact: int = 0) -> int:
+    """Launch size for ``n`` live slots: ``n`` itself up to ``exact``, above
+    that rounded up to a multiple of ``granule``; at most ``capacity``.  One
+    graph is captured per size, so the granule bounds the number of graphs;
+    empty slots in a launch are work done on zeros, which ``exact`` spares the
+    small launches (a lone one-slice job runs one slice, not ``granule``)."""
     if n <= 0:
         return 0
+    if n <= exact:
+        return min(n, capacity)
     g = max(1, int(granule))
     return min(-(-n // g) * g, capacity)
 
 
-def bucket_sizes(capacity: int, granule: int = 1):
+def bucket_sizes(capacity: int, granule: int = 1, exact: int = 0):
     """Every launch size ``bucket`` can return for this capacity."""
-    return sorted({bucket(n, capacity, granule) for n in range(1, capacity + 1)})
+    return sorted({bucket(n, capacity, granule, exact) for n in range(1, capacity + 1)})
 
 
 # --------------------------------------------------------------------------- memory

@@ -82,6 +82,9 @@ def test_bucket_sizes():
     assert bucket(47, 46, 4) == 46
     assert bucket_sizes(10, 4) == [4, 8, 10]
     assert bucket_sizes(3) == [1, 2, 3]
+    # exact small launches, then steps of the granule
+    assert [bucket(n, 64, 4, 8) for n in (1, 3, 8, 9, 12, 13, 64)] == [1, 3, 8, 12, 12, 16, 64]
+    assert bucket_sizes(20, 4, 8) == [1, 2, 3, 4, 5, 6, 7, 8, 12, 16, 20]
 
 
 def test_memory_budget():
