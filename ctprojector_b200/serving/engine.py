@@ -198,7 +198,8 @@ class Lane:
         self.capacity = int(capacity)
         self.pool = SlotPool(self.capacity)
         self.dev = engine.device
-        self.stream = torch.cuda.Stream(self.dev)
+        # one stream per lane (lanes overlap on the GPU), or the engine's one
+        self.stream = engine.shared_stream if engine.shared_stream is not None else torch.cuda.Stream(self.dev)
         self.jobs: Dict[int, List] = {}  # job id -> [job, steps left]
         self.events: deque = deque()
         self.last_used = time.perf_counter()
@@ -563,7 +564,7 @@ class Engine:
 
     def __init__(self, device=None, hbm_bytes: Optional[int] = None, max_wait: float = 1.0,
                  use_graphs: bool = True, capacity: Optional[Dict[str, int]] = None, slices_per_lane: int = 64,
-                 track_busy: bool = False, faults=None, max_alloc_retries: int = 3):
+                 track_busy: bool = False, faults=None, max_alloc_retries: int = 3, lane_streams: bool = True):
         if not torch.cuda.is_available():
             raise RuntimeError("the reconstruction server needs a CUDA device")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -586,6 +587,9 @@ class Engine:
         self.busy_tracker = None
         self.faults = faults
         self.max_alloc_retries = int(max_alloc_retries)
+        # lane_streams=False: every lane enqueues on one stream, so lanes do not
+        # run concurrently (batching within a lane stays)
+        self.shared_stream = None if lane_streams else torch.cuda.Stream(self.device)
         self.alloc_failures: Dict[str, int] = {}
         self.alloc_errors: Dict[str, str] = {}
         self.rejected: List[Job] = []

@@ -179,3 +179,37 @@ def test_adjoint_identity(run):
     rhs = float(torch.sum(x.double() * aty))
     den = float(torch.linalg.vector_norm(ax)) * float(torch.linalg.vector_norm(y.double()))
     assert abs(lhs - rhs) / den <= ADJ_TOL, f"{run['name']}: {abs(lhs - rhs) / den:.3g}"
+
+
+def test_diagonal_views_are_an_operator_choice_not_an_error(run, oracle):
+    """Views exactly on a 45 degree diagonal (4 of the 984-view and 360-view
+    fan configurations): the reference switches the fan back projector's axis
+    on |__cosf| > |__sinf| there, so its result depends on the fast
+    intrinsics' rounding; the kernels make the same comparison with the same
+    intrinsics, the FP64 oracle uses exact trigonometry.  Measured on slice 0
+    with every view: ours and the reference agree within 1e-5, both are the
+    same distance from the oracle, and without the diagonal views both are
+    within 1e-5 of it -- the whole difference is the operator at those views."""
+    if run["kind"] != "fan":
+        pytest.skip("the hard axis switch of the back projector is fan-beam only")
+    from make_golden import Ref
+
+    scan, p, M = run["scan"], run["p"], run["M"]
+    ang = run["ang"]
+    keep = _off_diagonal(ang)
+    if len(keep) == len(ang):
+        pytest.skip("no view of this configuration lies on a diagonal")
+    y = np.ascontiguousarray(run["y"][:1])
+    o = oracle.dd_bp(scan, y, ang, "fan")
+    u = host(M.distance_driven_bp(p, dev(y), dev(ang)))
+    r = Ref(REF_LIB).dd_bp(scan, y, ang, True, 0)
+    e_ours, e_ref = rel_l2(u, o), rel_l2(r, o)
+    print(f"{run['name']}: {len(ang) - len(keep)} diagonal views; BP vs the exact-trigonometry oracle: ours "
+          f"{e_ours:.3g}, reference {e_ref:.3g}; ours vs reference {rel_l2(u, r):.3g}")
+    assert rel_l2(u, r) <= TOL
+    if e_ref > TOL:  # the intrinsics pick the other axis than exact trigonometry at these views
+        assert abs(e_ours - e_ref) <= 0.05 * e_ref
+    else:  # they pick the same axis here
+        assert e_ours <= TOL
+    yk, ak = np.ascontiguousarray(y[:, keep]), np.ascontiguousarray(ang[keep])
+    assert rel_l2(host(M.distance_driven_bp(p, dev(yk), dev(ak))), oracle.dd_bp(scan, yk, ak, "fan")) <= TOL
