@@ -556,8 +556,19 @@ __device__ __forceinline__ void small_dft<3>(double2* v) {
     v[2] = csub(m, r);
 }
 
-// One radix-R stage: sub-transforms of length ns are merged R at a time
-// (twiddle t of stage ns is tw[t * n / (ns R)], tw[t] = exp(-2 pi i t / n)).
+// Shared-memory slot of element i: i with its low three bits XORed by the
+// next three, a permutation within each aligned group of 8 (buffers are
+// rounded up to a multiple of 8).  The first stage writes each thread's
+// outputs 8 elements apart, which would put the 8 threads of a 16-byte
+// access phase on the same banks; swizzled they are spread over all banks,
+// while the contiguous accesses of the other stages stay contiguous.
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 7); }
+
+// One radix-R stage: sub-transforms of length ns are merged R at a time.
+// The twiddles of a butterfly are the powers w, w^2, ... of
+// w = tw[k * n / (ns R)] (tw[t] = exp(-2 pi i t / n)): one table load, the
+// other powers by FP64 complex products (their rounding, ~R ulp, is far below
+// the FP32 output's).
 template <int R>
 __device__ __forceinline__ void fft_stage(const double2* __restrict__ src, double2* __restrict__ dst,
                                           const double2* __restrict__ tw, int n, int ns) {
@@ -566,15 +577,20 @@ __device__ __forceinline__ void fft_stage(const double2* __restrict__ src, doubl
         const int k = j % ns;
         double2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = src[j + r * nr];
+        for (int r = 0; r < R; ++r) v[r] = src[swz(j + r * nr)];
         if (ns > 1) {
+            const double2 w = __ldg(tw + k * tstep);
+            double2 wr = w;
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + k * r * tstep));
+            for (int r = 1; r < R; ++r) {
+                v[r] = cmul(v[r], wr);
+                if (r + 1 < R) wr = cmul(wr, w);
+            }
         }
         small_dft<R>(v);
         const int d = (j - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) dst[d + r * ns] = v[r];
+        for (int r = 0; r < R; ++r) dst[swz(d + r * ns)] = v[r];
     }
 }
 
@@ -638,23 +654,24 @@ __global__ void __launch_bounds__(256) conv_rows_kernel(float* __restrict__ out,
             v.x = (double)in.load(r0, j, nu) * w;
             v.y = two ? (double)in.load(r0 + 1, j, nu) * w : 0.0;
         }
-        conv_smem[j] = v;
+        conv_smem[swz(j)] = v;
     }
     __syncthreads();
-    int a = fft_forward(conv_smem, 0, plan.n, tw, plan);
+    const int stride = (plan.n + 7) & ~7;  // one buffer, rounded up for the swizzle
+    int a = fft_forward(conv_smem, 0, stride, tw, plan);
     double2* buf = conv_smem + a;
     for (int j = threadIdx.x; j < plan.n; j += blockDim.x) {
         const double k = __ldg(spec + j);
-        const double2 y = buf[j];
-        buf[j] = make_double2(y.x * k, -y.y * k);  // conjugate of the product with the real spectrum
+        const double2 y = buf[swz(j)];
+        buf[swz(j)] = make_double2(y.x * k, -y.y * k);  // conjugate of the product with the real spectrum
     }
     __syncthreads();
-    a = fft_forward(conv_smem, a, plan.n - a, tw, plan);
+    a = fft_forward(conv_smem, a, stride - a, tw, plan);
     buf = conv_smem + a;
     float* y0 = out + r0 * nu;
     float* y1 = y0 + nu;
     for (int n = threadIdx.x; n < nu; n += blockDim.x) {
-        const double2 v = buf[n];
+        const double2 v = buf[swz(n)];
         y0[n] = (float)(v.x * scale);
         if (two) y1[n] = (float)(-v.y * scale);
     }
@@ -732,7 +749,7 @@ int ramp_filter_conv(float* fprj, const Rows prj, const ctp_geometry& g, bool fa
     const double scale = M_PI / (double)g.nview * (double)g.du / (fan ? (double)g.dso : 1.0) / N;
     int threads = (N / 8 + 31) / 32 * 32;
     threads = threads < 64 ? 64 : threads > 256 ? 256 : threads;
-    const size_t smem = 2 * sizeof(double2) * N;
+    const size_t smem = 2 * sizeof(double2) * (size_t)((N + 7) & ~7);
     if (smem > 48 * 1024) {
         cudaError_t e =
             cudaFuncSetAttribute(conv_rows_kernel<Rows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

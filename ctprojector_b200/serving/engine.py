@@ -3,8 +3,9 @@
 Jobs (an FBP or an SQS-TV reconstruction of one scan) arrive over time.  Jobs
 whose scan protocol (geometry + algorithm) is the same share a *lane*: one set
 of device-resident buffers with a fixed number of slots (image slices for the
-fan/parallel protocols, volumes for cone), its own CUDA stream and captured
-CUDA graphs.  Each pass of the server loop
+fan/parallel protocols, volumes for cone) and captured CUDA graphs; the
+lanes enqueue on the engine's stream (or one stream each, ``lane_streams``).
+Each pass of the server loop
 
 1. moves arrived jobs to the arrival queue,
 2. admits queued jobs into free slots (creating a lane if the HBM budget
@@ -12,8 +13,8 @@ CUDA graphs.  Each pass of the server loop
    lane's stream,
 3. advances every lane with work by one step (one SQS iteration over all its
    live slots, or one batched FBP), unless its previous-but-one step is still
-   running, so lanes run concurrently on the GPU and stay at most two steps
-   ahead of the host,
+   running, so the lanes' steps interleave on the GPU and stay at most two
+   steps ahead of the host,
 4. retires finished jobs: a device-to-host copy of their slots into pinned
    memory, then the slots are freed and the live ones packed to the front.
 
@@ -564,7 +565,7 @@ class Engine:
 
     def __init__(self, device=None, hbm_bytes: Optional[int] = None, max_wait: float = 1.0,
                  use_graphs: bool = True, capacity: Optional[Dict[str, int]] = None, slices_per_lane: int = 64,
-                 track_busy: bool = False, faults=None, max_alloc_retries: int = 3, lane_streams: bool = True):
+                 track_busy: bool = False, faults=None, max_alloc_retries: int = 3, lane_streams: bool = False):
         if not torch.cuda.is_available():
             raise RuntimeError("the reconstruction server needs a CUDA device")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -587,8 +588,13 @@ class Engine:
         self.busy_tracker = None
         self.faults = faults
         self.max_alloc_retries = int(max_alloc_retries)
-        # lane_streams=False: every lane enqueues on one stream, so lanes do not
-        # run concurrently (batching within a lane stays)
+        # By default every lane enqueues on one stream: lanes take turns on
+        # the GPU while the jobs of a lane share its launches.  Measured on the
+        # B200 with 40 jobs of the mix with cone volumes: 4.84 recons/s against
+        # 4.11 with one stream per lane (concurrent lanes slow each other's
+        # kernels down more than they fill the GPU's gaps), and 27.0 against
+        # 25.6 on the 150-job 2D stream.  lane_streams=True gives every lane
+        # its own stream.
         self.shared_stream = None if lane_streams else torch.cuda.Stream(self.device)
         self.alloc_failures: Dict[str, int] = {}
         self.alloc_errors: Dict[str, str] = {}
