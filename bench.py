@@ -778,10 +778,18 @@ def run_op(op: str, workload: str, repeat: int) -> int:
                "filter_exact": lambda: D.ramp_filter(scan, prj, "hann", code, exact=True)}
     if op not in ops:
         raise SystemExit(f"op {op!r} is not defined for workload {workload!r}")
-    for _ in range(1 + max(0, repeat)):
+    ops[op]()
+    times = []
+    for _ in range(max(0, repeat)):
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
         ops[op]()
+        t1.record()
+        t1.synchronize()
+        times.append(t0.elapsed_time(t1))
     torch.cuda.synchronize()
-    print(f"{op} {workload}: ok")
+    tail = f", median {float(np.median(times)):.4f} ms over {len(times)} warm calls (CUDA events)" if times else ""
+    print(f"{op} {workload}: ok{tail}")
     return 0
 
 

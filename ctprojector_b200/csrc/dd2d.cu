@@ -696,10 +696,29 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
-// One image line's contribution to a thread's NI edge groups.  T is the
-// line's midpoint table (FP64 entries {C + r/2 as the low and high words of a
-// double, r, 0}, pointing at the origin entry h), t the line's coordinate
-// from the anchor line, positions clamped to [lo_lim, hi_lim].
+// Layout of one line's midpoint table (n cells, entries 0..n): n + 1 FP64
+// values C_i + r_i/2 padded to an even count, then n + 1 FP32 cell values r_i
+// padded to a multiple of four.  Both parts, and so every line of a stack of
+// tables, start on a 16-byte boundary, as bulk copies require.  A warp reads
+// 8 + 4 bytes per edge in two accesses instead of one 16-byte access: the
+// edges of a warp spread over more entries than lanes, so the wavefronts of a
+// read grow with the bytes spanned, not with the number of accesses.
+__host__ __device__ __forceinline__ int line_nf(int n) { return (n + 2) & ~1; }
+__host__ __device__ __forceinline__ int line_nr(int n) { return (n + 4) & ~3; }
+__host__ __device__ __forceinline__ size_t line_bytes(int n) { return (size_t)8 * line_nf(n) + (size_t)4 * line_nr(n); }
+
+// The FP64 and FP32 parts of a line table, offset to the origin entry h.
+__device__ __forceinline__ const double* line_f(const unsigned char* line, int h) {
+    return reinterpret_cast<const double*>(line) + h;
+}
+__device__ __forceinline__ const float* line_r(const unsigned char* line, int n, int h) {
+    return reinterpret_cast<const float*>(line + 8 * line_nf(n)) + h;
+}
+
+// One image line's contribution to a thread's NI edge groups.  Fm and Rc are
+// the FP64 midpoint values and the FP32 cell values of the line's table,
+// offset to the origin entry h; t is the line's coordinate from the anchor
+// line, positions clamped to [lo_lim, hi_lim].
 //   parallel: edge position A + B t, the same slope B for every edge of a
 //        view, so a cell's footprint has the same width on every line; the
 //        lane adds F at its edge (accd += entry in FP64, the small r * frac
@@ -716,7 +735,8 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // included, whose results are dropped), so tau and its weight are computed
 // once per line from group 0's source coordinate.
 template <bool FAN, int NI, bool ONEV = false>
-__device__ __forceinline__ void fp_line(const float4* __restrict__ T, float t, float lo_lim, float hi_lim,
+__device__ __forceinline__ void fp_line(const double* __restrict__ Fm, const float* __restrict__ Rc, float t,
+                                        float lo_lim, float hi_lim,
                                         const float (&A)[NI], const float (&B)[NI], const float (&S)[NI],
                                         double (&accd)[NI], float (&alo)[NI]) {
     float tau1 = t, wgt1 = 1.f;
@@ -737,15 +757,16 @@ __device__ __forceinline__ void fp_line(const float4* __restrict__ T, float t, f
         const float xr = fmaf(B[q], tau, A[q]);
         const float xs = clampf(xr, lo_lim, hi_lim);
         const float tt = xs + kRoundMagic;
-        const float4 e = T[__float_as_int(tt) - kRoundMagicBits];
+        const int i = __float_as_int(tt) - kRoundMagicBits;
+        const double F = Fm[i];
+        const float r = Rc[i];
         const float frac = xs - (tt - kRoundMagic);
-        const double F = __hiloint2double(__float_as_int(e.y), __float_as_int(e.x));
         if constexpr (FAN) {
             accd[q] = fma(wd, F, accd[q]);
-            alo[q] = fmaf(wgt * e.z, frac, alo[q]);
+            alo[q] = fmaf(wgt * r, frac, alo[q]);
         } else {
             accd[q] += F;
-            alo[q] = fmaf(e.z, frac, alo[q]);
+            alo[q] = fmaf(r, frac, alo[q]);
         }
     }
 }
@@ -776,12 +797,14 @@ __device__ __forceinline__ float fp_cell_sum(double accd, float W) {
 // round (half to even) onto table entries 0 and n or n - 1.
 __device__ __forceinline__ int fp_origin(int n) { return (n >> 1) & ~1; }
 
-// FP64 midpoint table of one line, built by one warp: n+1 entries
-// {C_i + r_i/2 as the low and high words of a double, r_i, 0} with C_i the
-// integral over cells [0, i) and r_i the cell value (0 past the end).
+// FP64 midpoint table of one line, built by one warp: n+1 entries C_i + r_i/2
+// and r_i (line_nf), C_i the integral over cells [0, i) and r_i the cell
+// value (0 past the end); the padding entries are zero.
 template <typename Tin>
-__device__ __forceinline__ void stage_line_fp64(float4* __restrict__ T, const Tin* __restrict__ row, int n,
-                                                int lane) {
+__device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line, const Tin* __restrict__ row,
+                                                int n, int lane) {
+    double* Fm = reinterpret_cast<double*>(line);
+    float* Rc = reinterpret_cast<float*>(line + 8 * line_nf(n));
     const int E = (n + 1 + 31) / 32;
     const int k0 = lane * E;
     double tot = 0.0;
@@ -800,30 +823,32 @@ __device__ __forceinline__ void stage_line_fp64(float4* __restrict__ T, const Ti
         const int k = k0 + q;
         if (k <= n) {
             const float r = k < n ? ldf(row + k) : 0.f;
-            const double m = c + 0.5 * (double)r;
-            T[k] = make_float4(__int_as_float(__double2loint(m)), __int_as_float(__double2hiint(m)), r, 0.f);
+            Fm[k] = c + 0.5 * (double)r;
+            Rc[k] = r;
             c += (double)r;
         }
     }
+    if (n + 1 + lane < line_nf(n)) Fm[n + 1 + lane] = 0.0;
+    if (n + 1 + lane < line_nr(n)) Rc[n + 1 + lane] = 0.f;
 }
 
 // Stage lines (length n, stride n between lines) into consecutive tables.
 template <typename Tin>
-__device__ void stage_lines(float4* __restrict__ tab, const Tin* __restrict__ src, int nlines, int n, int warp,
-                            int lane, int nwarps) {
+__device__ void stage_lines(unsigned char* __restrict__ tab, const Tin* __restrict__ src, int nlines, int n,
+                            int warp, int lane, int nwarps) {
     for (int l = warp; l < nlines; l += nwarps)
-        stage_line_fp64(tab + (size_t)l * (n + 1), src + (size_t)l * n, n, lane);
+        stage_line_fp64(tab + (size_t)l * line_bytes(n), src + (size_t)l * n, n, lane);
 }
 
 // The tables of every line of a stack of slices (one warp per line), for the
 // forward projector that streams them into shared memory.
 template <typename Tin>
-__global__ void __launch_bounds__(256) line_tables_kernel(float4* __restrict__ out, const Tin* __restrict__ src,
-                                                          long long nlines, int n) {
+__global__ void __launch_bounds__(256) line_tables_kernel(unsigned char* __restrict__ out,
+                                                          const Tin* __restrict__ src, long long nlines, int n) {
     const int lane = threadIdx.x & 31;
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long l = w0; l < nlines; l += nw) stage_line_fp64(out + l * (n + 1), src + l * n, n, lane);
+    for (long long l = w0; l < nlines; l += nw) stage_line_fp64(out + l * line_bytes(n), src + l * n, n, lane);
 }
 
 // NI = edge groups per warp (compile time, so the group loop is straight-line
@@ -840,7 +865,8 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
                                                            const Tin* __restrict__ imgT, DDTab tab, Grid g, Det d,
                                                            int nview, int vgroup, int nrows_chunk,
                                                            const float* __restrict__ deg, int unweight_par) {
-    extern __shared__ float4 s_lines[];
+    extern __shared__ float4 s_lines4[];
+    unsigned char* s_lines = reinterpret_cast<unsigned char*>(s_lines4);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int v0 = blockIdx.x * vgroup;
     const int nvg = min(vgroup, nview - v0);
@@ -892,9 +918,11 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
             __syncthreads();
             stage_lines<Tin>(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
             __syncthreads();
-            for (int r = 0; r < nlc; ++r)
-                fp_line<FAN, NI, ONEV>(s_lines + (size_t)r * (n + 1) + h, (float)(l0 + r - anchor), lo_lim, hi_lim,
-                                       A, B, S, accd, alo);
+            for (int r = 0; r < nlc; ++r) {
+                const unsigned char* line = s_lines + (size_t)r * line_bytes(n);
+                fp_line<FAN, NI, ONEV>(line_f(line, h), line_r(line, n, h), (float)(l0 + r - anchor), lo_lim,
+                                       hi_lim, A, B, S, accd, alo);
+            }
             if ((c + 1) % renorm == 0) fp_renorm<NI>(accd, alo);
         }
         fp_renorm<NI>(accd, alo);
@@ -995,11 +1023,12 @@ template <bool FAN, int NI>
 constexpr int fp_stream_min_blocks() { return NI <= 8 ? 3 : 2; }
 
 template <bool FAN, int NI, typename Tout, bool ONEV = false>
-__global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const float4* __restrict__ ltab0,
-                                                             const float4* __restrict__ ltab1, DDTab tab, Grid g,
+__global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const unsigned char* __restrict__ ltab0,
+                                                             const unsigned char* __restrict__ ltab1, DDTab tab, Grid g,
                                                              Det d, int nview, int vgroup, int rchunk,
                                                              const float* __restrict__ deg, int unweight_par) {
-    extern __shared__ float4 s_ring[];  // [2][rchunk * (max(nx, ny) + 1)]
+    extern __shared__ float4 s_ring4[];  // [2][rchunk line tables of max(nx, ny) cells]
+    unsigned char* s_ring = reinterpret_cast<unsigned char*>(s_ring4);
     __shared__ __align__(8) unsigned long long s_bar[2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int v0 = blockIdx.x * vgroup;
@@ -1008,7 +1037,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
     const int iz = slice % g.nz, b = slice / g.nz;
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
     const int nitems = nvg * ipv;
-    const size_t ring = (size_t)rchunk * (max(g.nx, g.ny) + 1);
+    const size_t ring = (size_t)rchunk * line_bytes(max(g.nx, g.ny));  // bytes per buffer
 
     // orientations with work in this CTA: rows (o = 0) for views traced along
     // y, columns (o = 1) for views traced along x, both in the blend band
@@ -1023,18 +1052,18 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
     const int nc0 = act0 ? (g.ny + rchunk - 1) / rchunk : 0;
     const int nc1 = act1 ? (g.nx + rchunk - 1) / rchunk : 0;
     const int K = nc0 + nc1;
-    const float4* src0 = ltab0 + (size_t)slice * g.ny * (g.nx + 1);
-    const float4* src1 = ltab1 + (size_t)slice * g.nx * (g.ny + 1);
+    const unsigned char* src0 = ltab0 + (size_t)slice * g.ny * line_bytes(g.nx);
+    const unsigned char* src1 = ltab1 + (size_t)slice * g.nx * line_bytes(g.ny);
 
     auto issue = [&](int k) {
         const int o = k < nc0 ? 0 : 1;
         const int c = o == 0 ? k : k - nc0;
         const int n = o == 0 ? g.nx : g.ny, nl = o == 0 ? g.ny : g.nx;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
-        const unsigned bytes = (unsigned)((size_t)nlc * (n + 1) * sizeof(float4));
+        const unsigned bytes = (unsigned)((size_t)nlc * line_bytes(n));
         unsigned long long* bar = &s_bar[k & 1];
         mbar_expect_tx(bar, bytes);
-        bulk_copy_g2s(s_ring + (k & 1) * ring, (o == 0 ? src0 : src1) + (size_t)l0 * (n + 1), bytes, bar);
+        bulk_copy_g2s(s_ring + (k & 1) * ring, (o == 0 ? src0 : src1) + (size_t)l0 * line_bytes(n), bytes, bar);
     };
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);
@@ -1088,13 +1117,16 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         }
         if (!mbar_wait_bounded(&s_bar[k & 1], (k >> 1) & 1, k == 0 ? first_polls : kWaitPolls)) failed = true;
         failed = __any_sync(0xffffffffu, failed);  // the cell sums shuffle: whole warps stop together
-        const float4* buf = s_ring + (k & 1) * ring;
+        const unsigned char* buf = s_ring + (k & 1) * ring;
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
         const float lo_lim = -shift, hi_lim = (float)n - shift;
         float tl = (float)(l0 - anchor);  // line coordinate, stepped exactly
-        for (int r = 0; r < nlc && !failed; ++r, tl += 1.f)
-            fp_line<FAN, NI, ONEV>(buf + (size_t)r * (n + 1) + h, tl, lo_lim, hi_lim, A, B, S, accd, alo);
+        const size_t lb = line_bytes(n);
+        for (int r = 0; r < nlc && !failed; ++r, tl += 1.f) {
+            const unsigned char* line = buf + r * lb;
+            fp_line<FAN, NI, ONEV>(line_f(line, h), line_r(line, n, h), tl, lo_lim, hi_lim, A, B, S, accd, alo);
+        }
         if ((c + 1) % renorm == 0 || c == last) fp_renorm<NI>(accd, alo);
         if (c == last && !failed) {
 #pragma unroll
@@ -1712,13 +1744,13 @@ size_t fp_workspace_min(const ctp_geometry& g) {
 
 size_t fp_line_tables_bytes(const ctp_geometry& g) {
     size_t slices = g.nbatch * g.nz;
-    return align_up(slices * (g.ny * (g.nx + 1) + g.nx * (g.ny + 1)) * sizeof(float4));
+    return align_up(slices * (g.ny * line_bytes((int)g.nx) + g.nx * line_bytes((int)g.ny)));
 }
 
 // Lines per chunk of the streamed path's two-buffer ring, or 0 if one line
 // per buffer does not fit.
 int fp_stream_chunk(const ctp_geometry& g) {
-    size_t line = (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+    size_t line = line_bytes((int)std::max(g.nx, g.ny));
     if (2 * line > 200 * 1024) return 0;
     int r = (int)((66 * 1024) / (2 * line));
     return std::max(1, std::min(r, 8));
@@ -1766,7 +1798,7 @@ bool fp_fast_ok(const ctp_geometry& g, int& vgroup, int& nrows) {
         }
     }
     if (vgroup < 1) return false;
-    size_t line = (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+    size_t line = line_bytes((int)std::max(g.nx, g.ny));
     nrows = 8;
     while (nrows > 1 && nrows * line > 110 * 1024) nrows /= 2;
     return nrows * line <= 200 * 1024;
@@ -1857,8 +1889,8 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     // without room for the line tables runs the staged kernel
     if (shaped && rchunk > 0 && ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
         // streamed path: line tables of rows (from the image) and columns (from its transpose)
-        float4* lt0 = reinterpret_cast<float4*>(ws + fp_workspace_min(g));
-        float4* lt1 = lt0 + g.nbatch * g.nz * g.ny * (g.nx + 1);
+        unsigned char* lt0 = reinterpret_cast<unsigned char*>(ws + fp_workspace_min(g));
+        unsigned char* lt1 = lt0 + g.nbatch * g.nz * g.ny * line_bytes((int)g.nx);
         long long rows = (long long)(g.nbatch * g.nz * g.ny), cols = (long long)(g.nbatch * g.nz * g.nx);
         const unsigned rgrid = (unsigned)std::min<long long>((rows + 7) / 8, 148 * 16);
         const unsigned cgrid = (unsigned)std::min<long long>((cols + 7) / 8, 148 * 16);
@@ -1879,7 +1911,7 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
             }
         }
         const int rc_s = rchunk;
-        size_t shm = 2 * (size_t)rc_s * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+        size_t shm = 2 * (size_t)rc_s * line_bytes((int)std::max(g.nx, g.ny));
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)nslices);
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -1906,7 +1938,7 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         return check_launch("dd2d_fp_stream_kernel");
     }
     if (shaped) {
-        size_t shm = (size_t)nrows * (std::max(g.nx, g.ny) + 1) * sizeof(float4);
+        size_t shm = (size_t)nrows * line_bytes((int)std::max(g.nx, g.ny));
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)(g.nbatch * g.nz));
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);

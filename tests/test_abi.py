@@ -98,9 +98,10 @@ def test_bp_workspace_holds_view_parts():
 
 def test_fp_workspace_line_tables_up_to_128_edge_groups():
     """The fast forward projectors serve detectors of up to 128 groups of 31
-    cells (3937 cells): their workspace holds the streamed line tables
-    (16 B per entry, rows and columns of a 256 x 256 slice); wider detectors
-    take the general kernel, whose workspace has none."""
+    cells (3937 cells): their workspace holds the streamed line tables (per
+    line of 256 cells, 258 FP64 and 260 FP32 entries; rows and columns of a
+    256 x 256 slice); wider detectors take the general kernel, whose
+    workspace has none."""
     from ctprojector_b200._lib import Geometry, lib
 
     def ws(nu):
@@ -110,7 +111,7 @@ def test_fp_workspace_line_tables_up_to_128_edge_groups():
     def edge_table(nu, nview=40):
         return (2 * (2 * nview * (nu + 1) + nview * nu) + 5 * nview) * 4
 
-    line_tables = 2 * 256 * 257 * 16
+    line_tables = 2 * 256 * (258 * 8 + 260 * 4)
     image = 256 * 256 * 4
     assert ws(3000) >= edge_table(3000) + image + line_tables
     assert ws(4000) < edge_table(4000) + image + line_tables

@@ -109,7 +109,7 @@ def _scratch_allocations():
 
 def test_noalloc_staged_path_allocates_nothing():
     """The 16-slice 512 x 512 stack with 60 views of 768 cells: its edge table
-    and transposed image fit the fixed scratch but its line tables (134 MB) do
+    and transposed image fit the fixed scratch but its line tables (101 MB) do
     not, so the call runs the staged kernel (tables built per CTA in shared
     memory).  Three calls in a row: each equals ctp_dd2d_fp, none makes a
     scratch allocation, and the device's free memory does not move between
