@@ -678,15 +678,21 @@ __global__ void __launch_bounds__(kTile* kTile) dd2d_bp_adjoint_kernel(
 // DDFPTracing (distanceDriven2DBoxInt.cu:21-106).
 constexpr int kFMaxItems = 16;  // edge groups (of 32 edges) per warp
 
-// Running integral at x' + 1/2 from a midpoint table: entry i holds
-// (C_i + r_i / 2, r_i) with C_i the integral up to cell i, so
-// F(x) = entry.x + r_i (x - 1/2 - i) for the cell i nearest x - 1/2.  The
-// nearest integer comes from the float adder (x' + 1.5*2^23 rounds x' to an
-// integer in the low mantissa bits), which keeps the lookup off the
-// conversion pipe.  x' = x - 1/2 must lie in [-1/2, n - 1/2], moved by the
-// origin h of the positions (fp_origin).
+// Running integral along a line from its midpoint table.  The line of n
+// cells gets a zero cell on each side (cells -1 and n); table entry k = i + 1
+// of cell i in [-1, n] holds M_i = C_i + r_i/2 and r_i, C_i the integral up
+// to cell i, so F(x) = M_i + r_i (x' - i) at x' = x - 1/2 for the cell i
+// nearest x'.  Edge positions are normalised, xn = (x' + 1) / (n + 1), and
+// clamped to [0, 1] by the saturating FP32 fused multiply-add that computes
+// them, so the clamped x' = xn (n + 1) - 1 spans [-1, n] and every lookup
+// stays inside the table (NaN saturates to 0).  The nearest integer comes
+// from the float adder in the same kind of instruction: xn (n + 1) +
+// (1.5*2^23 - 1) rounds x' to an integer in the low mantissa bits, and
+// xn (n + 1) + (1.5*2^23 - 1 - that sum) is its fraction, both from the exact
+// product; the mantissa bits, times the entry size, plus a base offset are
+// the entry's shared-memory address.
 constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
-constexpr int kRoundMagicBits = 0x4B400000;
+constexpr unsigned kRoundMagicBits = 0x4B400000u;
 
 // Approximate reciprocal (the PTX rcp.approx instruction, flushing
 // subnormals): one instruction, relative error about 1 ulp.
@@ -696,49 +702,70 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
-// Layout of one line's midpoint table (n cells, entries 0..n): n + 1 FP64
-// values C_i + r_i/2 padded to an even count, then n + 1 FP32 cell values r_i
-// padded to a multiple of four.  Both parts, and so every line of a stack of
-// tables, start on a 16-byte boundary, as bulk copies require.  A warp reads
-// 8 + 4 bytes per edge in two accesses instead of one 16-byte access: the
-// edges of a warp spread over more entries than lanes, so the wavefronts of a
-// read grow with the bytes spanned, not with the number of accesses.
-__host__ __device__ __forceinline__ int line_nf(int n) { return (n + 2) & ~1; }
-__host__ __device__ __forceinline__ int line_nr(int n) { return (n + 4) & ~3; }
+// a * b + c rounded once, clamped to [0, 1] (NaN to 0)
+__device__ __forceinline__ float fma_sat(float a, float b, float c) {
+    float y;
+    asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(y) : "f"(a), "f"(b), "f"(c));
+    return y;
+}
+
+__device__ __forceinline__ double lds_f64(unsigned addr) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+    return v;
+}
+
+__device__ __forceinline__ float lds_f32(unsigned addr) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+
+// Layout of one line's midpoint table (n cells, entries 0..n+1): n + 2 FP64
+// values M_i padded to an even count, then n + 2 FP32 cell values r_i padded
+// to a multiple of four.  Both parts, and so every line of a stack of tables,
+// start on a 16-byte boundary, as bulk copies require.  A warp reads 8 + 4
+// bytes per edge in two accesses: the edges of a warp spread over more
+// entries than lanes, so the wavefronts of a read grow with the bytes
+// spanned, and 12 bytes span fewer than one 16-byte entry would.
+__host__ __device__ __forceinline__ int line_nf(int n) { return (n + 3) & ~1; }
+__host__ __device__ __forceinline__ int line_nr(int n) { return (n + 5) & ~3; }
 __host__ __device__ __forceinline__ size_t line_bytes(int n) { return (size_t)8 * line_nf(n) + (size_t)4 * line_nr(n); }
 
-// The FP64 and FP32 parts of a line table, offset to the origin entry h.
-__device__ __forceinline__ const double* line_f(const unsigned char* line, int h) {
-    return reinterpret_cast<const double*>(line) + h;
-}
-__device__ __forceinline__ const float* line_r(const unsigned char* line, int n, int h) {
-    return reinterpret_cast<const float*>(line + 8 * line_nf(n)) + h;
+// Shared-memory base offsets of a line table for the lookup of fp_line: the
+// address of the entry of cell i is base + size * (kRoundMagicBits + i) + size
+// (32-bit arithmetic, modulo 2^32).
+struct LineBase {
+    unsigned f, r;
+};
+__device__ __forceinline__ LineBase line_base(const unsigned char* line, int n) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(line);
+    return {a + 8u - 8u * kRoundMagicBits, a + 8u * (unsigned)line_nf(n) + 4u - 4u * kRoundMagicBits};
 }
 
-// One image line's contribution to a thread's NI edge groups.  Fm and Rc are
-// the FP64 midpoint values and the FP32 cell values of the line's table,
-// offset to the origin entry h; t is the line's coordinate from the anchor
-// line, positions clamped to [lo_lim, hi_lim].
-//   parallel: edge position A + B t, the same slope B for every edge of a
-//        view, so a cell's footprint has the same width on every line; the
-//        lane adds F at its edge (accd += entry in FP64, the small r * frac
-//        part in FP32 in alo, folded into accd every 16 lines).
+// One image line's contribution to a thread's NI edge groups.  L is the
+// line's table, t the line's coordinate from the anchor line, W = n + 1 and
+// Cm = 1.5*2^23 - 1.  Positions and slopes are normalised (xn above):
+//   parallel: edge position A + B t, A on the anchor line (fp_norm_grid) and
+//        the same slope B for every edge of a view, so a cell's footprint
+//        has the same width on every line; the lane adds F at its edge
+//        (accd += M in FP64, the small r * frac part in FP32 in alo, folded
+//        into accd every 16 lines).
 //   FAN: edge position A + B tau with A, S the source's position and line
 //        coordinate and tau = t - S the line's distance from the source
 //        (the same for every edge of the view), so the footprint between
-//        edges j and j+1 is (B_j+1 - B_j) tau wide; the lane adds F / tau
-//        (the FP32 weight 1/tau is common to the cell's two edges, so its
-//        rounding only reweights the line).
-// Positions are measured from the middle of the line so that their FP32
-// rounding is half as large.  ONEV (fan beams, one view per CTA): every edge
-// group of the warp belongs to the same view (dummy groups past the view
-// included, whose results are dropped), so tau and its weight are computed
-// once per line from group 0's source coordinate.
+//        edges j and j+1 is (B_j+1 - B_j) tau wide, and the rounding of the
+//        common A cancels in it; the lane adds F / tau (the FP32 weight
+//        1/tau is common to the cell's two edges, so its rounding only
+//        reweights the line).
+// ONEV (fan beams, one view per CTA): every edge group of the warp belongs
+// to the same view (dummy groups past the view included, whose results are
+// dropped), so tau and its weight are computed once per line from group 0's
+// source coordinate.
 template <bool FAN, int NI, bool ONEV = false>
-__device__ __forceinline__ void fp_line(const double* __restrict__ Fm, const float* __restrict__ Rc, float t,
-                                        float lo_lim, float hi_lim,
-                                        const float (&A)[NI], const float (&B)[NI], const float (&S)[NI],
-                                        double (&accd)[NI], float (&alo)[NI]) {
+__device__ __forceinline__ void fp_line(LineBase L, float t, float W, float Cm, const float (&A)[NI],
+                                        const float (&B)[NI], const float (&S)[NI], double (&accd)[NI],
+                                        float (&alo)[NI]) {
     float tau1 = t, wgt1 = 1.f;
     if constexpr (FAN && ONEV) {
         tau1 = t - S[0];
@@ -754,13 +781,12 @@ __device__ __forceinline__ void fp_line(const double* __restrict__ Fm, const flo
             wgt = rcp_approx(tau);
             wd = (double)wgt;
         }
-        const float xr = fmaf(B[q], tau, A[q]);
-        const float xs = clampf(xr, lo_lim, hi_lim);
-        const float tt = xs + kRoundMagic;
-        const int i = __float_as_int(tt) - kRoundMagicBits;
-        const double F = Fm[i];
-        const float r = Rc[i];
-        const float frac = xs - (tt - kRoundMagic);
+        const float xn = fma_sat(B[q], FAN ? tau : t, A[q]);
+        const float tt = fmaf(xn, W, Cm);
+        const unsigned bits = __float_as_uint(tt);
+        const double F = lds_f64(L.f + 8u * bits);
+        const float r = lds_f32(L.r + 4u * bits);
+        const float frac = fmaf(xn, W, Cm - tt);
         if constexpr (FAN) {
             accd[q] = fma(wd, F, accd[q]);
             alo[q] = fmaf(wgt * r, frac, alo[q]);
@@ -781,36 +807,49 @@ __device__ __forceinline__ void fp_renorm(double (&accd)[NI], float (&alo)[NI]) 
     }
 }
 
+// Normalised edge coordinate of fp_line on a line of n cells: (v + add) /
+// (n + 1) in FP64 (inv = 1 / (n + 1)), rounded to FP32 (add = 1/2 for a
+// position, 0 for a slope).
+__device__ __forceinline__ float fp_norm(double v, double add, double inv) { return (float)((v + add) * inv); }
+
+// Normalised position of a parallel-beam edge on the anchor line, on the
+// grid of multiples of 2^-24 (fp_norm, then rounded to that grid): the
+// positions A_j + B t of a view's edges share B t, so with every A_j on a
+// grid no finer than that of the sums, the sums of one binade round alike
+// and the footprint widths between the edges stay exactly A_j+1 - A_j, the
+// widths fp_cell_sum divides by.
+__device__ __forceinline__ float fp_norm_grid(double v, double add, double inv) {
+    constexpr double kGrid = 16777216.0;  // 2^24
+    return (float)(rint((v + add) * inv * kGrid) / kGrid);
+}
+
 // Sum over lines of the cell integral over the footprint width, for the cell
 // between this lane's edge and the next lane's (all lanes call it, sums
 // renormalised first): the difference of the two edge sums over the
-// difference of W, the edge's position at the anchor line (parallel) or its
-// slope (fan).
+// difference of W, the edge's normalised position at the anchor line
+// (parallel) or its normalised slope (fan); the caller divides by n + 1.
 __device__ __forceinline__ float fp_cell_sum(double accd, float W) {
     const double dn = __shfl_down_sync(0xffffffffu, accd, 1);
     const float Wn = __shfl_down_sync(0xffffffffu, W, 1);
     return __fdividef((float)(dn - accd), Wn - W);
 }
 
-// Offset of the position origin from the start of a line of n cells: the
-// middle entry.  Even, so that the clamped ends -h - 1/2 and n - h - 1/2
-// round (half to even) onto table entries 0 and n or n - 1.
-__device__ __forceinline__ int fp_origin(int n) { return (n >> 1) & ~1; }
-
-// FP64 midpoint table of one line, built by one warp: n+1 entries C_i + r_i/2
-// and r_i (line_nf), C_i the integral over cells [0, i) and r_i the cell
-// value (0 past the end); the padding entries are zero.
+// FP64 midpoint table of one line, built by one warp: entries k = 0..n+1 of
+// cells i = k - 1 (zero cells at -1 and n), M_i = C_i + r_i/2 and r_i, C_i
+// the integral over cells [0, i) and r_i the cell value; the padding entries
+// are zero.
 template <typename Tin>
 __device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line, const Tin* __restrict__ row,
                                                 int n, int lane) {
     double* Fm = reinterpret_cast<double*>(line);
     float* Rc = reinterpret_cast<float*>(line + 8 * line_nf(n));
-    const int E = (n + 1 + 31) / 32;
+    const int ne = n + 2;
+    const int E = (ne + 31) / 32;
     const int k0 = lane * E;
     double tot = 0.0;
     for (int q = 0; q < E; ++q) {
-        const int k = k0 + q;
-        if (k < n) tot += (double)ldf(row + k);
+        const int i = k0 + q - 1;
+        if (i >= 0 && i < n) tot += (double)ldf(row + i);
     }
     double inc = tot;  // inclusive scan of the lane totals
 #pragma unroll
@@ -820,16 +859,16 @@ __device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line
     }
     double c = inc - tot;
     for (int q = 0; q < E; ++q) {
-        const int k = k0 + q;
-        if (k <= n) {
-            const float r = k < n ? ldf(row + k) : 0.f;
+        const int k = k0 + q, i = k - 1;
+        if (k < ne) {
+            const float r = (i >= 0 && i < n) ? ldf(row + i) : 0.f;
             Fm[k] = c + 0.5 * (double)r;
             Rc[k] = r;
             c += (double)r;
         }
     }
-    if (n + 1 + lane < line_nf(n)) Fm[n + 1 + lane] = 0.0;
-    if (n + 1 + lane < line_nr(n)) Rc[n + 1 + lane] = 0.f;
+    if (ne + lane < line_nf(n)) Fm[ne + lane] = 0.0;
+    if (ne + lane < line_nr(n)) Rc[ne + lane] = 0.f;
 }
 
 // Stage lines (length n, stride n between lines) into consecutive tables.
@@ -883,13 +922,12 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
         float A[NI], B[NI], S[NI], alo[NI];
         double accd[NI];
         bool any = false;
-        const int h = fp_origin(n);
-        const float shift = 0.5f + (float)h;  // midpoint tables, origin at entry h
+        const double inv = 1.0 / (double)(n + 1);
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
             const int it = warp + 8 * q;
             // dummy edges (results dropped): positions in range, tau never 0
-            A[q] = (float)lane - shift;
+            A[q] = 0.5f;
             B[q] = 0.f;
             S[q] = 0.5f;
             accd[q] = 0.0;
@@ -902,8 +940,8 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
                 const int j = 31 * m + lane;
                 if (active && j <= d.nu) {
                     const size_t ie = (size_t)view * (d.nu + 1) + j;
-                    A[q] = (FAN ? tab.sP[o][view] : tab.eA[o][ie]) - shift;
-                    B[q] = tab.eB[o][ie];
+                    A[q] = FAN ? fp_norm(tab.sP[o][view], 0.5, inv) : fp_norm_grid(tab.eA[o][ie], 0.5, inv);
+                    B[q] = fp_norm((double)tab.eB[o][ie], 0.0, inv);
                     if (FAN) S[q] = tab.sS[o][view];
                     any = true;
                 }
@@ -911,18 +949,16 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
         }
         // every warp takes part in staging whether or not it has work
         if (!__syncthreads_or(any)) continue;
-        const float lo_lim = -shift, hi_lim = (float)n - shift;
+        const float W = (float)(n + 1), Cm = kRoundMagic - 1.f;
         const int renorm = max(1, 16 / nrows_chunk);  // chunks between renormalisations
         for (int l0 = 0, c = 0; l0 < nl; l0 += nrows_chunk, ++c) {
             const int nlc = min(nrows_chunk, nl - l0);
             __syncthreads();
             stage_lines<Tin>(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
             __syncthreads();
-            for (int r = 0; r < nlc; ++r) {
-                const unsigned char* line = s_lines + (size_t)r * line_bytes(n);
-                fp_line<FAN, NI, ONEV>(line_f(line, h), line_r(line, n, h), (float)(l0 + r - anchor), lo_lim,
-                                       hi_lim, A, B, S, accd, alo);
-            }
+            for (int r = 0; r < nlc; ++r)
+                fp_line<FAN, NI, ONEV>(line_base(s_lines + (size_t)r * line_bytes(n), n), (float)(l0 + r - anchor),
+                                       W, Cm, A, B, S, accd, alo);
             if ((c + 1) % renorm == 0) fp_renorm<NI>(accd, alo);
         }
         fp_renorm<NI>(accd, alo);
@@ -930,7 +966,7 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
         for (int q = 0; q < NI; ++q) {
             const int it = warp + 8 * q;
             if (it >= nitems) continue;
-            const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]);
+            const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]) / W;
             const int vi = it / ipv, m = it - vi * ipv;
             const int view = v0 + vi;
             const int k = 31 * m + lane;
@@ -1088,14 +1124,13 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         const int c = o == 0 ? k : k - nc0;
         const int n = o == 0 ? g.nx : g.ny, nl = o == 0 ? g.ny : g.nx;
         const int last = (o == 0 ? nc0 : nc1) - 1;
-        const int h = fp_origin(n);
-        const float shift = 0.5f + (float)h;  // midpoint tables, origin at entry h
         if (c == 0) {
+            const double inv = 1.0 / (double)(n + 1);
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
                 const int it = warp + 8 * q;
                 // dummy edges (results dropped): positions in range, tau never 0
-                A[q] = (float)lane - shift;
+                A[q] = 0.5f;
                 B[q] = 0.f;
                 S[q] = 0.5f;
                 accd[q] = 0.0;
@@ -1108,8 +1143,8 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
                     const int j = 31 * m + lane;
                     if (active && j <= d.nu) {
                         const size_t ie = (size_t)view * (d.nu + 1) + j;
-                        A[q] = (FAN ? tab.sP[o][view] : tab.eA[o][ie]) - shift;
-                        B[q] = tab.eB[o][ie];
+                        A[q] = FAN ? fp_norm(tab.sP[o][view], 0.5, inv) : fp_norm_grid(tab.eA[o][ie], 0.5, inv);
+                        B[q] = fp_norm((double)tab.eB[o][ie], 0.0, inv);
                         if (FAN) S[q] = tab.sS[o][view];
                     }
                 }
@@ -1120,20 +1155,19 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         const unsigned char* buf = s_ring + (k & 1) * ring;
         const int anchor = o == 0 ? tab.ym : tab.xm;
         const int l0 = c * rchunk, nlc = min(rchunk, nl - l0);
-        const float lo_lim = -shift, hi_lim = (float)n - shift;
+        const float W = (float)(n + 1), Cm = kRoundMagic - 1.f;
         float tl = (float)(l0 - anchor);  // line coordinate, stepped exactly
-        const size_t lb = line_bytes(n);
-        for (int r = 0; r < nlc && !failed; ++r, tl += 1.f) {
-            const unsigned char* line = buf + r * lb;
-            fp_line<FAN, NI, ONEV>(line_f(line, h), line_r(line, n, h), tl, lo_lim, hi_lim, A, B, S, accd, alo);
-        }
+        LineBase L = line_base(buf, n);
+        const unsigned lb = (unsigned)line_bytes(n);
+        for (int r = 0; r < nlc && !failed; ++r, tl += 1.f, L.f += lb, L.r += lb)
+            fp_line<FAN, NI, ONEV>(L, tl, W, Cm, A, B, S, accd, alo);
         if ((c + 1) % renorm == 0 || c == last) fp_renorm<NI>(accd, alo);
         if (c == last && !failed) {
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
                 const int it = warp + 8 * q;
                 if (it >= nitems) continue;
-                const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]);
+                const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]) / (float)(n + 1);
                 const int vi = it / ipv, m = it - vi * ipv;
                 const int view = v0 + vi;
                 const int kk = 31 * m + lane;
