@@ -743,6 +743,23 @@ __device__ __forceinline__ LineBase line_base(const unsigned char* line, int n) 
     return {a + 8u - 8u * kRoundMagicBits, a + 8u * (unsigned)line_nf(n) + 4u - 4u * kRoundMagicBits};
 }
 
+// Edge group q of a warp: its view within the CTA (vi) and its group of 31
+// cells within the view (m).  wpv > 0: each view has wpv consecutive warps
+// and a warp's groups all belong to one view (fan beams share the line's
+// weight across them); wpv == 0: the CTA's edge groups are numbered view by
+// view across the 8 warps, it = warp + 8 q (parallel beams, densest packing).
+// The group is real if vi < the CTA's views and m < the groups per view.
+__device__ __forceinline__ void fp_item(int warp, int q, int ipv, int wpv, int& vi, int& m) {
+    if (wpv > 0) {
+        vi = warp / wpv;
+        m = warp - vi * wpv + wpv * q;
+    } else {
+        const int it = warp + 8 * q;
+        vi = it / ipv;
+        m = it - vi * ipv;
+    }
+}
+
 // One image line's contribution to a thread's NI edge groups.  L is the
 // line's table, t the line's coordinate from the anchor line, W = n + 1 and
 // Cm = 1.5*2^23 - 1.  Positions and slopes are normalised (xn above):
@@ -758,30 +775,22 @@ __device__ __forceinline__ LineBase line_base(const unsigned char* line, int n) 
 //        common A cancels in it; the lane adds F / tau (the FP32 weight
 //        1/tau is common to the cell's two edges, so its rounding only
 //        reweights the line).
-// ONEV (fan beams, one view per CTA): every edge group of the warp belongs
-// to the same view (dummy groups past the view included, whose results are
-// dropped), so tau and its weight are computed once per line from group 0's
-// source coordinate.
-template <bool FAN, int NI, bool ONEV = false>
+// Fan beams: every edge group of the warp belongs to the same view (fp_item;
+// dummy groups past the view included, whose results are dropped), so tau and
+// its weight are computed once per line from group 0's source coordinate.
+template <bool FAN, int NI>
 __device__ __forceinline__ void fp_line(LineBase L, float t, float W, float Cm, const float (&A)[NI],
                                         const float (&B)[NI], const float (&S)[NI], double (&accd)[NI],
                                         float (&alo)[NI]) {
-    float tau1 = t, wgt1 = 1.f;
-    if constexpr (FAN && ONEV) {
-        tau1 = t - S[0];
-        wgt1 = rcp_approx(tau1);
+    float tau = t, wgt = 1.f;
+    if constexpr (FAN) {
+        tau = t - S[0];  // |tau| >= 1/2 (a dummy warp) or the source's distance
+        wgt = rcp_approx(tau);
     }
-    const double wd1 = (double)wgt1;
+    const double wd = (double)wgt;
 #pragma unroll
     for (int q = 0; q < NI; ++q) {
-        float tau = tau1, wgt = wgt1;
-        double wd = wd1;
-        if constexpr (FAN && !ONEV) {
-            tau = t - S[q];  // |tau| >= 1/2 (dummies) or the source's distance
-            wgt = rcp_approx(tau);
-            wd = (double)wgt;
-        }
-        const float xn = fma_sat(B[q], FAN ? tau : t, A[q]);
+        const float xn = fma_sat(B[q], tau, A[q]);
         const float tt = fmaf(xn, W, Cm);
         const unsigned bits = __float_as_uint(tt);
         const double F = lds_f64(L.f + 8u * bits);
@@ -899,10 +908,10 @@ __global__ void __launch_bounds__(256) line_tables_kernel(unsigned char* __restr
 template <bool FAN, int NI>
 constexpr int fp_fast_min_blocks() { return NI <= 4 ? 3 : 2; }
 
-template <bool FAN, int NI, typename Tin, typename Tout, bool ONEV = false>
+template <bool FAN, int NI, typename Tin, typename Tout>
 __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_fast_kernel(Tout* __restrict__ prj, const Tin* __restrict__ img,
                                                            const Tin* __restrict__ imgT, DDTab tab, Grid g, Det d,
-                                                           int nview, int vgroup, int nrows_chunk,
+                                                           int nview, int vgroup, int wpv, int nrows_chunk,
                                                            const float* __restrict__ deg, int unweight_par) {
     extern __shared__ float4 s_lines4[];
     unsigned char* s_lines = reinterpret_cast<unsigned char*>(s_lines4);
@@ -912,7 +921,6 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
     const int slice = blockIdx.y;  // b * nz + iz, detector row iv = iz
     const int iz = slice % g.nz, b = slice / g.nz;
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
-    const int nitems = nvg * ipv;
 
     for (int o = 0; o < 2; ++o) {
         const int n = o == 0 ? g.nx : g.ny;   // cells per line
@@ -925,15 +933,15 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
         const double inv = 1.0 / (double)(n + 1);
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
-            const int it = warp + 8 * q;
+            int vi, m;
+            fp_item(warp, q, ipv, wpv, vi, m);
             // dummy edges (results dropped): positions in range, tau never 0
             A[q] = 0.5f;
             B[q] = 0.f;
             S[q] = 0.5f;
             accd[q] = 0.0;
             alo[q] = 0.f;
-            if (it < nitems) {
-                const int vi = it / ipv, m = it - vi * ipv;
+            if (vi < nvg && m < ipv) {
                 const int view = v0 + vi;
                 const float wx = tab.wx[view];
                 const bool active = o == 0 ? wx > 0.f : wx < 1.f;
@@ -957,17 +965,17 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
             stage_lines<Tin>(s_lines, src + (size_t)l0 * n, nlc, n, warp, lane, 8);
             __syncthreads();
             for (int r = 0; r < nlc; ++r)
-                fp_line<FAN, NI, ONEV>(line_base(s_lines + (size_t)r * line_bytes(n), n), (float)(l0 + r - anchor),
+                fp_line<FAN, NI>(line_base(s_lines + (size_t)r * line_bytes(n), n), (float)(l0 + r - anchor),
                                        W, Cm, A, B, S, accd, alo);
             if ((c + 1) % renorm == 0) fp_renorm<NI>(accd, alo);
         }
         fp_renorm<NI>(accd, alo);
 #pragma unroll
         for (int q = 0; q < NI; ++q) {
-            const int it = warp + 8 * q;
-            if (it >= nitems) continue;
+            int vi, m;
+            fp_item(warp, q, ipv, wpv, vi, m);
+            if (vi >= nvg || m >= ipv) continue;
             const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]) / W;
-            const int vi = it / ipv, m = it - vi * ipv;
             const int view = v0 + vi;
             const int k = 31 * m + lane;
             const float wx = tab.wx[view];
@@ -983,9 +991,9 @@ __global__ void __launch_bounds__(256, (fp_fast_min_blocks<FAN, NI>())) dd2d_fp_
         // FORCE_FBP on parallel FP: cancel the ray-length weight
         // (ReverseWeightBPParallelKernel, distanceDriven2DUtils.cu:68-94)
         for (int q = 0; q < NI; ++q) {
-            const int it = warp + 8 * q;
-            if (it >= nitems) continue;
-            const int vi = it / ipv, m = it - vi * ipv;
+            int vi, m;
+            fp_item(warp, q, ipv, wpv, vi, m);
+            if (vi >= nvg || m >= ipv) continue;
             const int view = v0 + vi;
             const int k = 31 * m + lane;
             if (lane >= 31 || k >= d.nu) continue;
@@ -1058,10 +1066,10 @@ __device__ unsigned int g_first_wait_polls = kWaitPolls;
 template <bool FAN, int NI>
 constexpr int fp_stream_min_blocks() { return NI <= 8 ? 3 : 2; }
 
-template <bool FAN, int NI, typename Tout, bool ONEV = false>
+template <bool FAN, int NI, typename Tout>
 __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const unsigned char* __restrict__ ltab0,
                                                              const unsigned char* __restrict__ ltab1, DDTab tab, Grid g,
-                                                             Det d, int nview, int vgroup, int rchunk,
+                                                             Det d, int nview, int vgroup, int wpv, int rchunk,
                                                              const float* __restrict__ deg, int unweight_par) {
     extern __shared__ float4 s_ring4[];  // [2][rchunk line tables of max(nx, ny) cells]
     unsigned char* s_ring = reinterpret_cast<unsigned char*>(s_ring4);
@@ -1072,7 +1080,6 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
     const int slice = blockIdx.y;  // b * nz + iz, detector row iv = iz
     const int iz = slice % g.nz, b = slice / g.nz;
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
-    const int nitems = nvg * ipv;
     const size_t ring = (size_t)rchunk * line_bytes(max(g.nx, g.ny));  // bytes per buffer
 
     // orientations with work in this CTA: rows (o = 0) for views traced along
@@ -1128,15 +1135,15 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
             const double inv = 1.0 / (double)(n + 1);
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
-                const int it = warp + 8 * q;
+                int vi, m;
+                fp_item(warp, q, ipv, wpv, vi, m);
                 // dummy edges (results dropped): positions in range, tau never 0
                 A[q] = 0.5f;
                 B[q] = 0.f;
                 S[q] = 0.5f;
                 accd[q] = 0.0;
                 alo[q] = 0.f;
-                if (it < nitems) {
-                    const int vi = it / ipv, m = it - vi * ipv;
+                if (vi < nvg && m < ipv) {
                     const int view = v0 + vi;
                     const float wx = tab.wx[view];
                     const bool active = o == 0 ? wx > 0.f : wx < 1.f;
@@ -1160,15 +1167,15 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         LineBase L = line_base(buf, n);
         const unsigned lb = (unsigned)line_bytes(n);
         for (int r = 0; r < nlc && !failed; ++r, tl += 1.f, L.f += lb, L.r += lb)
-            fp_line<FAN, NI, ONEV>(L, tl, W, Cm, A, B, S, accd, alo);
+            fp_line<FAN, NI>(L, tl, W, Cm, A, B, S, accd, alo);
         if ((c + 1) % renorm == 0 || c == last) fp_renorm<NI>(accd, alo);
         if (c == last && !failed) {
 #pragma unroll
             for (int q = 0; q < NI; ++q) {
-                const int it = warp + 8 * q;
-                if (it >= nitems) continue;
+                int vi, m;
+                fp_item(warp, q, ipv, wpv, vi, m);
+                if (vi >= nvg || m >= ipv) continue;
                 const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]) / (float)(n + 1);
-                const int vi = it / ipv, m = it - vi * ipv;
                 const int view = v0 + vi;
                 const int kk = 31 * m + lane;
                 const float wx = tab.wx[view];
@@ -1195,9 +1202,9 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
         // FORCE_FBP on parallel FP: cancel the ray-length weight
         // (ReverseWeightBPParallelKernel, distanceDriven2DUtils.cu:68-94)
         for (int q = 0; q < NI; ++q) {
-            const int it = warp + 8 * q;
-            if (it >= nitems) continue;
-            const int vi = it / ipv, m = it - vi * ipv;
+            int vi, m;
+            fp_item(warp, q, ipv, wpv, vi, m);
+            if (vi >= nvg || m >= ipv) continue;
             const int view = v0 + vi;
             const int kk = 31 * m + lane;
             if (lane >= 31 || kk >= d.nu) continue;
@@ -1865,30 +1872,30 @@ bool fp_stream_shape(const ctp_geometry& g, int& vgroup, int& ni, int max_ni = 1
 }
 
 // Views per CTA and edge groups per warp of the fan forward projectors.
-// The kernels are issue-bound, so their time goes as (waves of resident
-// CTAs) x (edge-group slots per CTA) x (CTAs sharing an SM); the shape
-// minimising that product wins, the larger view group on a tie (fewer
-// copies of the slice's tables).  Several views per CTA take 4 or 8 groups
-// per warp (six registers per group, three CTAs per SM).  A single view per
-// CTA lets the edge groups share the per-line weight and the source
-// coordinate (fp_line ONEV, five registers per group), so it also takes 12 or
-// 16 groups (two CTAs per SM): detectors of up to 128 groups of 31 cells.
-// False if one view does not fit 16 groups per warp.
+// Each of the v views of a CTA (1, 2, 4 or 8) gets 8 / v consecutive warps,
+// so that a warp's edge groups share the per-line weight and the source
+// coordinate (fp_item, fp_line); a view's groups take ceil(ipv v / 8) per
+// warp, rounded up to a compiled count (4, 8, 12 or 16).  The kernels are
+// issue-bound, so the launch's time goes as its CTAs times a CTA's groups per
+// warp plus the per-line work they share (measured at about half a group on
+// the 4 x 512^2, 984-view, 888-cell fan workload: 1.85, 1.81 and 1.75 ms for
+// 1, 2 and 4 views per CTA); the cheapest shape wins, the larger view group
+// on a tie (fewer copies of the slice's tables), among those that keep at
+// least two CTAs per SM.  False if one view does not fit 16 groups per warp
+// (detectors of more than 128 groups of 31 cells).
 bool fan_shape(const ctp_geometry& g, int nslices, int sms, int& vgroup, int& ni) {
     const int ipv = (int)((g.nu + 30) / 31);
     vgroup = 0;
     ni = 0;
     if (ipv == 0 || g.nview == 0 || nslices <= 0) return false;
     long long best = -1;
-    for (int v = 1; v <= (int)g.nview; ++v) {
-        const int per_warp = (v * ipv + 7) / 8;
-        int n = per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : 0;
-        if (!n && v == 1) n = per_warp <= 12 ? 12 : per_warp <= 16 ? 16 : 0;
-        if (!n) break;
-        const int cpsm = n <= 8 ? 3 : 2;
-        const long long slots = (long long)cpsm * std::max(sms, 1);
+    for (int v = 1; v <= 8 && v <= (int)g.nview; v *= 2) {
+        const int per_warp = (ipv * v + 7) / 8;
+        const int n = per_warp <= 4 ? 4 : per_warp <= 8 ? 8 : per_warp <= 12 ? 12 : per_warp <= 16 ? 16 : 0;
+        if (!n) continue;
         const long long units = (long long)((g.nview + v - 1) / v) * nslices;
-        const long long cost = (units + slots - 1) / slots * n * cpsm;
+        if (v > 1 && units < 2LL * std::max(sms, 1)) break;
+        const long long cost = units * (2 * n + 1);
         if (best < 0 || cost <= best) {
             best = cost;
             vgroup = v;
@@ -1947,53 +1954,42 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         const int rc_s = rchunk;
         size_t shm = 2 * (size_t)rc_s * line_bytes((int)std::max(g.nx, g.ny));
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)nslices);
+        const bool fan = geom == 0;
+        const int wpv = fan ? 8 / sv : 0;  // fan beams: warps per view (fp_item)
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
             cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), lt0, lt1, tab, make_grid(g), make_det(g), (int)g.nview, sv,
-                                      rc_s, deg, unweight);
+                                      wpv, rc_s, deg, unweight);
         };
-        const bool fan = geom == 0;
 #define CTP_FP_STREAM(NI_)                                                       \
     if (fan) launch(dd2d_fp_stream_kernel<true, NI_, Tout>);                     \
     else launch(dd2d_fp_stream_kernel<false, NI_, Tout>)
-        if (fan && sv == 1) {
-            // one view per CTA: the per-line weight is shared by the edge groups
-            if (ni == 4) launch(dd2d_fp_stream_kernel<true, 4, Tout, true>);
-            else if (ni == 8) launch(dd2d_fp_stream_kernel<true, 8, Tout, true>);
-            else if (ni == 12) launch(dd2d_fp_stream_kernel<true, 12, Tout, true>);
-            else launch(dd2d_fp_stream_kernel<true, 16, Tout, true>);
-        }
-        else if (ni == 4) { CTP_FP_STREAM(4); }
+        if (ni == 4) { CTP_FP_STREAM(4); }
         else if (ni == 8) { CTP_FP_STREAM(8); }
-        else if (ni == 12) launch(dd2d_fp_stream_kernel<false, 12, Tout>);  // (fan: one view per CTA, above)
-        else launch(dd2d_fp_stream_kernel<false, 16, Tout>);
+        else if (ni == 12) { CTP_FP_STREAM(12); }
+        else { CTP_FP_STREAM(16); }
 #undef CTP_FP_STREAM
         return check_launch("dd2d_fp_stream_kernel");
     }
     if (shaped) {
         size_t shm = (size_t)nrows * line_bytes((int)std::max(g.nx, g.ny));
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)(g.nbatch * g.nz));
+        const bool fan = geom == 0;
+        const int wpv = fan ? 8 / sv : 0;  // fan beams: warps per view (fp_item)
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
             cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), cptr<Tin>(img), imgT, tab, make_grid(g), make_det(g),
-                                      (int)g.nview, sv, nrows, deg, unweight);
+                                      (int)g.nview, sv, wpv, nrows, deg, unweight);
         };
-        const bool fan = geom == 0;
 #define CTP_FP_STAGED(NI_)                                                       \
     if (fan) launch(dd2d_fp_fast_kernel<true, NI_, Tin, Tout>);                  \
     else launch(dd2d_fp_fast_kernel<false, NI_, Tin, Tout>)
-        if (fan && sv == 1) {
-            if (ni == 4) launch(dd2d_fp_fast_kernel<true, 4, Tin, Tout, true>);
-            else if (ni == 8) launch(dd2d_fp_fast_kernel<true, 8, Tin, Tout, true>);
-            else if (ni == 12) launch(dd2d_fp_fast_kernel<true, 12, Tin, Tout, true>);
-            else launch(dd2d_fp_fast_kernel<true, 16, Tin, Tout, true>);
-        }
-        else if (ni == 4) { CTP_FP_STAGED(4); }
+        if (ni == 4) { CTP_FP_STAGED(4); }
         else if (ni == 8) { CTP_FP_STAGED(8); }
-        else if (ni == 12) launch(dd2d_fp_fast_kernel<false, 12, Tin, Tout>);  // (fan: one view per CTA, above)
-        else launch(dd2d_fp_fast_kernel<false, 16, Tin, Tout>);
+        else if (ni == 12) { CTP_FP_STAGED(12); }
+        else { CTP_FP_STAGED(16); }
 #undef CTP_FP_STAGED
         return check_launch("dd2d_fp_fast_kernel");
     }
