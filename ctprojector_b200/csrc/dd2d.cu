@@ -847,9 +847,8 @@ __device__ __forceinline__ float fp_cell_sum(double accd, float W) {
 // cells i = k - 1 (zero cells at -1 and n), M_i = C_i + r_i/2 and r_i, C_i
 // the integral over cells [0, i) and r_i the cell value; the padding entries
 // are zero.
-template <typename Tin>
-__device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line, const Tin* __restrict__ row,
-                                                int n, int lane) {
+template <typename Cell>
+__device__ __forceinline__ void build_line_fp64(unsigned char* __restrict__ line, int n, int lane, Cell cell) {
     double* Fm = reinterpret_cast<double*>(line);
     float* Rc = reinterpret_cast<float*>(line + 8 * line_nf(n));
     const int ne = n + 2;
@@ -858,7 +857,7 @@ __device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line
     double tot = 0.0;
     for (int q = 0; q < E; ++q) {
         const int i = k0 + q - 1;
-        if (i >= 0 && i < n) tot += (double)ldf(row + i);
+        if (i >= 0 && i < n) tot += (double)cell(i);
     }
     double inc = tot;  // inclusive scan of the lane totals
 #pragma unroll
@@ -870,7 +869,7 @@ __device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line
     for (int q = 0; q < E; ++q) {
         const int k = k0 + q, i = k - 1;
         if (k < ne) {
-            const float r = (i >= 0 && i < n) ? ldf(row + i) : 0.f;
+            const float r = (i >= 0 && i < n) ? cell(i) : 0.f;
             Fm[k] = c + 0.5 * (double)r;
             Rc[k] = r;
             c += (double)r;
@@ -878,6 +877,13 @@ __device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line
     }
     if (ne + lane < line_nf(n)) Fm[ne + lane] = 0.0;
     if (ne + lane < line_nr(n)) Rc[ne + lane] = 0.f;
+}
+
+// The same from a row of the image in global memory.
+template <typename Tin>
+__device__ __forceinline__ void stage_line_fp64(unsigned char* __restrict__ line, const Tin* __restrict__ row,
+                                                int n, int lane) {
+    build_line_fp64(line, n, lane, [&](int i) { return ldf(row + i); });
 }
 
 // Stage lines (length n, stride n between lines) into consecutive tables.
@@ -888,15 +894,38 @@ __device__ void stage_lines(unsigned char* __restrict__ tab, const Tin* __restri
         stage_line_fp64(tab + (size_t)l * line_bytes(n), src + (size_t)l * n, n, lane);
 }
 
+// Shared memory of one warp of line_tables_kernel: a line's table, then its
+// cells (both multiples of 16 bytes).
+__host__ __device__ __forceinline__ size_t line_tables_warp_bytes(int n) {
+    return line_bytes(n) + (((size_t)n * 4 + 15) & ~(size_t)15);
+}
+
 // The tables of every line of a stack of slices (one warp per line), for the
-// forward projector that streams them into shared memory.
+// forward projector that streams them into shared memory.  The warp reads the
+// line's cells into shared memory with coalesced loads, builds the table
+// there (each lane scans a run of consecutive entries) and writes it out with
+// coalesced 16-byte stores.
 template <typename Tin>
 __global__ void __launch_bounds__(256) line_tables_kernel(unsigned char* __restrict__ out,
                                                           const Tin* __restrict__ src, long long nlines, int n) {
-    const int lane = threadIdx.x & 31;
+    extern __shared__ float4 s_lt4[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const size_t lb = line_bytes(n);
+    unsigned char* tab = reinterpret_cast<unsigned char*>(s_lt4) + warp * line_tables_warp_bytes(n);
+    float* cells = reinterpret_cast<float*>(tab + lb);
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long l = w0; l < nlines; l += nw) stage_line_fp64(out + l * line_bytes(n), src + l * n, n, lane);
+    for (long long l = w0; l < nlines; l += nw) {
+        const Tin* row = src + l * n;
+        for (int i = lane; i < n; i += 32) cells[i] = ldf(row + i);
+        __syncwarp();
+        build_line_fp64(tab, n, lane, [&](int i) { return cells[i]; });
+        __syncwarp();
+        const uint4* from = reinterpret_cast<const uint4*>(tab);
+        uint4* to = reinterpret_cast<uint4*>(out + l * lb);
+        for (int i = lane; i < (int)(lb / 16); i += 32) to[i] = from[i];
+        __syncwarp();
+    }
 }
 
 // NI = edge groups per warp (compile time, so the group loop is straight-line
@@ -1933,10 +1962,15 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         unsigned char* lt0 = reinterpret_cast<unsigned char*>(ws + fp_workspace_min(g));
         unsigned char* lt1 = lt0 + g.nbatch * g.nz * g.ny * line_bytes((int)g.nx);
         long long rows = (long long)(g.nbatch * g.nz * g.ny), cols = (long long)(g.nbatch * g.nz * g.nx);
-        const unsigned rgrid = (unsigned)std::min<long long>((rows + 7) / 8, 148 * 16);
-        const unsigned cgrid = (unsigned)std::min<long long>((cols + 7) / 8, 148 * 16);
-        line_tables_kernel<Tin><<<rgrid, 256, 0, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
-        line_tables_kernel<Tin><<<cgrid, 256, 0, s>>>(lt1, imgT, cols, (int)g.ny);
+        // warps per CTA: as many as 96 KB of shared memory holds (at least one)
+        const size_t wb = line_tables_warp_bytes((int)std::max(g.nx, g.ny));
+        const int lt_warps = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / wb));
+        const size_t lt_shm = (size_t)lt_warps * wb;
+        cudaFuncSetAttribute(line_tables_kernel<Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lt_shm);
+        const unsigned rgrid = (unsigned)std::min<long long>((rows + lt_warps - 1) / lt_warps, 148 * 8);
+        const unsigned cgrid = (unsigned)std::min<long long>((cols + lt_warps - 1) / lt_warps, 148 * 8);
+        line_tables_kernel<Tin><<<rgrid, 32 * lt_warps, lt_shm, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
+        line_tables_kernel<Tin><<<cgrid, 32 * lt_warps, lt_shm, s>>>(lt1, imgT, cols, (int)g.ny);
         if ((rc = check_launch("line_tables_kernel"))) return rc;
         // one slice per CTA (sharing the edge work across two slices halves the
         // lines per table chunk, and the warps then wait on the copies instead)
