@@ -1272,6 +1272,80 @@ constexpr int kPT = 32;        // tile edge
 constexpr int kPViews = 32;    // views per staged chunk
 constexpr int kPMaxWin = 255;  // staged cells per view (table holds win+1 entries)
 
+// Window tables of the fast back projectors, staged by one warp M at a time:
+// for each item, entries k = 0 .. win of (running sum of the window cells
+// before k + value/2, value) for the cells w0 .. w0 + win - 1 of the detector
+// row at `row` (cells off the detector, and the entry past the window, are
+// zero; ok = false stages zeros, valid = false writes nothing).  Lane l scans
+// the PER consecutive entries from l PER of every item: it issues all M PER
+// loads before it sums, so that the items' load latencies overlap, then the
+// warp scans the lane sums and the lane writes its entries.
+template <typename Tp>
+struct WinItem {
+    float2* T;
+    const Tp* row;
+    int w0;
+    bool ok, valid;
+};
+// Windows a warp stages together: on the parallel 16 x 512^2, 720-view batch
+// the back projection takes 1.97, 1.75 and 1.90 ms with 1, 2 and 4 (4 spills).
+constexpr int kStageBatch = 2;
+
+template <int PER, int M, typename Tp>
+__device__ __forceinline__ void stage_windows_per(const WinItem<Tp> (&it)[M], int win, int nu, int lane) {
+    const int k0 = lane * PER;
+    float v[M][PER];
+    float run[M], incl[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int k = k0 + q, cell = it[m].w0 + k;
+            v[m][q] = (it[m].ok && k < win && cell >= 0 && cell < nu) ? ldf(it[m].row + cell) : 0.f;
+        }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        run[m] = 0.f;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) run[m] += v[m][q];
+        incl[m] = run[m];
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const float t = __shfl_up_sync(0xffffffffu, incl[m], o);
+            if (lane >= o) incl[m] += t;
+        }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        if (!it[m].valid) continue;
+        float base = incl[m] - run[m];
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int k = k0 + q;
+            if (k <= win) it[m].T[k] = make_float2(fmaf(0.5f, v[m][q], base), v[m][q]);
+            base += v[m][q];
+        }
+    }
+}
+
+// The same for any window of up to 255 cells: PER = ceil((win + 1) / 32),
+// a compile-time count, so a lane issues exactly its loads.
+template <int M, typename Tp>
+__device__ __forceinline__ void stage_windows(const WinItem<Tp> (&it)[M], int win, int nu, int lane) {
+    switch ((win + 1 + 31) / 32) {
+        case 1: stage_windows_per<1>(it, win, nu, lane); break;
+        case 2: stage_windows_per<2>(it, win, nu, lane); break;
+        case 3: stage_windows_per<3>(it, win, nu, lane); break;
+        case 4: stage_windows_per<4>(it, win, nu, lane); break;
+        case 5: stage_windows_per<5>(it, win, nu, lane); break;
+        case 6: stage_windows_per<6>(it, win, nu, lane); break;
+        case 7: stage_windows_per<7>(it, win, nu, lane); break;
+        default: stage_windows_per<8>(it, win, nu, lane); break;
+    }
+}
+
 struct ParView {
     float jb, jx, jy, sx;  // jb: window coordinate - 1/2 of the tile's first pixel centre
     float sy, jc, hx, hy;  // sx, sy: signed normalisations (0 = term inactive); jc: absolute coordinate
@@ -1375,49 +1449,27 @@ __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict_
         }
         __syncthreads();
         // stage (running sum + value/2, value) for window cells w0 .. w0+win-1; entry win = (total, 0)
-        for (int sv = warp; sv < S * nvc; sv += 8) {
-            const int s = sv / nvc, vi = sv - s * nvc;
-            const int w0 = s_w0[vi];
-            bool ok = w0 != INT_MIN;
-            const Tp* srow = rows[0];
-            bool rok = row_ok[0];
+        for (int sv0 = warp; sv0 < S * nvc; sv0 += 8 * kStageBatch) {
+            WinItem<Tp> it[kStageBatch];
 #pragma unroll
-            for (int q = 1; q < S; ++q)
-                if (s == q) {
-                    srow = rows[q];
-                    rok = row_ok[q];
-                }
-            ok = ok && rok;
-            const int view = v0 + vi;
-            const int per = (stride + 31) / 32;
-            const int k0 = lane * per;
-            float v[8];
-            float run = 0.f;
+            for (int m = 0; m < kStageBatch; ++m) {
+                const int sv = sv0 + 8 * m;
+                const int s = sv / nvc, vi = sv - s * nvc;
+                const Tp* srow = rows[0];
+                bool rok = row_ok[0];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                int k = k0 + q;
-                float x = 0.f;
-                if (ok && q < per && k < win) {
-                    int cell = w0 + k;
-                    if (cell >= 0 && cell < d.nu) x = ldf(srow + (size_t)view * vstride + cell);
-                }
-                v[q] = x;
-                run += x;
+                for (int q = 1; q < S; ++q)
+                    if (s == q) {
+                        srow = rows[q];
+                        rok = row_ok[q];
+                    }
+                it[m].valid = sv < S * nvc;
+                it[m].w0 = s_w0[vi];
+                it[m].ok = it[m].valid && it[m].w0 != INT_MIN && rok;
+                it[m].T = s_tab + s * tstride + vi * stride;
+                it[m].row = srow + (size_t)(v0 + vi) * vstride;
             }
-            float incl = run;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                float t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            float base = incl - run;
-            float2* T = s_tab + s * tstride + vi * stride;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                int k = k0 + q;
-                if (q < per && k < stride) T[k] = make_float2(fmaf(0.5f, v[q], base), v[q]);
-                base += v[q];
-            }
+            stage_windows(it, win, d.nu, lane);
         }
         __syncthreads();
         for (int vi = 0; vi < nvc; ++vi) {
@@ -1623,48 +1675,27 @@ __global__ void __launch_bounds__(256) dd2d_bp_fan_fast_kernel(Tout* __restrict_
             s_view[vi] = V;
         }
         __syncthreads();
-        for (int sv = warp; sv < S * nvc; sv += 8) {
-            const int s = sv / nvc, vi = sv - s * nvc;
-            const int w0 = s_view[vi].w0;
-            const Tp* srow = rows[0];
-            bool rok = row_ok[0];
+        for (int sv0 = warp; sv0 < S * nvc; sv0 += 8 * kStageBatch) {
+            WinItem<Tp> it[kStageBatch];
 #pragma unroll
-            for (int q = 1; q < S; ++q)
-                if (s == q) {
-                    srow = rows[q];
-                    rok = row_ok[q];
-                }
-            const bool ok = w0 != INT_MIN && rok;
-            const int view = v0 + vi;
-            const int per = (stride + 31) / 32;
-            const int k0 = lane * per;
-            float v[8];
-            float run = 0.f;
+            for (int m = 0; m < kStageBatch; ++m) {
+                const int sv = sv0 + 8 * m;
+                const int s = sv / nvc, vi = sv - s * nvc;
+                const Tp* srow = rows[0];
+                bool rok = row_ok[0];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                int k = k0 + q;
-                float x = 0.f;
-                if (ok && q < per && k < win) {
-                    int cell = w0 + k;
-                    if (cell >= 0 && cell < d.nu) x = ldf(srow + (size_t)view * vstride + cell);
-                }
-                v[q] = x;
-                run += x;
+                for (int q = 1; q < S; ++q)
+                    if (s == q) {
+                        srow = rows[q];
+                        rok = row_ok[q];
+                    }
+                it[m].valid = sv < S * nvc;
+                it[m].w0 = s_view[vi].w0;
+                it[m].ok = it[m].valid && it[m].w0 != INT_MIN && rok;
+                it[m].T = s_tab + s * tstride + vi * stride;
+                it[m].row = srow + (size_t)(v0 + vi) * vstride;
             }
-            float incl = run;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                float t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            float base = incl - run;
-            float2* T = s_tab + s * tstride + vi * stride;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                int k = k0 + q;
-                if (q < per && k < stride) T[k] = make_float2(fmaf(0.5f, v[q], base), v[q]);
-                base += v[q];
-            }
+            stage_windows(it, win, d.nu, lane);
         }
         __syncthreads();
         for (int vi = 0; vi < nvc; ++vi) {
