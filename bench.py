@@ -138,10 +138,10 @@ def algorithmic_bytes(nnz_slice: int, nb: int, scan) -> dict:
     return {"fp": proj, "bp": proj, "filter": 4 * 2 * n_prj, "bp_fbp": proj}
 
 
-# ours: launches of our own kernels per step (FP: edge table, transpose, row
-# and column line tables, streamed sweep; BP: gather; filter: one FFT row
-# convolution over every row; FBP BP: gather)
-OUR_LAUNCHES_PER_STEP = 5 + 1 + 1 + 1
+# ours: launches of our own kernels per step (FP: edge table, view order,
+# transpose, row and column line tables, streamed sweep; BP: gather; filter:
+# one FFT row convolution over every row; FBP BP: gather)
+OUR_LAUNCHES_PER_STEP = 6 + 1 + 1 + 1
 
 # The filter of the step runs in exact mode: FP64 arithmetic in one launch
 # (conv_rows_kernel).  The default mode replays the reference's FP32
@@ -153,7 +153,7 @@ FILTER_NOTE = ("hann ramp filter in exact mode (FP64 arithmetic, one launch; ~1e
 
 # the launches behind each timed projector operation (the roofline names the dominant one)
 ROOFLINE_KERNEL = {
-    "fp": "dd2d_fp_stream_kernel (with its edge-table, transpose and line-table launches)",
+    "fp": "dd2d_fp_stream_kernel (with its edge-table, view-order, transpose and line-table launches)",
     "bp": "dd2d_bp_par_fast_kernel",
     "bp_fbp": "dd2d_bp_par_fast_kernel (FBP weighting)",
 }

@@ -115,6 +115,7 @@ _SIGNATURES = {
     "ctp_dequantize_u16": [_P, _P, _P, _P, _S, _S, c_uint, _P],
     "ctp_ramp_filter_u16": [_P, _P, _P, _P, _GP, c_int, c_int, _P],
     "ctp_set_wait_limit": [c_uint],
+    "ctp_set_fp_stream_slices": [c_int],
     "ctp_scratch_allocations": [_P],
     "cSiddonFanProjection": [_P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, _F, _F, _F, _S, _S, _S, _F, _F, _F, _F, _F, _F],
     "cSiddonFanBackprojection": [_P, _P, _P, c_int, _S, _S, _S, _F, _F, _F, _F, _F, _F, _S, _S, _S, _F, _F, _F, _F, _F,

@@ -14,6 +14,7 @@ namespace ctp {
 // launchers defined in dd2d.cu, fbp.cu, siddon.cu, tomo.cu
 int dd2d_fp(void*, const void*, const float*, const ctp_geometry&, int, int, unsigned, void*, size_t, cudaStream_t);
 size_t dd2d_fp_workspace(const ctp_geometry&, int, int, unsigned);
+void set_fp_stream_cap(int max_slices);
 int dd2d_bp(void*, const void*, const float*, const ctp_geometry&, int, int, unsigned, void*, size_t, cudaStream_t);
 size_t dd2d_bp_workspace(const ctp_geometry&, int, int, unsigned);
 int dd2d_nnz(unsigned long long*, const float*, const ctp_geometry&, int, cudaStream_t);
@@ -757,6 +758,11 @@ int ctp_sqs_tv_update(float* x_out, void* x_lp, const float* x, const float* bp,
 int ctp_wait_timeouts(unsigned int* count) { return wait_timeouts(count); }
 
 int ctp_set_wait_limit(unsigned int first_chunk_polls) { return set_first_wait_polls(first_chunk_polls); }
+
+int ctp_set_fp_stream_slices(int max_slices) {
+    set_fp_stream_cap(max_slices);
+    return CTP_OK;
+}
 
 int ctp_quantize_u16(unsigned short* code, float* lo, float* step, const float* y, size_t nrows, size_t row_len,
                      void* stream) {

@@ -32,6 +32,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <type_traits>
 
@@ -1095,18 +1096,61 @@ __device__ unsigned int g_first_wait_polls = kWaitPolls;
 template <bool FAN, int NI>
 constexpr int fp_stream_min_blocks() { return NI <= 8 ? 3 : 2; }
 
+// The views in the order the streamed forward projector takes them: those of
+// the blend band (0 < wx < 1), which sweep both orientations and so take
+// about twice as long, first, then the others, each in their original order
+// (a stable partition).  The launch dispatches view groups in this order, so
+// its longest CTAs start in the first wave instead of trailing the last.
+// One CTA; ballots and per-warp counts give each view its position.
+__global__ void __launch_bounds__(1024) blend_first_kernel(int* __restrict__ order, const float* __restrict__ wx,
+                                                           int nview) {
+    __shared__ int s_cnt[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    auto in_band = [&](int v) { return v < nview && wx[v] > 0.f && wx[v] < 1.f; };
+    int nband = 0;
+    for (int t0 = 0; t0 < nview; t0 += blockDim.x) nband += __syncthreads_count(in_band(t0 + threadIdx.x));
+    int placed_band = 0, placed_rest = 0;
+    for (int t0 = 0; t0 < nview; t0 += blockDim.x) {
+        const int v = t0 + threadIdx.x;
+        const bool in = v < nview, band = in_band(v);
+        const unsigned mb = __ballot_sync(0xffffffffu, band), mi = __ballot_sync(0xffffffffu, in);
+        const unsigned below = (1u << lane) - 1u;
+        if (lane == 0) s_cnt[warp] = __popc(mb) | (__popc(mi) << 16);
+        __syncthreads();
+        int band_before = __popc(mb & below), all_before = __popc(mi & below), tile_band = 0, tile_all = 0;
+        for (int w = 0; w < nw; ++w) {
+            const int c = s_cnt[w];
+            if (w < warp) {
+                band_before += c & 0xffff;
+                all_before += c >> 16;
+            }
+            tile_band += c & 0xffff;
+            tile_all += c >> 16;
+        }
+        if (in)
+            order[band ? placed_band + band_before : nband + placed_rest + (all_before - band_before)] = v;
+        placed_band += tile_band;
+        placed_rest += tile_all - tile_band;
+        __syncthreads();
+    }
+}
+
 template <bool FAN, int NI, typename Tout>
 __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_fp_stream_kernel(Tout* __restrict__ prj, const unsigned char* __restrict__ ltab0,
                                                              const unsigned char* __restrict__ ltab1, DDTab tab, Grid g,
-                                                             Det d, int nview, int vgroup, int wpv, int rchunk,
-                                                             const float* __restrict__ deg, int unweight_par) {
+                                                             Det d, int nview, int vgroup, int wpv, int rchunk, int slice0,
+                                                             const int* __restrict__ order, const float* __restrict__ deg,
+                                                             int unweight_par) {
     extern __shared__ float4 s_ring4[];  // [2][rchunk line tables of max(nx, ny) cells]
     unsigned char* s_ring = reinterpret_cast<unsigned char*>(s_ring4);
     __shared__ __align__(8) unsigned long long s_bar[2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int v0 = blockIdx.x * vgroup;
+    // view group blockIdx.y of the views in `order` (blend-band views first),
+    // slice b * nz + iz (detector row iv = iz) whose tables are the launch's
+    // blockIdx.x-th
+    const int v0 = blockIdx.y * vgroup;
     const int nvg = min(vgroup, nview - v0);
-    const int slice = blockIdx.y;  // b * nz + iz, detector row iv = iz
+    const int slice = slice0 + (int)blockIdx.x;
     const int iz = slice % g.nz, b = slice / g.nz;
     const int ipv = (d.nu + 30) / 31;  // edge groups per view
     const size_t ring = (size_t)rchunk * line_bytes(max(g.nx, g.ny));  // bytes per buffer
@@ -1115,7 +1159,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
     // y, columns (o = 1) for views traced along x, both in the blend band
     bool act0 = false, act1 = false;
     for (int vi = threadIdx.x; vi < nvg; vi += blockDim.x) {
-        const float wx = tab.wx[v0 + vi];
+        const float wx = tab.wx[order[v0 + vi]];
         act0 |= wx > 0.f;
         act1 |= wx < 1.f;
     }
@@ -1124,8 +1168,8 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
     const int nc0 = act0 ? (g.ny + rchunk - 1) / rchunk : 0;
     const int nc1 = act1 ? (g.nx + rchunk - 1) / rchunk : 0;
     const int K = nc0 + nc1;
-    const unsigned char* src0 = ltab0 + (size_t)slice * g.ny * line_bytes(g.nx);
-    const unsigned char* src1 = ltab1 + (size_t)slice * g.nx * line_bytes(g.ny);
+    const unsigned char* src0 = ltab0 + (size_t)blockIdx.x * g.ny * line_bytes(g.nx);
+    const unsigned char* src1 = ltab1 + (size_t)blockIdx.x * g.nx * line_bytes(g.ny);
 
     auto issue = [&](int k) {
         const int o = k < nc0 ? 0 : 1;
@@ -1173,7 +1217,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
                 accd[q] = 0.0;
                 alo[q] = 0.f;
                 if (vi < nvg && m < ipv) {
-                    const int view = v0 + vi;
+                    const int view = order[v0 + vi];
                     const float wx = tab.wx[view];
                     const bool active = o == 0 ? wx > 0.f : wx < 1.f;
                     const int j = 31 * m + lane;
@@ -1205,7 +1249,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
                 fp_item(warp, q, ipv, wpv, vi, m);
                 if (vi >= nvg || m >= ipv) continue;
                 const float sum = fp_cell_sum(accd[q], FAN ? B[q] : A[q]) / (float)(n + 1);
-                const int view = v0 + vi;
+                const int view = order[v0 + vi];
                 const int kk = 31 * m + lane;
                 const float wx = tab.wx[view];
                 const bool active = o == 0 ? wx > 0.f : wx < 1.f;
@@ -1234,7 +1278,7 @@ __global__ void __launch_bounds__(256, (fp_stream_min_blocks<FAN, NI>())) dd2d_f
             int vi, m;
             fp_item(warp, q, ipv, wpv, vi, m);
             if (vi >= nvg || m >= ipv) continue;
-            const int view = v0 + vi;
+            const int view = order[v0 + vi];
             const int kk = 31 * m + lane;
             if (lane >= 31 || kk >= d.nu) continue;
             float sn, cs;
@@ -1837,15 +1881,59 @@ const T* cptr(const void* p) { return static_cast<const T*>(p); }
 template <typename T>
 T* mptr(void* p) { return static_cast<T*>(p); }
 
-// Scratch of the forward projector: the edge table and the transposed image
-// (every path), then the line tables of the streamed path.
-size_t fp_workspace_min(const ctp_geometry& g) {
-    return align_up(table_floats(g.nview, g.nu) * sizeof(float)) + align_up(g.nbatch * g.nz * g.ny * g.nx * 4);
+// Scratch of the forward projector.  Every path starts with the edge table
+// and the order in which the streamed path takes the views.  The staged and
+// general kernels then read the transposed image of every slice
+// (fp_workspace_min).  The streamed path runs in chunks of slices: per chunk
+// the transposed slices and the row and column line tables
+// (fp_stream_bytes), rebuilt in the same buffer for each chunk.
+size_t fp_edge_table_bytes(const ctp_geometry& g) {
+    return align_up(table_floats(g.nview, g.nu) * sizeof(float)) + align_up(g.nview * sizeof(int));
 }
 
-size_t fp_line_tables_bytes(const ctp_geometry& g) {
-    size_t slices = g.nbatch * g.nz;
-    return align_up(slices * (g.ny * line_bytes((int)g.nx) + g.nx * line_bytes((int)g.ny)));
+size_t fp_workspace_min(const ctp_geometry& g) {
+    return fp_edge_table_bytes(g) + align_up(g.nbatch * g.nz * g.ny * g.nx * 4);
+}
+
+size_t fp_slice_tables_bytes(const ctp_geometry& g) {
+    return g.ny * line_bytes((int)g.nx) + g.nx * line_bytes((int)g.ny);
+}
+
+size_t fp_stream_bytes(const ctp_geometry& g, size_t chunk) {
+    return fp_edge_table_bytes(g) + align_up(chunk * g.ny * g.nx * 4) + align_up(chunk * fp_slice_tables_bytes(g));
+}
+
+// Largest chunk of the streamed path (transposed slices and line tables,
+// about 7.3 MB per 512 x 512 slice).  Measured on the 16-slice 512^2,
+// 720-view batch (B200, warm caches, every launch of one call): chunks of 4
+// slices stay resident in the L2 between the launches that write the
+// tables and the sweep that reads them, 73 MB of DRAM traffic per call (1.4x
+// the image and projections) at 3.27 ms; chunks of 8, 220 MB at 2.95 ms; one
+// chunk of 16, 576 MB at 2.86 ms.  The sweep is bound by shared memory and
+// instruction issue (576 MB in 2.86 ms is 3% of the HBM bandwidth), and a
+// chunk's launch of 2 waves pays its tail, so the default takes large
+// chunks; smaller workspaces (and ctp_set_fp_stream_slices) take smaller ones.
+constexpr size_t kFPChunkBytes = (size_t)256 << 20;
+
+// Cap on the slices per chunk (ctp_set_fp_stream_slices): negative = none,
+// 0 = no streamed path.
+std::atomic<int> g_fp_stream_cap{-1};
+
+// Slices per chunk of the streamed path with `ws` bytes of scratch: the
+// largest count up to the chunk limit (and the cap) whose scratch fits,
+// evened out over the chunks the stack then takes; 0 if one slice does not
+// fit.
+int fp_stream_slices(const ctp_geometry& g, size_t ws) {
+    const size_t nslices = g.nbatch * g.nz;
+    const size_t per = g.ny * g.nx * 4 + fp_slice_tables_bytes(g);
+    if (nslices == 0 || per == 0) return 0;
+    size_t c = std::min(nslices, std::max<size_t>(1, kFPChunkBytes / per));
+    const int cap = g_fp_stream_cap.load();
+    if (cap >= 0) c = std::min(c, (size_t)cap);
+    while (c > 0 && fp_stream_bytes(g, c) > ws) --c;
+    if (c == 0) return 0;
+    const size_t nchunks = (nslices + c - 1) / c;
+    return (int)((nslices + nchunks - 1) / nchunks);
 }
 
 // Lines per chunk of the streamed path's two-buffer ring, or 0 if one line
@@ -1971,45 +2059,47 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
     DDTab tab;
     int rc = build_table(reinterpret_cast<float*>(ws), deg, g, geom, s, tab, (type & CTP_TYPE_BRANCHLESS) ? 1 : 0);
     if (rc) return rc;
-    Tin* imgT = reinterpret_cast<Tin*>(ws + align_up(table_floats(g.nview, g.nu) * sizeof(float)));
-    dim3 tg((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 31) / 32), (unsigned)(g.nbatch * g.nz));
-    transpose_kernel<Tin><<<tg, dim3(32, 8), 0, s>>>(imgT, cptr<Tin>(img), (int)g.nx, (int)g.ny);
-    if ((rc = check_launch("transpose_kernel"))) return rc;
+    Tin* imgT = reinterpret_cast<Tin*>(ws + fp_edge_table_bytes(g));
+    const size_t slice_px = g.ny * g.nx;
+    auto transpose = [&](const Tin* from, int nsl) {
+        dim3 tg((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 31) / 32), (unsigned)nsl);
+        transpose_kernel<Tin><<<tg, dim3(32, 8), 0, s>>>(imgT, from, (int)g.nx, (int)g.ny);
+        return check_launch("transpose_kernel");
+    };
     int unweight = (geom == 1) && (type & CTP_TYPE_FORCE_FBP);
     int vgroup = 0, nrows = 0;
     const int rchunk = fp_stream_chunk(g);
-    // views per CTA and edge groups per warp
     const int nslices = (int)(g.nbatch * g.nz);
+    // the streamed path is the faster one from a single slice up (the tables
+    // are built once per slice instead of once per view group); it runs in
+    // chunks of slices sized to the workspace (fp_stream_slices), and a
+    // workspace without room for one slice's tables runs the staged kernel
+    const bool fast = fp_fast_ok(g, vgroup, nrows);
+    const int chunk = fast && rchunk > 0 ? fp_stream_slices(g, ws_bytes) : 0;
+    // views per CTA and edge groups per warp, for the slices of one launch
     int sms = 148, dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int launch_slices = chunk > 0 ? chunk : nslices;
     int sv = 0, ni = 0;
-    const bool shaped = fp_fast_ok(g, vgroup, nrows) &&
-                        (geom == 0 ? fan_shape(g, nslices, sms, sv, ni) : fp_stream_shape(g, sv, ni, kFMaxItems));
-    // the streamed path is the faster one from a single slice up (the tables
-    // are built once per slice instead of once per view group); a workspace
-    // without room for the line tables runs the staged kernel
-    if (shaped && rchunk > 0 && ws_bytes >= fp_workspace_min(g) + fp_line_tables_bytes(g)) {
-        // streamed path: line tables of rows (from the image) and columns (from its transpose)
-        unsigned char* lt0 = reinterpret_cast<unsigned char*>(ws + fp_workspace_min(g));
-        unsigned char* lt1 = lt0 + g.nbatch * g.nz * g.ny * line_bytes((int)g.nx);
-        long long rows = (long long)(g.nbatch * g.nz * g.ny), cols = (long long)(g.nbatch * g.nz * g.nx);
+    const bool shaped = fast && (geom == 0 ? fan_shape(g, launch_slices, sms, sv, ni)
+                                           : fp_stream_shape(g, sv, ni, kFMaxItems));
+    if (shaped && chunk > 0) {
+        // streamed path: per chunk, the line tables of rows (from the image)
+        // and columns (from its transpose), then the sweep
+        unsigned char* lt0 =
+            reinterpret_cast<unsigned char*>(ws + fp_edge_table_bytes(g) + align_up(chunk * slice_px * 4));
+        unsigned char* lt1 = lt0 + (size_t)chunk * g.ny * line_bytes((int)g.nx);
         // warps per CTA: as many as 96 KB of shared memory holds (at least one)
         const size_t wb = line_tables_warp_bytes((int)std::max(g.nx, g.ny));
         const int lt_warps = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / wb));
         const size_t lt_shm = (size_t)lt_warps * wb;
         cudaFuncSetAttribute(line_tables_kernel<Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lt_shm);
-        const unsigned rgrid = (unsigned)std::min<long long>((rows + lt_warps - 1) / lt_warps, 148 * 8);
-        const unsigned cgrid = (unsigned)std::min<long long>((cols + lt_warps - 1) / lt_warps, 148 * 8);
-        line_tables_kernel<Tin><<<rgrid, 32 * lt_warps, lt_shm, s>>>(lt0, cptr<Tin>(img), rows, (int)g.nx);
-        line_tables_kernel<Tin><<<cgrid, 32 * lt_warps, lt_shm, s>>>(lt1, imgT, cols, (int)g.ny);
-        if ((rc = check_launch("line_tables_kernel"))) return rc;
         // one slice per CTA (sharing the edge work across two slices halves the
         // lines per table chunk, and the warps then wait on the copies instead)
         if (geom != 0) {
             // a grid short of one wave of resident CTAs (few slices) takes
             // smaller view groups: more CTAs, each streaming the slice's tables
-            for (int cap = 8; cap >= 4 && ((g.nview + sv - 1) / sv) * (size_t)nslices < 2 * (size_t)sms;
-                 cap /= 2) {
+            for (int cap = 8; cap >= 4 && ((g.nview + sv - 1) / sv) * (size_t)chunk < 2 * (size_t)sms; cap /= 2) {
                 int sv2 = 0, ni2 = 0;
                 if (!fp_stream_shape(g, sv2, ni2, cap)) break;
                 sv = sv2;
@@ -2018,25 +2108,47 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
         }
         const int rc_s = rchunk;
         size_t shm = 2 * (size_t)rc_s * line_bytes((int)std::max(g.nx, g.ny));
-        dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)nslices);
         const bool fan = geom == 0;
         const int wpv = fan ? 8 / sv : 0;  // fan beams: warps per view (fp_item)
-        auto launch = [&](auto kern) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-            kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), lt0, lt1, tab, make_grid(g), make_det(g), (int)g.nview, sv,
-                                      wpv, rc_s, deg, unweight);
-        };
+        int* order = reinterpret_cast<int*>(ws + align_up(table_floats(g.nview, g.nu) * sizeof(float)));
+        blend_first_kernel<<<1, 1024, 0, s>>>(order, tab.wx, (int)g.nview);
+        if ((rc = check_launch("blend_first_kernel"))) return rc;
+        for (int s0 = 0; s0 < nslices; s0 += chunk) {
+            const int cs = std::min(chunk, nslices - s0);
+            const Tin* from = cptr<Tin>(img) + (size_t)s0 * slice_px;
+            if ((rc = transpose(from, cs))) return rc;
+            const long long rows = (long long)cs * g.ny, cols = (long long)cs * g.nx;
+            const unsigned rgrid = (unsigned)std::min<long long>((rows + lt_warps - 1) / lt_warps, 148 * 8);
+            const unsigned cgrid = (unsigned)std::min<long long>((cols + lt_warps - 1) / lt_warps, 148 * 8);
+            line_tables_kernel<Tin><<<rgrid, 32 * lt_warps, lt_shm, s>>>(lt0, from, rows, (int)g.nx);
+            line_tables_kernel<Tin><<<cgrid, 32 * lt_warps, lt_shm, s>>>(lt1, imgT, cols, (int)g.ny);
+            if ((rc = check_launch("line_tables_kernel"))) return rc;
+            // slices along x, view groups along y: CTAs are dispatched view
+            // group by view group, the blend band's first
+            dim3 fg((unsigned)cs, (unsigned)((g.nview + sv - 1) / sv));
+            auto launch = [&](auto kern) {
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+                cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                kern<<<fg, 256, shm, s>>>(mptr<Tout>(prj), lt0, lt1, tab, make_grid(g), make_det(g), (int)g.nview,
+                                          sv, wpv, rc_s, s0, order, deg, unweight);
+            };
 #define CTP_FP_STREAM(NI_)                                                       \
     if (fan) launch(dd2d_fp_stream_kernel<true, NI_, Tout>);                     \
     else launch(dd2d_fp_stream_kernel<false, NI_, Tout>)
-        if (ni == 4) { CTP_FP_STREAM(4); }
-        else if (ni == 8) { CTP_FP_STREAM(8); }
-        else if (ni == 12) { CTP_FP_STREAM(12); }
-        else { CTP_FP_STREAM(16); }
+            if (ni == 4) { CTP_FP_STREAM(4); }
+            else if (ni == 8) { CTP_FP_STREAM(8); }
+            else if (ni == 12) { CTP_FP_STREAM(12); }
+            else { CTP_FP_STREAM(16); }
 #undef CTP_FP_STREAM
-        return check_launch("dd2d_fp_stream_kernel");
+            if ((rc = check_launch("dd2d_fp_stream_kernel"))) return rc;
+        }
+        return CTP_OK;
     }
+    // the staged and general kernels read the transposed image of every slice
+    if (ws_bytes < fp_workspace_min(g))
+        return set_error(CTP_ERR_INVALID_ARGUMENT, "dd2d_fp: workspace of %zu bytes, the kernel needs %zu", ws_bytes,
+                         fp_workspace_min(g));
+    if ((rc = transpose(cptr<Tin>(img), nslices))) return rc;
     if (shaped) {
         size_t shm = (size_t)nrows * line_bytes((int)std::max(g.nx, g.ny));
         dim3 fg((unsigned)((g.nview + sv - 1) / sv), (unsigned)(g.nbatch * g.nz));
@@ -2068,21 +2180,41 @@ int launch_fp(void* prj, const void* img, const float* deg, const ctp_geometry& 
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
-size_t dd2d_fp_workspace(const ctp_geometry& g, int, int, unsigned) {
+namespace {
+// The streamed forward projector applies (slices projected one to one onto
+// detector rows, at most 128 edge groups per view, a line table pair fits
+// the shared-memory ring).
+bool fp_streamable(const ctp_geometry& g) {
     int vgroup = 0, nrows = 0;
-    bool stream = fp_fast_ok(g, vgroup, nrows) && fp_stream_chunk(g) > 0;
-    return fp_workspace_min(g) + (stream ? fp_line_tables_bytes(g) : 0);
+    return fp_fast_ok(g, vgroup, nrows) && fp_stream_chunk(g) > 0 && (g.nu + 30) / 31 <= 8 * kFMaxItems;
+}
+
+// The least workspace a caller may pass: one slice per chunk of the streamed
+// path where it applies, else the staged and general kernels' minimum.
+size_t fp_workspace_least(const ctp_geometry& g) {
+    return fp_streamable(g) && g_fp_stream_cap.load() != 0 ? std::min(fp_workspace_min(g), fp_stream_bytes(g, 1))
+                                                            : fp_workspace_min(g);
+}
+}  // namespace
+
+void set_fp_stream_cap(int max_slices) { g_fp_stream_cap.store(max_slices < 0 ? -1 : max_slices); }
+
+// The workspace of the fastest path: the streamed one in its largest chunks.
+size_t dd2d_fp_workspace(const ctp_geometry& g, int, int, unsigned) {
+    const int c = fp_streamable(g) ? fp_stream_slices(g, SIZE_MAX) : 0;
+    return c > 0 ? fp_stream_bytes(g, (size_t)c) : fp_workspace_min(g);
 }
 
 int dd2d_fp(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
             unsigned flags, void* workspace, size_t workspace_bytes, cudaStream_t s) {
     if (geom != 0 && geom != 1) return set_error(CTP_ERR_INVALID_ARGUMENT, "geom must be 0 (fan) or 1 (parallel)");
     Scratch scr;
-    // a caller's workspace of at least the minimum runs the staged path, one of
-    // the full query size (and scratch taken here) the streamed path
+    // a caller's workspace runs the streamed path in chunks of as many slices
+    // as it holds (the staged kernel if not one), scratch taken here the
+    // largest chunks of the workspace query
     const size_t full = dd2d_fp_workspace(g, geom, type, flags);
     const size_t have = workspace ? workspace_bytes : full;
-    int rc = scr.acquire(workspace, workspace_bytes, workspace ? fp_workspace_min(g) : full, s);
+    int rc = scr.acquire(workspace, workspace_bytes, workspace ? fp_workspace_least(g) : full, s);
     if (rc) return rc;
     bool in16 = flags & (CTP_FLAG_IN_BF16 | CTP_FLAG_IN_FP16);
     bool out16 = flags & (CTP_FLAG_OUT_BF16 | CTP_FLAG_OUT_FP16);
@@ -2374,7 +2506,7 @@ static int fp_scratch_address(void** out) {
 
 int dd2d_fp_noalloc(void* prj, const void* img, const float* deg, const ctp_geometry& g, int geom, int type,
                     unsigned flags, cudaStream_t s) {
-    size_t need = fp_workspace_min(g);
+    size_t need = fp_workspace_least(g);
     if (need > kNoAllocScratchBytes)
         return set_error(CTP_ERR_TOO_LARGE,
                          "ctp_dd2d_fp_noalloc needs %zu bytes of scratch; its fixed buffer holds %zu "

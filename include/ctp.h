@@ -238,10 +238,24 @@ int cTVSQS3D(float* s1, float* s2, float* var, const float* img, float wx, float
 /* ======================================================================== */
 /* geom 0 = fan (g->du is the angular cell size), 1 = parallel.
  * Replaces the cupyDistanceDriven{Fan,Parallel}Projection path
- * (distanceDriven2D.cu:109-200).  Default: overwrite prj. */
+ * (distanceDriven2D.cu:109-200).  Default: overwrite prj.  workspace may be
+ * NULL (the library's stream-ordered pool supplies the scratch); otherwise
+ * it holds workspace_bytes, at least a minimum that depends on the geometry.
+ * The streamed projector runs in chunks of slices, as many per chunk as the
+ * workspace holds up to 256 MiB of line tables and transposed slices;
+ * ctp_dd2d_fp_workspace returns the size of the largest chunks.  Smaller
+ * workspaces take smaller chunks, and one without room for a single slice's
+ * tables runs the staged kernel.  Every path gives the same result. */
 int ctp_dd2d_fp(void* prj, const void* img, const float* deg, const ctp_geometry* g, int geom, int typeProjector,
                 unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
 size_t ctp_dd2d_fp_workspace(const ctp_geometry* g, int geom, int typeProjector, unsigned flags);
+
+/* Caps the slices per chunk of the streamed forward projector of this
+ * process (max_slices > 0), makes it run the staged kernel (0), or lifts the
+ * cap (negative, the default).  Four slices of 512 x 512 per chunk keep the
+ * line tables resident in the L2 (a seventh of the DRAM traffic, about 14%
+ * more time).  For tests and tuning; no counterpart in the reference. */
+int ctp_set_fp_stream_slices(int max_slices);
 
 /* DD back projection (distanceDriven2D.cu:384-478).  Default: img += BP(prj)
  * in the reference's normalised form; CTP_FLAG_ADJOINT gives the exact

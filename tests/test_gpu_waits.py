@@ -1,6 +1,7 @@
 """The streamed forward projector (line tables copied into shared memory by
-bulk asynchronous copies) against the staged one on the same inputs, and the
-device-side wait counter: every bounded mbarrier wait of the run completed."""
+bulk asynchronous copies), in one chunk of slices and in several, against the
+staged one on the same inputs, and the device-side wait counter: every
+bounded mbarrier wait of the run completed."""
 import ctypes
 
 import numpy as np
@@ -43,10 +44,22 @@ def test_streamed_fp_equals_staged(geom_kind, n, nview, nu, du):
     img = torch.tensor(rng.uniform(0, 1, (8, 1, n, n)).astype(np.float32), device="cuda")
     span = 2 * np.pi if geom_kind == 0 else np.pi
     ang = torch.tensor((np.arange(nview) * span / nview).astype(np.float32), device="cuda")
-    full = lib().ctp_dd2d_fp_workspace(ctypes.byref(g), geom_kind, 0, 0)
+    L = lib()
+    full = L.ctp_dd2d_fp_workspace(ctypes.byref(g), geom_kind, 0, 0)
     streamed = _fp(g, geom_kind, img, ang, full)
-    # a workspace short of the line tables (but holding the rest) runs the staged kernel
-    staged = _fp(g, geom_kind, img, ang, full - 256)
+    try:
+        # the streamed path in chunks of 1 and 3 slices (3 + 3 + 2): the same
+        # tables and sums per slice, so the same bits
+        for cap in (1, 3):
+            assert L.ctp_set_fp_stream_slices(cap) == 0
+            chunked = _fp(g, geom_kind, img, ang, L.ctp_dd2d_fp_workspace(ctypes.byref(g), geom_kind, 0, 0))
+            torch.cuda.synchronize()
+            assert torch.equal(chunked, streamed), f"chunks of {cap} slices"
+        # no streamed path: the staged kernel (tables built per CTA in shared memory)
+        assert L.ctp_set_fp_stream_slices(0) == 0
+        staged = _fp(g, geom_kind, img, ang, L.ctp_dd2d_fp_workspace(ctypes.byref(g), geom_kind, 0, 0))
+    finally:
+        assert L.ctp_set_fp_stream_slices(-1) == 0
     torch.cuda.synchronize()
     assert rel_l2(streamed.cpu().numpy(), staged.cpu().numpy()) <= 1e-6
 

@@ -90,7 +90,7 @@ def test_noalloc_rejects_requests_beyond_its_buffer():
     L = lib()
     cap = L.ctp_dd2d_fp_noalloc_capacity()
     assert cap == 32 << 20
-    g = _geometry(64, 512, 720, 768, 0.8, 0.8)  # 64 MiB transposed image alone
+    g = _geometry(1, 512, 720, 3000, 0.8, 0.8)  # 52 MB edge table alone
     assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) > cap
     dummy = torch.empty(1, device="cuda")
     p = ctypes.c_void_p(dummy.data_ptr())
@@ -107,43 +107,69 @@ def _scratch_allocations():
     return c.value
 
 
-def test_noalloc_staged_path_allocates_nothing():
-    """The 16-slice 512 x 512 stack with 60 views of 768 cells: its edge table
-    and transposed image fit the fixed scratch but its line tables (101 MB) do
-    not, so the call runs the staged kernel (tables built per CTA in shared
-    memory).  Three calls in a row: each equals ctp_dd2d_fp, none makes a
-    scratch allocation, and the device's free memory does not move between
-    the second and the third."""
+def _noalloc_repeat(g, geom_kind, img, ang, calls=3):
+    """ctp_dd2d_fp with the queried workspace, then `calls` noalloc calls:
+    each must equal it, none may make a scratch allocation, and the device's
+    free memory must not move between the last two."""
     from ctprojector_b200._lib import lib
 
     L = lib()
-    rng = np.random.default_rng(99)
-    nb, n, nview, nu = 16, 512, 60, 768
-    g = _geometry(nb, n, nview, nu, 0.8, 0.8)
-    cap = L.ctp_dd2d_fp_noalloc_capacity()
-    assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) > cap  # line tables do not fit
-    img = torch.tensor(rng.uniform(0, 0.03, (nb, 1, n, n)).astype(np.float32), device="cuda")
-    ang = torch.tensor(np.sort(rng.uniform(0, np.pi, nview)).astype(np.float32), device="cuda")
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    shape = (nb, nview, 1, nu)
-    ws_bytes = L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0)
+    shape = (g.nbatch, g.nview, g.nv, g.nu)
+    ws_bytes = L.ctp_dd2d_fp_workspace(ctypes.byref(g), geom_kind, 0, 0)
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
     ref = torch.empty(shape, dtype=torch.float32, device="cuda")
     assert L.ctp_dd2d_fp(ctypes.c_void_p(ref.data_ptr()), ctypes.c_void_p(img.data_ptr()),
-                         ctypes.c_void_p(ang.data_ptr()), ctypes.byref(g), 1, 0, 0,
+                         ctypes.c_void_p(ang.data_ptr()), ctypes.byref(g), geom_kind, 0, 0,
                          ctypes.c_void_p(ws.data_ptr()), ws_bytes, stream) == 0
-    outs = [torch.full(shape, float("nan"), dtype=torch.float32, device="cuda") for _ in range(3)]
+    outs = [torch.full(shape, float("nan"), dtype=torch.float32, device="cuda") for _ in range(calls)]
     torch.cuda.synchronize()
     allocs0 = _scratch_allocations()
     free = []
     for out in outs:
         assert L.ctp_dd2d_fp_noalloc(ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(img.data_ptr()),
-                                     ctypes.c_void_p(ang.data_ptr()), ctypes.byref(g), 1, 0, 0, stream) == 0
+                                     ctypes.c_void_p(ang.data_ptr()), ctypes.byref(g), geom_kind, 0, 0, stream) == 0
         torch.cuda.synchronize()
         free.append(torch.cuda.mem_get_info()[0])
     assert _scratch_allocations() == allocs0
-    assert free[1] == free[2]
+    assert free[-2] == free[-1]
     r = ref.cpu().numpy()
     assert np.isfinite(r).all() and np.abs(r).max() > 0
     for out in outs:
         assert rel_l2(out.cpu().numpy(), r) <= TOL
+
+
+def test_noalloc_chunked_stream_on_the_benchmark_stack():
+    """The 16-slice 512 x 512 stack with 720 views of 768 cells: the full
+    query (one chunk of 16 slices, 130 MB) exceeds the fixed 32 MiB, which
+    holds the edge table and chunks of 2 slices' transposed images and line
+    tables, so the call runs the streamed kernel in 8 chunks.  Three calls in
+    a row equal ctp_dd2d_fp and allocate nothing."""
+    from ctprojector_b200._lib import lib
+
+    L = lib()
+    rng = np.random.default_rng(98)
+    nb, n, nview, nu = 16, 512, 720, 768
+    g = _geometry(nb, n, nview, nu, 0.8, 0.8)
+    assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) > L.ctp_dd2d_fp_noalloc_capacity()
+    img = torch.tensor(rng.uniform(0, 0.03, (nb, 1, n, n)).astype(np.float32), device="cuda")
+    ang = torch.tensor((np.arange(nview) * np.pi / nview).astype(np.float32), device="cuda")
+    _noalloc_repeat(g, 1, img, ang)
+
+
+def test_noalloc_staged_path_allocates_nothing():
+    """One 2048 x 2048 slice with 60 views of 2560 cells: its edge table and
+    transposed image fit the fixed scratch but one slice's line tables
+    (101 MB) do not, so the call runs the staged kernel (tables built per
+    CTA in shared memory).  Three calls in a row equal ctp_dd2d_fp and
+    allocate nothing."""
+    from ctprojector_b200._lib import lib
+
+    L = lib()
+    rng = np.random.default_rng(99)
+    nb, n, nview, nu = 1, 2048, 60, 2560
+    g = _geometry(nb, n, nview, nu, 0.8, 0.8)
+    assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) > L.ctp_dd2d_fp_noalloc_capacity()
+    img = torch.tensor(rng.uniform(0, 0.03, (nb, 1, n, n)).astype(np.float32), device="cuda")
+    ang = torch.tensor(np.sort(rng.uniform(0, np.pi, nview)).astype(np.float32), device="cuda")
+    _noalloc_repeat(g, 1, img, ang)
