@@ -117,6 +117,43 @@ def test_fp_workspace_line_tables_up_to_128_edge_groups():
     assert ws(4000) < edge_table(4000) + image + line_tables
 
 
+def _align(x, a=256):
+    return (x + a - 1) // a * a
+
+
+def test_fp_workspace_follows_the_stream_chunk():
+    """The streamed forward projector runs in chunks of slices, each chunk's
+    transposed slices and line tables rebuilt in one buffer.  For the
+    16-slice 512 x 512, 720-view, 768-cell batch the query returns one chunk
+    of all 16 slices; capped at 4 slices per chunk (ctp_set_fp_stream_slices)
+    a quarter of that; with the streamed path off (cap 0), the staged
+    kernel's edge table and transposed stack.  Host-side sizing only: no GPU."""
+    from ctprojector_b200._lib import Geometry, lib
+
+    L = lib()
+    nb, n, nview, nu = 16, 512, 720, 768
+    g = Geometry(nb, n, n, 1, 0.8, 0.8, 1, 0, 0, 0, nu, 1, nview, 0.8, 1, 0, 0, 1000.0, 500.0)
+    edge = _align((2 * (2 * nview * (nu + 1) + nview * nu) + 5 * nview) * 4) + _align(nview * 4)
+    line = (n + 2) * 8 + (n + 4) * 4  # FP64 and FP32 entries of one line's table, each padded
+    slice_tables = 2 * n * line
+    slice_px = n * n * 4
+
+    def stream(chunk):
+        return edge + _align(chunk * slice_px) + _align(chunk * slice_tables)
+
+    try:
+        assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) == stream(16)
+        assert L.ctp_set_fp_stream_slices(4) == 0
+        assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) == stream(4)
+        assert L.ctp_set_fp_stream_slices(3) == 0  # 16 slices in chunks of at most 3: 6 chunks of 3 or fewer
+        assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) == stream(3)
+        assert L.ctp_set_fp_stream_slices(0) == 0
+        assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) == edge + _align(nb * slice_px)
+    finally:
+        assert L.ctp_set_fp_stream_slices(-1) == 0
+    assert L.ctp_dd2d_fp_workspace(ctypes.byref(g), 1, 0, 0) == stream(16)
+
+
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     import ctprojector_b200._lib as L
     from ctprojector_b200.errors import CTProjectorError
