@@ -1404,8 +1404,9 @@ inline size_t par_fast_smem(int win, int S) {
 // positions and each lookup's index and fraction are shared; only the table
 // reads and the sums repeat per slice.
 // Views are split over blockIdx.z in parts of vper (a multiple of kPViews)
-// when the tile grid alone leaves SMs idle; part z writes its own partial
-// volume at img + z * part_elems (summed by bp_parts_sum_kernel).
+// when the tile grid alone leaves SMs idle or fills its last wave poorly
+// (bp_view_parts); part z writes its own partial volume at
+// img + z * part_elems (summed by bp_parts_sum_kernel).
 template <typename Tp, typename Tout, int S>
 __global__ void __launch_bounds__(256) dd2d_bp_par_fast_kernel(Tout* __restrict__ img, const Tp* __restrict__ prj,
                                                                const float* __restrict__ deg, int nview, Grid g,
@@ -2276,7 +2277,26 @@ int bp_view_parts(size_t ctas, int nview, int& vper) {
         return 1;
     }
     int parts = 1;
-    if (ctas > 0 && ctas < (size_t)sms) parts = (int)std::min<size_t>(8, (2 * (size_t)sms + ctas - 1) / ctas);
+    if (ctas > 0 && ctas < (size_t)sms) {
+        parts = (int)std::min<size_t>(8, (2 * (size_t)sms + ctas - 1) / ctas);
+    } else if (ctas >= 2 * (size_t)sms && ctas < 6 * (size_t)sms) {
+        // A grid of one to three waves of equal CTAs (2 resident per SM: the
+        // fast kernels' registers and shared memory) whose last wave is far
+        // from full leaves SMs idle at the end: split the views into the
+        // parts (up to 8) that fill the waves best, summed by one more pass
+        // over the output.  Measured: the 4-slice 512^2 fan batch (512 CTAs,
+        // 1.7 waves) 1.60 -> 1.39 ms with 4 parts; the 16-slice parallel
+        // batch (1024 CTAs, 3.5 waves, whose tail is already spread over the
+        // SMs) unchanged with 2.
+        const double slots = 2.0 * sms;
+        auto fill = [&](int p) {
+            const double waves = (double)ctas * p / slots;
+            return waves / std::ceil(waves);
+        };
+        if (fill(1) < 0.95)
+            for (int p = 2; p <= 8; ++p)
+                if (fill(p) > fill(parts) + 0.02) parts = p;
+    }
     parts = std::max(1, std::min(parts, chunks));
     vper = ((chunks + parts - 1) / parts) * kPViews;
     return (nview + vper - 1) / vper;

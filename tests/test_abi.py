@@ -81,11 +81,18 @@ def test_workspace_queries_need_no_gpu():
     assert lib().ctp_tomo_bp_workspace(ctypes.byref(g)) >= 16 * 720 * 768 * 4
 
 
+def _align(x, a=256):
+    return (x + a - 1) // a * a
+
+
 def test_bp_workspace_holds_view_parts():
     """One 256 x 256 fan slice gives the fast back projector 64 tiles, fewer
     than the SMs, so its views are split into parts with FP32 partial
-    volumes in the workspace (besides the pre-weighted sinogram); the
-    16-slice batch needs no parts."""
+    volumes in the workspace (besides the pre-weighted sinogram).  A
+    16-slice 256^2 fan stack (512 CTAs of two slices: 1.7 waves of 2 per SM
+    on 148 SMs) takes the 4 parts that fill the waves best; the 16-slice
+    512^2 parallel batch (1024 CTAs of four slices, 3.5 waves) takes none.
+    Host-side sizing only: no GPU."""
     from ctprojector_b200._lib import Geometry, lib
 
     da = 1.2858 / 1085.6
@@ -93,7 +100,10 @@ def test_bp_workspace_holds_view_parts():
     stack = Geometry(16, 256, 256, 1, 1.0, 1.0, 1, 0, 0, 0, 736, 1, 360, da, 1, 0, 0, 1085.6, 595.0)
     pre = 360 * 736 * 4
     assert lib().ctp_dd2d_bp_workspace(ctypes.byref(one), 0, 0, 0) >= pre + 2 * 256 * 256 * 4
-    assert lib().ctp_dd2d_bp_workspace(ctypes.byref(stack), 0, 0, 0) < 16 * pre + 4096
+    stack_ws = lib().ctp_dd2d_bp_workspace(ctypes.byref(stack), 0, 0, 0)
+    assert stack_ws == _align(16 * pre) + _align(4 * 16 * 256 * 256 * 4)
+    par = Geometry(16, 512, 512, 1, 0.8, 0.8, 1, 0, 0, 0, 768, 1, 720, 0.8, 1, 0, 0, 1000, 500)
+    assert lib().ctp_dd2d_bp_workspace(ctypes.byref(par), 1, 0, 0) == 0
 
 
 def test_fp_workspace_line_tables_up_to_128_edge_groups():
@@ -115,10 +125,6 @@ def test_fp_workspace_line_tables_up_to_128_edge_groups():
     image = 256 * 256 * 4
     assert ws(3000) >= edge_table(3000) + image + line_tables
     assert ws(4000) < edge_table(4000) + image + line_tables
-
-
-def _align(x, a=256):
-    return (x + a - 1) // a * a
 
 
 def test_fp_workspace_follows_the_stream_chunk():
